@@ -1,0 +1,565 @@
+// les_api.cu -- implementation of the C ABI in include/les_gpu.h.
+//
+// Owns the device arena of one solver context, the host-side derivation of the constant
+// table (with the same operations the reference applies to its macros and loaded species
+// data), uploads/downloads in the reference's [i][j][k] order, and the stream-ordered step.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "les_ctx.h"
+#include "les_gpu.h"
+
+using les::DevCtx;
+
+struct lesgpu_ctx {
+    DevCtx d;
+    lesgpu_config cfg;
+    lesgpu_species sp;
+};
+
+namespace {
+
+int fail(lesgpu_ctx* c, int code, const std::string& msg) {
+    if (c) c->d.err = msg;
+    return code;
+}
+
+int cuda_fail(lesgpu_ctx* c, cudaError_t e, const char* where) {
+    std::string m = std::string(where) + ": " + cudaGetErrorString(e);
+    if (c) c->d.err = m;
+    return LESGPU_ECUDA;
+}
+
+#define CK(call)                                                   \
+    do {                                                           \
+        cudaError_t e_ = (call);                                   \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call);   \
+    } while (0)
+
+bool all_zero4(const double* c) { return c[0] == 0.0 && c[1] == 0.0 && c[2] == 0.0 && c[3] == 0.0; }
+
+// Constant table: grid spacings and the species/model constants in the form the kernels use.
+void build_consts(const lesgpu_config& g, const lesgpu_species& sp, les::Consts& C) {
+    memset(&C, 0, sizeof(C));
+    C.nx = g.nx; C.ny = g.ny; C.nz = g.nz;
+    C.flame_accel = g.flame_accel;
+    C.weno_step = g.weno_transition_step;
+    C.dx = g.lx / (double)g.nx;          // DX (:104-106)
+    C.dy = g.ly / (double)g.ny;
+    C.dz = g.lz / (double)g.nz;
+    C.two_dx = 2.0 * C.dx; C.two_dy = 2.0 * C.dy; C.two_dz = 2.0 * C.dz;
+    C.dxx = C.dx * C.dx; C.dyy = C.dy * C.dy; C.dzz = C.dz * C.dz;
+    C.dx4 = pow(C.dx, 4.0);
+    C.inlet_center_z = g.lz / 2.0;       // INLET_CENTER_Z (:110)
+    for (int s = 0; s < les::NSP; s++) {
+        C.mw[s] = sp.mw[s];
+        C.mwk[s] = sp.mw[s] / 1000.0;
+        C.t_mid[s] = sp.t_mid[s];
+        for (int q = 0; q < 7; q++) { C.nasa_high[s][q] = sp.nasa_high[s][q]; C.nasa_low[s][q] = sp.nasa_low[s][q]; }
+        for (int q = 0; q < 4; q++) { C.eta[s][q] = sp.eta[s][q]; C.lam[s][q] = sp.lambda[s][q]; }
+        C.eta_zero[s] = all_zero4(sp.eta[s]);
+        C.lam_zero[s] = all_zero4(sp.lambda[s]);
+    }
+    int sym = 1;
+    for (int a = 0; a < les::NSP; a++)
+        for (int b = 0; b < les::NSP; b++) {
+            for (int q = 0; q < 4; q++) C.dco[a][b][q] = sp.dcoef[a][b][q];
+            C.dco_zero[a][b] = all_zero4(sp.dcoef[a][b]);
+            if (a != b && memcmp(sp.dcoef[a][b], sp.dcoef[b][a], 4 * sizeof(double)) != 0) sym = 0;
+            // Wilke / Wassiljew pair constants (:1540, :1855), evaluated with the host libm
+            // exactly as the reference evaluates them per cell.
+            C.wpow[a][b] = pow(sp.mw[b] / sp.mw[a], 0.25);
+            C.wden[a][b] = sqrt(8.0) * sqrt(1.0 + sp.mw[a] / sp.mw[b]);
+        }
+    C.dco_sym = sym;
+    C.cs_u = g.cs_unburned; C.cs_b = g.cs_burnt; C.cs_boost = g.cs_flame_boost;
+    C.accel_strength = g.accel_strength;
+    C.accel_center = g.accel_center;
+    C.two_w2 = 2.0 * g.accel_width * g.accel_width;
+    C.relax = g.relax;
+    C.s_l = g.s_l; C.nu_u = g.nu_unburnt; C.d3 = g.d3;
+    double dF = g.nu_unburnt / (g.s_l + 1e-10);                         // :1941
+    C.ssr_cdF = 10.0 * dF;                                              // :1943
+    double tau = (g.rho_unburnt_approx / g.rho_burnt_approx) - 1.0;     // :2703
+    C.tau_sl = tau * g.s_l;
+    C.sc_t2 = 2.0 * g.sc_t; C.pr_t2 = 2.0 * g.pr_t;
+    C.t_in = g.inlet_temperature; C.t_amb = g.ambient_temperature;
+    C.t_burnt_span = g.burnt_gas_temperature - g.inlet_temperature;
+    // inlet composition and stoichiometry (:4101-4120)
+    const double phi = g.equivalence_ratio;
+    double m_f = 1.0, m_o2 = 5.0 / phi, m_n2 = m_o2 * 3.76;
+    double mass_total = m_f * sp.mw[0] + m_o2 * sp.mw[1] + m_n2 * sp.mw[2];
+    C.inletYk[0] = (m_f * sp.mw[0]) / mass_total;
+    C.inletYk[1] = (m_o2 * sp.mw[1]) / mass_total;
+    C.inletYk[2] = (m_n2 * sp.mw[2]) / mass_total;
+    C.inletYk[3] = 0.0; C.inletYk[4] = 0.0;
+    C.ambientYk[0] = 0.0; C.ambientYk[1] = 0.232; C.ambientYk[2] = 0.768; C.ambientYk[3] = 0.0; C.ambientYk[4] = 0.0;
+    double st_o2 = (5.0 * sp.mw[1]) / sp.mw[0];
+    double st_co2 = (3.0 * sp.mw[3]) / sp.mw[0];
+    double st_h2o = (4.0 * sp.mw[4]) / sp.mw[0];
+    C.cons_o2 = C.inletYk[0] * st_o2;
+    C.prod_co2 = C.inletYk[0] * st_co2;
+    C.prod_h2o = C.inletYk[0] * st_h2o;
+    C.u_in = g.inlet_velocity;
+    C.noise_amp = 0.10 * g.inlet_velocity;                              // :2987
+    C.ti_rms = g.inlet_velocity * g.turbulence_intensity;              // :1050
+}
+
+unsigned char* read_record(FILE* fp, int* len) {
+    int n;
+    if (fread(&n, sizeof(int), 1, fp) != 1 || n < 0 || n > (1 << 26)) return nullptr;
+    unsigned char* b = (unsigned char*)malloc((size_t)n + 1);
+    if (!b) return nullptr;
+    if (fread(b, 1, (size_t)n, fp) != (size_t)n) { free(b); return nullptr; }
+    int e;
+    if (fread(&e, sizeof(int), 1, fp) != 1 || e != n) { free(b); return nullptr; }
+    if (len) *len = n;
+    return b;
+}
+
+size_t fields_for_precision() { return 55; }
+
+}  // namespace
+
+extern "C" {
+
+int lesgpu_load_species(const char* chem_path, const char* tran_path, lesgpu_species* out) {
+    if (!chem_path || !tran_path || !out) return LESGPU_EINVAL;
+    memset(out, 0, sizeof(*out));
+    FILE* fp = fopen(chem_path, "rb");
+    if (!fp) return LESGPU_EIO;
+    int len = 0, mm = 0, kk = 0;
+    unsigned char* b = read_record(fp, &len);
+    if (!b) { fclose(fp); return LESGPU_EIO; }
+    free(b);
+    b = read_record(fp, &len);
+    if (!b || len < 20) { free(b); fclose(fp); return LESGPU_EIO; }
+    memcpy(&mm, b + 12, 4); memcpy(&kk, b + 16, 4);
+    free(b);
+    if (kk != LESGPU_NSP || mm < 0 || mm > 64) { fclose(fp); return LESGPU_EIO; }
+    b = read_record(fp, &len);
+    if (!b) { fclose(fp); return LESGPU_EIO; }
+    free(b);
+    b = read_record(fp, &len);
+    size_t per = 16 + 4 * (size_t)mm + 8 + 8 + 4 + 24 + 2 * 56;
+    if (!b || (size_t)len < 8 + per * LESGPU_NSP) { free(b); fclose(fp); return LESGPU_EIO; }
+    for (int i = 0; i < LESGPU_NSP; i++) {
+        size_t base = 8 + (size_t)i * per;
+        size_t mwo = base + 16 + 4 * (size_t)mm + 8;
+        size_t tmo = mwo + 8 + 4 + 16;
+        memcpy(&out->mw[i], b + mwo, 8);
+        memcpy(&out->t_mid[i], b + tmo, 8);
+        memcpy(out->nasa_high[i], b + tmo + 8, 56);
+        memcpy(out->nasa_low[i], b + tmo + 8 + 56, 56);
+    }
+    free(b);
+    fclose(fp);
+    fp = fopen(tran_path, "rb");
+    if (!fp) return LESGPU_EIO;
+    for (int r = 0; r < 4; r++) {
+        b = read_record(fp, &len);
+        if (!b) { fclose(fp); return LESGPU_EIO; }
+        free(b);
+    }
+    b = read_record(fp, &len);
+    if (!b || len < 32 * LESGPU_NSP) { free(b); fclose(fp); return LESGPU_EIO; }
+    for (int i = 0; i < LESGPU_NSP; i++) memcpy(out->lambda[i], b + 32 * i, 32);
+    free(b);
+    b = read_record(fp, &len);
+    if (!b || len < 32 * LESGPU_NSP) { free(b); fclose(fp); return LESGPU_EIO; }
+    for (int i = 0; i < LESGPU_NSP; i++) memcpy(out->eta[i], b + 32 * i, 32);
+    free(b);
+    b = read_record(fp, &len);
+    if (!b || len < 32 * LESGPU_NSP * LESGPU_NSP) { free(b); fclose(fp); return LESGPU_EIO; }
+    for (int i = 0; i < LESGPU_NSP; i++)
+        for (int j = 0; j < LESGPU_NSP; j++) memcpy(out->dcoef[i][j], b + 32 * (i * LESGPU_NSP + j), 32);
+    free(b);
+    fclose(fp);
+    for (int i = 0; i < LESGPU_NSP; i++)
+        if (!(out->mw[i] > 0.0)) return LESGPU_EIO;
+    return LESGPU_OK;
+}
+
+size_t lesgpu_bytes_for_grid(int nx, int ny, int nz, int precision) {
+    size_t n = (size_t)nx * ny * nz;
+    size_t esz = (precision == LESGPU_FP32) ? 4 : 8;
+    size_t nb = ((size_t)(nz + les::BX - 1) / les::BX) * ((ny + les::BY - 1) / les::BY) * nx;
+    size_t planes = (size_t)ny * nz;
+    return fields_for_precision() * n * esz + n +              // fields + attribute bytes
+           (6 * nb + 64) * sizeof(double) +                       // reduction partials
+           planes * (3 * sizeof(double) + 2 * sizeof(int)) +      // SEM planes + inlet maps
+           3 * planes * sizeof(double) + sizeof(les::Consts) + sizeof(les::Scalars) + (1 << 16);
+}
+
+int lesgpu_create(const lesgpu_config* cfg, const lesgpu_species* sp, lesgpu_ctx** out) {
+    if (!cfg || !sp || !out) return LESGPU_EINVAL;
+    *out = nullptr;
+    if (cfg->nx < 4 || cfg->ny < 4 || cfg->nz < 4 || cfg->num_vortices < 0) return LESGPU_EINVAL;
+    if (cfg->precision != LESGPU_FP64 && cfg->precision != LESGPU_FP32) return LESGPU_EINVAL;
+    if ((size_t)cfg->ny * cfg->nz > (size_t)1 << 30 || (size_t)cfg->nx > 65535) return LESGPU_EINVAL;
+    lesgpu_ctx* ctx = new (std::nothrow) lesgpu_ctx();
+    if (!ctx) return LESGPU_ENOMEM;
+    ctx->cfg = *cfg;
+    ctx->sp = *sp;
+    DevCtx& d = ctx->d;
+    d.nx = cfg->nx; d.ny = cfg->ny; d.nz = cfg->nz;
+    d.n = (size_t)cfg->nx * cfg->ny * cfg->nz;
+    d.precision = cfg->precision;
+    d.esz = (cfg->precision == LESGPU_FP32) ? 4 : 8;
+    build_consts(*cfg, *sp, d.hC);
+    cudaError_t e = cudaSetDevice(cfg->device);
+    if (e != cudaSuccess) { int r = cuda_fail(ctx, e, "cudaSetDevice"); delete ctx; return r; }
+    e = cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { int r = cuda_fail(ctx, e, "cudaStreamCreate"); delete ctx; return r; }
+    // one arena for all per-cell fields; each field starts on a 256-byte boundary
+    const size_t fb = ((d.n * d.esz + 255) / 256) * 256;
+    const size_t nf = fields_for_precision();
+    d.arena_bytes = nf * fb;
+    e = cudaMalloc(&d.arena, d.arena_bytes);
+    if (e != cudaSuccess) { ctx->d.err = "device arena allocation failed"; lesgpu_destroy(ctx); return LESGPU_ENOMEM; }
+    cudaMemsetAsync(d.arena, 0, d.arena_bytes, d.stream);
+    char* p = (char*)d.arena;
+    auto take = [&]() { void* r = p; p += fb; return r; };
+    for (int q = 0; q < les::NSTATE; q++) d.S[q] = take();
+    for (int q = 0; q < les::NSTATE; q++) d.St[q] = take();
+    for (int q = 0; q < les::NSTATE; q++) d.F[q] = take();
+    d.mu_mix = take(); d.nu = take();
+    for (int s = 0; s < les::NSP; s++) d.D[s] = take();
+    d.aT = take(); d.nu_t = take(); d.S_mag = take(); d.ST = take(); d.mu_eff = take();
+    for (int q = 0; q < les::NACC; q++) d.acc[q] = take();
+    size_t nb = ((size_t)(d.nz + les::BX - 1) / les::BX) * ((d.ny + les::BY - 1) / les::BY) * d.nx;
+    d.part_len = 6 * nb + 64;
+    size_t planes = (size_t)d.ny * d.nz;
+    bool ok = cudaMalloc(&d.attr, d.n) == cudaSuccess &&
+              cudaMalloc(&d.dC, sizeof(les::Consts)) == cudaSuccess &&
+              cudaMalloc(&d.dS, sizeof(les::Scalars)) == cudaSuccess &&
+              cudaMalloc(&d.part, d.part_len * sizeof(double)) == cudaSuccess &&
+              cudaMalloc(&d.plane, 3 * planes * sizeof(double)) == cudaSuccess &&
+              cudaMalloc(&d.noise, 3 * planes * sizeof(double)) == cudaSuccess &&
+              cudaMalloc(&d.inlet_list, planes * sizeof(int)) == cudaSuccess &&
+              cudaMalloc(&d.inlet_pos, planes * sizeof(int)) == cudaSuccess &&
+              cudaMalloc(&d.flag, sizeof(int)) == cudaSuccess;
+    if (!ok) { ctx->d.err = "device allocation failed"; lesgpu_destroy(ctx); return LESGPU_ENOMEM; }
+    d.nv_cap = cfg->num_vortices > 0 ? cfg->num_vortices : 1;
+    if (cudaMalloc(&d.vort, (size_t)d.nv_cap * 7 * sizeof(double)) != cudaSuccess) {
+        ctx->d.err = "vortex buffer allocation failed";
+        lesgpu_destroy(ctx);
+        return LESGPU_ENOMEM;
+    }
+    d.h_pinned_len = d.n * 8;
+    if (cudaMallocHost(&d.h_pinned, d.h_pinned_len) != cudaSuccess) {
+        d.h_pinned = nullptr;
+        d.h_pinned_len = 0;
+    }
+    cudaMemsetAsync(d.dS, 0, sizeof(les::Scalars), d.stream);
+    cudaMemsetAsync(d.attr, 0, d.n, d.stream);
+    cudaMemsetAsync(d.plane, 0, 3 * planes * sizeof(double), d.stream);
+    cudaMemsetAsync(d.noise, 0, 3 * planes * sizeof(double), d.stream);
+    cudaMemcpyAsync(d.dC, &d.hC, sizeof(les::Consts), cudaMemcpyHostToDevice, d.stream);
+    e = cudaStreamSynchronize(d.stream);
+    if (e != cudaSuccess) { int r = cuda_fail(ctx, e, "create"); lesgpu_destroy(ctx); return r; }
+    d.total_bytes = d.arena_bytes + d.n + d.part_len * sizeof(double) + 3 * planes * sizeof(double) * 2 +
+                    2 * planes * sizeof(int) + (size_t)d.nv_cap * 7 * sizeof(double) + sizeof(les::Consts) +
+                    sizeof(les::Scalars);
+    *out = ctx;
+    return LESGPU_OK;
+}
+
+void lesgpu_destroy(lesgpu_ctx* ctx) {
+    if (!ctx) return;
+    DevCtx& d = ctx->d;
+    if (d.stream) cudaStreamSynchronize(d.stream);
+    void* bufs[] = {d.arena, d.attr, d.dC, d.dS, d.part, d.plane, d.noise, d.vort, d.inlet_list, d.inlet_pos,
+                    d.probe_st, d.probe_out, d.flag, d.dbg_cp, d.dbg_lam, d.dbg_alpha};
+    for (void* b : bufs)
+        if (b) cudaFree(b);
+    for (int q = 0; q < les::NACC; q++)
+        if (d.kd[q]) cudaFree(d.kd[q]);
+    if (d.h_pinned) cudaFreeHost(d.h_pinned);
+    if (d.stream) cudaStreamDestroy(d.stream);
+    delete ctx;
+}
+
+const char* lesgpu_last_error(const lesgpu_ctx* ctx) { return ctx ? ctx->d.err.c_str() : "null context"; }
+
+size_t lesgpu_device_bytes(const lesgpu_ctx* ctx) { return ctx ? ctx->d.total_bytes : 0; }
+
+int lesgpu_upload_attribute(lesgpu_ctx* ctx, const int* attr) {
+    if (!ctx || !attr) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    std::vector<uint8_t> a8(d.n);
+    for (size_t q = 0; q < d.n; q++) {
+        if (attr[q] < 0 || attr[q] > 6) return fail(ctx, LESGPU_EINVAL, "attribute codes must be in 0..6");
+        a8[q] = (uint8_t)attr[q];
+    }
+    // inlet cells of the i = 0 face in (j, k) order (:4366-4367)
+    const size_t planes = (size_t)d.ny * d.nz;
+    std::vector<int> list, pos(planes, -1);
+    for (int j = 0; j < d.ny; j++)
+        for (int k = 0; k < d.nz; k++) {
+            size_t p = (size_t)j * d.nz + k;
+            if (attr[p] == 1) { pos[p] = (int)list.size(); list.push_back((int)p); }
+        }
+    // total fluid volume of the <rho_f> average, summed serially as the reference does (:2545)
+    const double dv = d.hC.dx * d.hC.dy * d.hC.dz;
+    double tv = 0.0;
+    for (size_t q = 0; q < d.n; q++) {
+        int v = attr[q];
+        if (v == 1 || v == 2 || v == 3 || v == 5) tv += dv;
+    }
+    d.hC.total_volume = tv;
+    d.hC.n_inlet = (int)list.size();
+    d.n_inlet = (int)list.size();
+    d.h_inlet = list;
+    CK(cudaMemcpyAsync(d.attr, a8.data(), d.n, cudaMemcpyHostToDevice, d.stream));
+    if (!list.empty())
+        CK(cudaMemcpyAsync(d.inlet_list, list.data(), list.size() * sizeof(int), cudaMemcpyHostToDevice, d.stream));
+    CK(cudaMemcpyAsync(d.inlet_pos, pos.data(), planes * sizeof(int), cudaMemcpyHostToDevice, d.stream));
+    CK(cudaMemcpyAsync(d.dC, &d.hC, sizeof(les::Consts), cudaMemcpyHostToDevice, d.stream));
+    CK(cudaStreamSynchronize(d.stream));
+    d.have_attr = true;
+    return LESGPU_OK;
+}
+
+static int copy_field_in(lesgpu_ctx* ctx, void* dst, const double* src) {
+    DevCtx& d = ctx->d;
+    if (d.esz == 8) {
+        CK(cudaMemcpyAsync(dst, src, d.n * 8, cudaMemcpyHostToDevice, d.stream));
+        CK(cudaStreamSynchronize(d.stream));
+        return LESGPU_OK;
+    }
+    std::vector<float> tmp(d.n);
+    for (size_t q = 0; q < d.n; q++) tmp[q] = (float)src[q];
+    CK(cudaMemcpyAsync(dst, tmp.data(), d.n * 4, cudaMemcpyHostToDevice, d.stream));
+    CK(cudaStreamSynchronize(d.stream));
+    return LESGPU_OK;
+}
+
+static int copy_field_out(lesgpu_ctx* ctx, double* dst, const void* src) {
+    DevCtx& d = ctx->d;
+    if (d.esz == 8) {
+        CK(cudaMemcpyAsync(dst, src, d.n * 8, cudaMemcpyDeviceToHost, d.stream));
+        CK(cudaStreamSynchronize(d.stream));
+        return LESGPU_OK;
+    }
+    std::vector<float> tmp(d.n);
+    CK(cudaMemcpyAsync(tmp.data(), src, d.n * 4, cudaMemcpyDeviceToHost, d.stream));
+    CK(cudaStreamSynchronize(d.stream));
+    for (size_t q = 0; q < d.n; q++) dst[q] = (double)tmp[q];
+    return LESGPU_OK;
+}
+
+int lesgpu_upload_state(lesgpu_ctx* ctx, const double* const* fields, int nfields) {
+    if (!ctx || !fields || nfields < 1 || nfields > LESGPU_NSTATE) return LESGPU_EINVAL;
+    if (!ctx->d.have_attr) return fail(ctx, LESGPU_ESTATE, "upload the attribute map before the state");
+    for (int q = 0; q < nfields; q++) {
+        if (!fields[q]) return LESGPU_EINVAL;
+        int r = copy_field_in(ctx, ctx->d.S[q], fields[q]);
+        if (r) return r;
+    }
+    DevCtx& d = ctx->d;
+    // dt inputs as after start-up or a restart: nu and alpha are not part of the state
+    // (never restored by the reference), so their maxima start at zero (:4401-4408).
+    les::Scalars z{};
+    CK(cudaMemcpyAsync(d.dS, &z, sizeof(z), cudaMemcpyHostToDevice, d.stream));
+    cudaError_t e = (d.precision == LESGPU_FP64) ? les::umax_f64(d) : les::umax_f32(d);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "umax");
+    CK(cudaStreamSynchronize(d.stream));
+    d.have_state = (nfields == LESGPU_NSTATE) || d.have_state;
+    return LESGPU_OK;
+}
+
+int lesgpu_download_state(lesgpu_ctx* ctx, double* const* fields, int nfields) {
+    if (!ctx || !fields || nfields < 1 || nfields > LESGPU_NSTATE) return LESGPU_EINVAL;
+    for (int q = 0; q < nfields; q++) {
+        if (!fields[q]) return LESGPU_EINVAL;
+        int r = copy_field_out(ctx, fields[q], ctx->d.S[q]);
+        if (r) return r;
+    }
+    return LESGPU_OK;
+}
+
+static int ensure_debug(lesgpu_ctx* ctx) {
+    DevCtx& d = ctx->d;
+    if (d.dbg_cp) return LESGPU_OK;
+    size_t bytes = d.n * d.esz;
+    CK(cudaMalloc(&d.dbg_cp, bytes));
+    CK(cudaMalloc(&d.dbg_lam, bytes));
+    CK(cudaMalloc(&d.dbg_alpha, bytes));
+    for (int q = 0; q < les::NACC; q++) CK(cudaMalloc(&d.kd[q], bytes));
+    CK(cudaMemsetAsync(d.dbg_cp, 0, bytes, d.stream));
+    CK(cudaMemsetAsync(d.dbg_lam, 0, bytes, d.stream));
+    CK(cudaMemsetAsync(d.dbg_alpha, 0, bytes, d.stream));
+    for (int q = 0; q < les::NACC; q++) CK(cudaMemsetAsync(d.kd[q], 0, bytes, d.stream));
+    d.total_bytes += 13 * bytes;
+    return LESGPU_OK;
+}
+
+int lesgpu_set_debug(lesgpu_ctx* ctx, int enable) {
+    if (!ctx) return LESGPU_EINVAL;
+    if (enable) {
+        int r = ensure_debug(ctx);
+        if (r) return r;
+    }
+    ctx->d.debug = enable != 0;
+    return LESGPU_OK;
+}
+
+int lesgpu_get_field(lesgpu_ctx* ctx, int id, double* out) {
+    if (!ctx || !out) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    const void* src = nullptr;
+    if (id >= LESGPU_F_U && id <= LESGPU_F_Y4) src = d.S[id];
+    else if (id == LESGPU_F_NU_T) src = d.nu_t;
+    else if (id == LESGPU_F_S_MAG) src = d.S_mag;
+    else if (id >= LESGPU_F_U_F && id <= LESGPU_F_Y4_F) src = d.F[id - LESGPU_F_U_F];
+    else if (id == LESGPU_F_NU) src = d.nu;
+    else if (id == LESGPU_F_MU_MIX) src = d.mu_mix;
+    else if (id == LESGPU_F_ST) src = d.ST;
+    else if (id >= LESGPU_F_D0 && id <= LESGPU_F_D4) src = d.D[id - LESGPU_F_D0];
+    else if (id == LESGPU_F_CP || id == LESGPU_F_LAMBDA || id == LESGPU_F_ALPHA ||
+             (id >= LESGPU_F_K_RHOU && id <= LESGPU_F_K_Y4)) {
+        if (!d.debug) return fail(ctx, LESGPU_ESTATE, "enable lesgpu_set_debug before the step to read this field");
+        if (id == LESGPU_F_CP) src = d.dbg_cp;
+        else if (id == LESGPU_F_LAMBDA) src = d.dbg_lam;
+        else if (id == LESGPU_F_ALPHA) src = d.dbg_alpha;
+        else src = d.kd[id - LESGPU_F_K_RHOU];
+    } else {
+        return fail(ctx, LESGPU_EINVAL, "unknown field id");
+    }
+    return copy_field_out(ctx, out, src);
+}
+
+int lesgpu_dt_inputs(lesgpu_ctx* ctx, double* umax, double* numax, double* alphamax) {
+    if (!ctx || !umax || !numax || !alphamax) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    if (!d.have_state) return fail(ctx, LESGPU_ESTATE, "no state uploaded");
+    les::Scalars h;
+    CK(cudaMemcpyAsync(&h, d.dS, sizeof(h), cudaMemcpyDeviceToHost, d.stream));
+    CK(cudaStreamSynchronize(d.stream));
+    *umax = h.umax > 1e-10 ? h.umax : ctx->cfg.inlet_velocity;   // :1484
+    *numax = h.numax;
+    *alphamax = h.alphamax;
+    return LESGPU_OK;
+}
+
+int lesgpu_set_inflow(lesgpu_ctx* ctx, const double* vortices, int nv, const double* noise) {
+    if (!ctx || nv < 0 || (nv > 0 && !vortices)) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    if (!d.have_attr) return fail(ctx, LESGPU_ESTATE, "upload the attribute map first");
+    if (nv > d.nv_cap) {
+        double* nb = nullptr;
+        CK(cudaStreamSynchronize(d.stream));
+        CK(cudaMalloc(&nb, (size_t)nv * 7 * sizeof(double)));
+        cudaFree(d.vort);
+        d.vort = nb;
+        d.nv_cap = nv;
+    }
+    d.nv = nv;
+    if (nv > 0) CK(cudaMemcpyAsync(d.vort, vortices, (size_t)nv * 7 * sizeof(double), cudaMemcpyHostToDevice, d.stream));
+    if (d.n_inlet > 0) {
+        if (!noise) return LESGPU_EINVAL;
+        if (d.h_pinned == nullptr) return fail(ctx, LESGPU_ENOMEM, "pinned staging buffer unavailable");
+        // pack r1, r2, r3 of the inlet cells (the only cells the inflow condition reads);
+        // the pinned buffer is reused, so wait for the previous upload to finish first
+        CK(cudaStreamSynchronize(d.stream));
+        const size_t planes = (size_t)d.ny * d.nz;
+        for (int q = 0; q < d.n_inlet; q++) {
+            size_t p = (size_t)d.h_inlet[q];
+            d.h_pinned[3 * q + 0] = noise[p];
+            d.h_pinned[3 * q + 1] = noise[planes + p];
+            d.h_pinned[3 * q + 2] = noise[2 * planes + p];
+        }
+        CK(cudaMemcpyAsync(d.noise, d.h_pinned, 3 * (size_t)d.n_inlet * sizeof(double), cudaMemcpyHostToDevice,
+                           d.stream));
+    }
+    d.have_inflow = true;
+    return LESGPU_OK;
+}
+
+int lesgpu_step(lesgpu_ctx* ctx, double dt, int t_loop) {
+    if (!ctx) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    if (!d.have_state || !d.have_attr) return fail(ctx, LESGPU_ESTATE, "state and attribute map must be uploaded");
+    if (d.n_inlet > 0 && !d.have_inflow) return fail(ctx, LESGPU_ESTATE, "lesgpu_set_inflow must precede each step");
+    if (!(dt > 0.0) || !isfinite(dt)) return fail(ctx, LESGPU_EINVAL, "dt must be positive and finite");
+    cudaError_t e = (d.precision == LESGPU_FP64) ? les::step_f64(d, dt, t_loop) : les::step_f32(d, dt, t_loop);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "step");
+    d.have_inflow = false;
+    return LESGPU_OK;
+}
+
+int lesgpu_eval_rhs(lesgpu_ctx* ctx, int t_loop) {
+    if (!ctx) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    if (!d.have_state || !d.have_attr) return fail(ctx, LESGPU_ESTATE, "state and attribute map must be uploaded");
+    int r = lesgpu_set_debug(ctx, 1);
+    if (r) return r;
+    cudaError_t e = (d.precision == LESGPU_FP64) ? les::rhs_only_f64(d, t_loop) : les::rhs_only_f32(d, t_loop);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "eval_rhs");
+    CK(cudaStreamSynchronize(d.stream));
+    return LESGPU_OK;
+}
+
+int lesgpu_probe_lines(lesgpu_ctx* ctx, const int* i_stations, int n, int k_line, double* out) {
+    if (!ctx || n < 0 || (n > 0 && (!i_stations || !out))) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    if (n == 0) return LESGPU_OK;
+    if (k_line < 0 || k_line >= d.nz) return fail(ctx, LESGPU_EINVAL, "k_line out of range");
+    for (int q = 0; q < n; q++)
+        if (i_stations[q] < 0 || i_stations[q] >= d.nx) return fail(ctx, LESGPU_EINVAL, "station out of range");
+    if (n > d.probe_cap) {
+        CK(cudaStreamSynchronize(d.stream));
+        if (d.probe_st) cudaFree(d.probe_st);
+        if (d.probe_out) cudaFree(d.probe_out);
+        d.probe_st = nullptr;
+        d.probe_out = nullptr;
+        CK(cudaMalloc(&d.probe_st, n * sizeof(int)));
+        CK(cudaMalloc(&d.probe_out, (size_t)n * d.ny * 6 * sizeof(double)));
+        d.probe_cap = n;
+    }
+    CK(cudaMemcpyAsync(d.probe_st, i_stations, n * sizeof(int), cudaMemcpyHostToDevice, d.stream));
+    cudaError_t e = (d.precision == LESGPU_FP64) ? les::probe_f64(d, n, k_line) : les::probe_f32(d, n, k_line);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "probe");
+    CK(cudaMemcpyAsync(out, d.probe_out, (size_t)n * d.ny * 6 * sizeof(double), cudaMemcpyDeviceToHost, d.stream));
+    CK(cudaStreamSynchronize(d.stream));
+    return LESGPU_OK;
+}
+
+int lesgpu_monitor(lesgpu_ctx* ctx, double out[6]) {
+    if (!ctx || !out) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    cudaError_t e = (d.precision == LESGPU_FP64) ? les::monitor_f64(d) : les::monitor_f32(d);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "monitor");
+    les::Scalars h;
+    CK(cudaMemcpyAsync(&h, d.dS, sizeof(h), cudaMemcpyDeviceToHost, d.stream));
+    CK(cudaStreamSynchronize(d.stream));
+    for (int q = 0; q < 6; q++) out[q] = h.mon[q];
+    return LESGPU_OK;
+}
+
+int lesgpu_check_finite(lesgpu_ctx* ctx, int field_id) {
+    if (!ctx || field_id < 0 || field_id > LESGPU_F_NU_T) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    cudaError_t e = (d.precision == LESGPU_FP64) ? les::check_f64(d, field_id) : les::check_f32(d, field_id);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "check_finite");
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, d.flag, sizeof(int), cudaMemcpyDeviceToHost, d.stream));
+    CK(cudaStreamSynchronize(d.stream));
+    if (h) return fail(ctx, LESGPU_ENONFINITE, "non-finite value found");
+    return LESGPU_OK;
+}
+
+int lesgpu_sync(lesgpu_ctx* ctx) {
+    if (!ctx) return LESGPU_EINVAL;
+    CK(cudaStreamSynchronize(ctx->d.stream));
+    return LESGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,137 @@
+// les_common.cuh -- shared device-side definitions for the solver-step kernels.
+//
+// Field layout: structure of arrays, one contiguous array of NX*NY*NZ values per field in
+// the reference's [i][j][k] order (k fastest; les_combustion_solver.c:286), so host
+// uploads/downloads are plain copies and a warp reads 32 consecutive k-cells.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace les {
+
+constexpr int NSP = 5;
+constexpr int C3H8 = 0, O2 = 1, N2 = 2, CO2 = 3, H2O = 4;   // :129-133
+constexpr int NSTATE = 11;                                  // u v w T G rho Y0..Y4
+constexpr int NACC = 10;                                    // rhou rhov rhow T G Y0..Y4
+// thread-block shape of the per-cell passes: 32 consecutive k-cells x 8 j-rows
+constexpr int BX = 32, BY = 8, NT = BX * BY;
+
+// Fixed constants of the reference (les_combustion_solver.c:136-188, 2164-2166, 234-245).
+constexpr double R_UNIV = 8.314462;
+constexpr double PATM = 101325.0;
+constexpr double P_CONST = 101325.0;
+constexpr double G_GRAVITY = -9.81;
+constexpr double SMALL = 1e-10;
+constexpr double FILTER_W = 50.0;
+constexpr double TENO_CUT = 1.0e-6;
+constexpr double FORCE_LIMIT = 500.0;
+constexpr double RAMP_DIST = 0.03;
+constexpr double SSR_A = 0.2340, SSR_B = 0.2187;
+
+// Per-context constants, resident in device memory and read through the L1/constant path
+// (every access is warp-uniform).  All derived values are computed on the host with the
+// same operations the reference applies to its macros, so they are bit-identical.
+struct Consts {
+    int nx, ny, nz, flame_accel;
+    int weno_step, dco_sym, n_inlet, pad0;
+    double dx, dy, dz;
+    double two_dx, two_dy, two_dz;      // 2.0*DX ...
+    double dxx, dyy, dzz;               // DX*DX ...
+    double dx4;                         // pow(DX, 4.0)
+    double inlet_center_z;              // LZ/2.0
+    double total_volume;                // serial sum of DX*DY*DZ over attr {1,2,3,5} (:2545)
+    // species (:292-305)
+    double mw[NSP], mwk[NSP];           // g/mol and mw/1000.0
+    double t_mid[NSP];
+    double nasa_high[NSP][7], nasa_low[NSP][7];
+    double eta[NSP][4], lam[NSP][4], dco[NSP][NSP][4];
+    int eta_zero[NSP], lam_zero[NSP], dco_zero[NSP][NSP];
+    double wpow[NSP][NSP];              // pow(M_j/M_i, 0.25)           [i][j]
+    double wden[NSP][NSP];              // sqrt(8.0)*sqrt(1.0 + M_i/M_j) [i][j]
+    // model (:257-262, :2834, :2700-2704)
+    double cs_u, cs_b, cs_boost;
+    double accel_strength, accel_center, two_w2;   // two_w2 = 2.0*W*W
+    double relax;
+    double s_l, nu_u, d3;
+    double ssr_cdF;                     // 10.0 * (nu_u / (S_L + 1e-10))
+    double tau_sl;                      // tau * S_L
+    double sc_t2, pr_t2;                // 2.0*Sc_t, 2.0*Pr_t
+    double t_in, t_amb, t_burnt_span;   // T_u, T_amb, T_b - T_u
+    double inletYk[NSP], ambientYk[NSP];
+    double cons_o2, prod_co2, prod_h2o; // inletYk[C3H8] * stoich
+    double u_in, noise_amp;             // INLET_VELOCITY, 0.10*INLET_VELOCITY
+    double ti_rms;                      // INLET_VELOCITY * INLET_TURBULENCE_INTENSITY
+};
+
+// Reduction results written by the kernels' last-block epilogues.
+struct Scalars {
+    double rho_avg;                     // <rho_f> of the current stage (:2550)
+    double umax, numax, alphamax;       // dt inputs (:1472-1485, :4401-4408)
+    double mon[6];                      // monitor reductions
+    double sem[6];                      // SEM sums (debug)
+    unsigned int counter[4];            // last-block counters (0: filter, 1: bc, 2: aux)
+    int nonfinite;
+};
+
+__device__ __forceinline__ size_t cid(int i, int j, int k, int ny, int nz) {
+    return ((size_t)i * (size_t)ny + (size_t)j) * (size_t)nz + (size_t)k;
+}
+
+// x^3 and x^4 rounded once: glibc pow() returns the correctly rounded power for these
+// arguments, while a plain product rounds twice.  The exact square is split with fma,
+// the rest is carried as a double-double and rounded once at the end.
+__device__ __forceinline__ double pow3_rn(double x) {
+    double p = x * x;
+    double e = fma(x, x, -p);
+    double h = p * x;
+    double l = fma(p, x, -h);
+    l = fma(e, x, l);
+    return h + l;
+}
+__device__ __forceinline__ double pow4_rn(double x) {
+    double p = x * x;
+    double e = fma(x, x, -p);
+    double h = p * p;
+    double l = fma(p, p, -h);
+    l = fma(2.0 * p, e, l);
+    return h + l;
+}
+__device__ __forceinline__ float pow3_rn(float x) { return x * x * x; }
+__device__ __forceinline__ float pow4_rn(float x) { float p = x * x; return p * p; }
+
+// Deterministic block reductions (fixed shuffle tree, fixed warp order).
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double* sh, int tid) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = tid & 31, wid = tid >> 5;
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (wid == 0) {
+        r = (lane < NT / 32) ? sh[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+    }
+    __syncthreads();
+    return r;   // valid in thread 0
+}
+template <int NT>
+__device__ __forceinline__ double block_max(double v, double* sh, int tid) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    const int lane = tid & 31, wid = tid >> 5;
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    double r = -1.0e300;
+    if (wid == 0) {
+        r = (lane < NT / 32) ? sh[lane] : -1.0e300;
+        for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_down_sync(0xffffffffu, r, o));
+    }
+    __syncthreads();
+    return r;
+}
+template <int NT>
+__device__ __forceinline__ double block_min(double v, double* sh, int tid) {
+    return -block_max<NT>(-v, sh, tid);
+}
+
+}  // namespace les

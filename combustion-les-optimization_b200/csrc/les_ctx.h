@@ -1,0 +1,79 @@
+// les_ctx.h -- device context shared by the C-ABI layer and the per-precision launchers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+
+#include "les_common.cuh"
+
+namespace les {
+
+struct DevCtx {
+    int nx = 0, ny = 0, nz = 0, precision = 0;
+    size_t n = 0;                       // cells
+    size_t esz = 8;                     // bytes per field value
+    Consts hC{};                        // host copy of the constants
+    Consts* dC = nullptr;
+    Scalars* dS = nullptr;
+    uint8_t* attr = nullptr;
+    void* S[NSTATE] = {};               // state Phi_n (updated in place by the final combine)
+    void* St[NSTATE] = {};              // stage state (u_temp, ..., rho_temp)
+    void* F[NSTATE] = {};               // filtered stage fields
+    void* mu_mix = nullptr;
+    void* nu = nullptr;
+    void* D[NSP] = {};
+    void* aT = nullptr;
+    void* nu_t = nullptr;
+    void* S_mag = nullptr;
+    void* ST = nullptr;
+    void* mu_eff = nullptr;
+    void* acc[NACC] = {};
+    void* dbg_cp = nullptr;             // optional inspection buffers (lesgpu_get_field)
+    void* dbg_lam = nullptr;
+    void* dbg_alpha = nullptr;
+    void* kd[NACC] = {};
+    bool debug = false;
+    double* part = nullptr;             // per-block partials of the reductions
+    size_t part_len = 0;
+    double* plane = nullptr;            // SEM fluctuation planes, 3 x NY x NZ
+    double* noise = nullptr;            // packed white noise, 3 per inlet cell
+    double* vort = nullptr;             // vortices, 7 doubles each
+    int nv_cap = 0;
+    int nv = 0;
+    int* inlet_list = nullptr;          // plane index j*NZ+k of inlet cells, (j,k) order
+    int* inlet_pos = nullptr;           // plane index -> position in inlet_list (or -1)
+    int n_inlet = 0;
+    std::vector<int> h_inlet;           // host copy of inlet_list
+    int* probe_st = nullptr;
+    double* probe_out = nullptr;
+    int probe_cap = 0;
+    int* flag = nullptr;
+    void* arena = nullptr;              // one allocation backing all fields
+    size_t arena_bytes = 0;
+    size_t total_bytes = 0;
+    cudaStream_t stream = nullptr;
+    double* h_pinned = nullptr;         // pinned staging for small transfers
+    size_t h_pinned_len = 0;
+    bool have_attr = false, have_state = false, have_inflow = false;
+    std::string err;
+};
+
+// Per-precision entry points (les_f64.cu / les_f32.cu).
+cudaError_t sem_inflow(DevCtx& c);
+cudaError_t step_f64(DevCtx& c, double dt, int t_loop);
+cudaError_t umax_f64(DevCtx& c);
+cudaError_t monitor_f64(DevCtx& c);
+cudaError_t probe_f64(DevCtx& c, int n, int kline);
+cudaError_t check_f64(DevCtx& c, int field);
+cudaError_t rhs_only_f64(DevCtx& c, int t_loop);
+cudaError_t step_f32(DevCtx& c, double dt, int t_loop);
+cudaError_t rhs_only_f32(DevCtx& c, int t_loop);
+cudaError_t umax_f32(DevCtx& c);
+cudaError_t monitor_f32(DevCtx& c);
+cudaError_t probe_f32(DevCtx& c, int n, int kline);
+cudaError_t check_f32(DevCtx& c, int field);
+
+}  // namespace les

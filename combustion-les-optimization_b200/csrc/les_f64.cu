@@ -1,0 +1,28 @@
+// les_f64.cu -- plain FP64 form of the solver step.
+//
+// Built with -fmad=false: every multiply and add is rounded separately, as in the
+// reference (built for baseline x86-64, which has no FMA), so that apart from the libm
+// transcendentals and the order of the <rho_f> sum the kernels perform the reference's
+// floating-point operations one for one.
+#include "les_launch.cuh"
+#include "les_sem.cuh"
+
+namespace les {
+
+cudaError_t sem_inflow(DevCtx& c) {
+    if (c.n_inlet <= 0) return cudaSuccess;
+    const int tpb = 128;
+    k_sem_plane<<<(c.n_inlet + tpb - 1) / tpb, tpb, 7 * 512 * sizeof(double), c.stream>>>(c.dC, c.inlet_list, c.n_inlet,
+                                                                                         c.vort, c.nv, c.plane);
+    k_sem_normalize<<<1, 256, 0, c.stream>>>(c.dC, c.inlet_list, c.n_inlet, c.plane, c.dS);
+    return cudaGetLastError();
+}
+
+cudaError_t step_f64(DevCtx& c, double dt, int t_loop) { return step_impl<double>(c, dt, t_loop); }
+cudaError_t rhs_only_f64(DevCtx& c, int t_loop) { return rhs_only_impl<double>(c, t_loop); }
+cudaError_t umax_f64(DevCtx& c) { return umax_impl<double>(c); }
+cudaError_t monitor_f64(DevCtx& c) { return monitor_impl<double>(c); }
+cudaError_t probe_f64(DevCtx& c, int n, int kline) { return probe_impl<double>(c, n, kline); }
+cudaError_t check_f64(DevCtx& c, int field) { return check_impl<double>(c, field); }
+
+}  // namespace les

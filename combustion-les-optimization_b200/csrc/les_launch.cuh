@@ -1,0 +1,122 @@
+// les_launch.cuh -- stream-ordered launch sequence of one solver step, templated on the
+// field type.  Included once per precision translation unit.
+#pragma once
+
+#include "les_ctx.h"
+#include "les_kernels.cuh"
+
+namespace les {
+
+template <typename R>
+static F11<R> f11(void* const* p) {
+    F11<R> f;
+    for (int q = 0; q < NSTATE; q++) f.p[q] = (R*)p[q];
+    return f;
+}
+
+template <typename R>
+static PropBuf<R> props(const DevCtx& c) {
+    PropBuf<R> P;
+    P.mu_mix = (R*)c.mu_mix;
+    P.nu = (R*)c.nu;
+    for (int s = 0; s < NSP; s++) P.D[s] = (R*)c.D[s];
+    P.aT = (R*)c.aT;
+    P.nu_t = (R*)c.nu_t;
+    P.S_mag = (R*)c.S_mag;
+    P.ST = (R*)c.ST;
+    P.mu_eff = (R*)c.mu_eff;
+    P.dbg_cp = c.debug ? (R*)c.dbg_cp : nullptr;
+    P.dbg_lam = c.debug ? (R*)c.dbg_lam : nullptr;
+    P.dbg_alpha = c.debug ? (R*)c.dbg_alpha : nullptr;
+    return P;
+}
+
+static inline dim3 cell_grid(const DevCtx& c) {
+    return dim3((unsigned)((c.nz + BX - 1) / BX), (unsigned)((c.ny + BY - 1) / BY), (unsigned)c.nx);
+}
+
+template <typename R>
+cudaError_t step_impl(DevCtx& c, double dt, int t_loop) {
+    cudaStream_t st = c.stream;
+    const dim3 g = cell_grid(c), b(BX, BY);
+    F11<R> S = f11<R>(c.S), St = f11<R>(c.St), F = f11<R>(c.F);
+    PropBuf<R> P = props<R>(c);
+    AccBuf<R> acc;
+    for (int q = 0; q < NACC; q++) acc.p[q] = (R*)c.acc[q];
+    KDbg<R> kd;
+    for (int q = 0; q < NACC; q++) kd.p[q] = c.debug ? (R*)c.kd[q] : nullptr;
+    KDbg<R> knone;
+    for (int q = 0; q < NACC; q++) knone.p[q] = nullptr;
+
+    // SEM inflow plane (:943-1075)
+    sem_inflow(c);
+    // four RK4 stages (:4428-4544)
+    for (int s = 0; s < 4; s++) {
+        F11<R> in = (s == 0) ? S : St;
+        k_filter_props<R><<<g, b, 0, st>>>(c.dC, c.attr, in, F, P, c.part, c.dS, s == 3 ? 1 : 0);
+        k_strain<R><<<g, b, 0, st>>>(c.dC, c.attr, F, P);
+        // the k-arrays of the first stage are kept for inspection when requested
+        k_rhs_combine<R><<<g, b, 0, st>>>(c.dC, c.attr, F, P, S, St, acc, s == 0 ? kd : knone, c.dS, dt, s, t_loop);
+    }
+    // apply_boundary_conditions (:2967-3161)
+    {
+        const int tpb = 128;
+        k_bc_iface<R><<<dim3((c.nz + tpb - 1) / tpb, c.ny), tpb, 0, st>>>(c.dC, c.attr, S, c.plane, c.noise,
+                                                                            c.inlet_pos);
+        if (c.nx > 2) {
+            k_bc_jface<R><<<dim3((c.nz + tpb - 1) / tpb, c.nx - 2), tpb, 0, st>>>(c.dC, c.attr, S);
+            k_bc_kface<R><<<dim3((c.ny + tpb - 1) / tpb, c.nx - 2), tpb, 0, st>>>(c.dC, c.attr, S);
+        }
+        k_bc_eos<R><<<g, b, 0, st>>>(c.dC, c.attr, S, c.part, c.dS);
+    }
+    return cudaGetLastError();
+}
+
+// Stage-1 right-hand side at the current state with the inspection buffers filled; the
+// state itself is not advanced (dt = 0 leaves the stage state equal to Phi_n).
+template <typename R>
+cudaError_t rhs_only_impl(DevCtx& c, int t_loop) {
+    cudaStream_t st = c.stream;
+    const dim3 g = cell_grid(c), b(BX, BY);
+    F11<R> S = f11<R>(c.S), St = f11<R>(c.St), F = f11<R>(c.F);
+    PropBuf<R> P = props<R>(c);
+    AccBuf<R> acc;
+    for (int q = 0; q < NACC; q++) acc.p[q] = (R*)c.acc[q];
+    KDbg<R> kd;
+    for (int q = 0; q < NACC; q++) kd.p[q] = (R*)c.kd[q];
+    k_filter_props<R><<<g, b, 0, st>>>(c.dC, c.attr, S, F, P, c.part, c.dS, 1);
+    k_strain<R><<<g, b, 0, st>>>(c.dC, c.attr, F, P);
+    k_rhs_combine<R><<<g, b, 0, st>>>(c.dC, c.attr, F, P, S, St, acc, kd, c.dS, 0.0, 0, t_loop);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t umax_impl(DevCtx& c) {
+    k_umax<R><<<cell_grid(c), dim3(BX, BY), 0, c.stream>>>(c.dC, c.attr, f11<R>(c.S), c.part, c.dS);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t monitor_impl(DevCtx& c) {
+    const int nb = 592;   // 4 x 148 SMs
+    k_monitor<R><<<nb, NT, 0, c.stream>>>(c.dC, f11<R>(c.S), c.part, c.dS, c.n);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t probe_impl(DevCtx& c, int n, int kline) {
+    const int tpb = 64;
+    k_probe<R><<<dim3((c.ny + tpb - 1) / tpb, n), tpb, 0, c.stream>>>(c.dC, f11<R>(c.S), props<R>(c), c.probe_st, n,
+                                                                      kline, c.probe_out);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t check_impl(DevCtx& c, int field) {
+    cudaMemsetAsync(c.flag, 0, sizeof(int), c.stream);
+    const R* x = (field < NSTATE) ? (const R*)c.S[field] : (const R*)c.nu_t;
+    k_check_finite<R><<<592, 256, 0, c.stream>>>(x, c.n, c.flag);
+    return cudaGetLastError();
+}
+
+}  // namespace les

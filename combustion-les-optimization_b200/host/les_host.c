@@ -1,0 +1,517 @@
+/*
+ * les_host.c -- C host driver of the GPU solver step (include/les_solver.h).
+ *
+ * Mirrors the host side of the reference's main() (les_combustion_solver.c:4016-4632):
+ * start-up state, the glibc rand() stream that drives the SEM vortex recycling and the
+ * inflow white noise, the dt formula, and the probe / monitor / checkpoint files.  All
+ * floating-point expressions keep the reference's operation order (built with
+ * -ffp-contract=off) so the host-side numbers are bit-identical to the reference's.
+ */
+#include "les_solver.h"
+
+#include <errno.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ------------------------------------------------------------------ glibc rand() */
+/* srand()/rand() of glibc are random_r's TYPE_3 additive feedback generator: 31 words
+ * seeded by the Park-Miller LCG (16807 mod 2^31-1, Schrage's method), the recurrence
+ * x[i] = x[i-31] + x[i-3] (mod 2^32), 310 discarded outputs, and x[i] >> 1 returned.
+ * Restated here with a private state per solver instead of the process-wide one. */
+
+void les_rng_seed(les_rng* g, unsigned int seed) {
+    if (seed == 0) seed = 1;
+    g->r[0] = (int)seed;
+    int word = (int)seed;   /* the seed word is a signed 32-bit value */
+    for (int i = 1; i < 31; i++) {
+        long long hi = word / 127773;
+        long long lo = word % 127773;
+        long long nw = 16807 * lo - 2836 * hi;
+        if (nw < 0) nw += 2147483647;
+        word = (int)nw;
+        g->r[i] = word;
+    }
+    g->f = 3;     /* front tap: x[i-3] lives at (i-3) mod 31 */
+    g->b = 0;     /* back tap:  x[i-31] lives at i mod 31 */
+    g->n = 0;
+    for (int i = 0; i < 310; i++) (void)les_rng_next(g);
+    g->n = 0;
+}
+
+int les_rng_next(les_rng* g) {
+    unsigned int v = (unsigned int)g->r[g->f] + (unsigned int)g->r[g->b];
+    g->r[g->f] = (int)v;
+    if (++g->f >= 31) g->f = 0;
+    if (++g->b >= 31) g->b = 0;
+    g->n++;
+    return (int)(v >> 1);
+}
+
+static double rng01(les_rng* g) { return (double)les_rng_next(g) / (double)LES_RAND_MAX; }
+
+/* ------------------------------------------------------------------ solver object */
+
+struct les_solver {
+    lesgpu_config cfg;
+    lesgpu_species sp;
+    lesgpu_ctx* ctx;
+    les_rng rng;
+    int nx, ny, nz;
+    size_t n;
+    double dx, dy, dz;
+    int* attr;
+    double* vort;         /* nv x 7 */
+    double* noise;        /* 3 x NY x NZ */
+    double inletYk[LESGPU_NSP], ambientYk[LESGPU_NSP];
+    double stoich_o2, stoich_co2, stoich_h2o;
+    int t_loop;
+    double dt, umax;
+    char out_dir[1024];
+    int out_flags;
+    int probe_i[7];
+    double* probe_buf;
+    char err[256];
+};
+
+static int serr(les_solver* s, int code, const char* msg) {
+    if (s) snprintf(s->err, sizeof(s->err), "%s", msg);
+    return code;
+}
+
+static const double PROBE_X[7] = {0.010, 0.015, 0.020, 0.025, 0.030, 0.035, 0.040};   /* :274 */
+
+/* initialize_vortices (:861-897): three discarded test draws, then 7 draws per vortex. */
+void les_vortices_init(les_rng* g, const lesgpu_config* c, double* vort) {
+    (void)les_rng_next(g);
+    (void)les_rng_next(g);
+    (void)les_rng_next(g);
+    double u_rms = c->inlet_velocity * c->turbulence_intensity;
+    for (int i = 0; i < c->num_vortices; i++) {
+        double r1 = rng01(g), r2 = rng01(g), r3 = rng01(g), r4 = rng01(g);
+        double r5 = rng01(g), r6 = rng01(g), r7 = rng01(g);
+        double* v = vort + 7 * (size_t)i;
+        v[0] = (r1 - 0.5) * c->length_scale;
+        v[1] = r2 * c->ly;
+        v[2] = r3 * c->lz;
+        double min_r = c->length_scale * 0.5, max_r = c->length_scale * 1.5;
+        v[3] = min_r + (max_r - min_r) * r4;
+        v[4] = (r5 * 2.0 - 1.0) * u_rms;
+        v[5] = (r6 * 2.0 - 1.0) * u_rms;
+        v[6] = (r7 * 2.0 - 1.0) * u_rms;
+    }
+}
+
+/* update_vortices (:900-939): advect at U, recycle with 6 draws each in index order. */
+void les_vortices_update(les_rng* g, const lesgpu_config* c, double* vort, double dt) {
+    double u_rms = c->inlet_velocity * c->turbulence_intensity;
+    double box_x = c->length_scale;
+    for (int i = 0; i < c->num_vortices; i++) {
+        double* v = vort + 7 * (size_t)i;
+        v[0] += c->inlet_velocity * dt;
+        if (v[0] > box_x / 2.0) {
+            v[0] -= box_x;
+            double ry = rng01(g), rz = rng01(g);
+            v[1] = ry * c->ly;
+            v[2] = rz * c->lz;
+            double ru = rng01(g), rv = rng01(g), rw = rng01(g);
+            v[4] = (ru * 2.0 - 1.0) * u_rms;
+            v[5] = (rv * 2.0 - 1.0) * u_rms;
+            v[6] = (rw * 2.0 - 1.0) * u_rms;
+            double rr = rng01(g);
+            double min_r = c->length_scale * 0.5, max_r = c->length_scale * 1.5;
+            v[3] = min_r + (max_r - min_r) * rr;
+        }
+    }
+}
+
+/* The inflow white noise of apply_boundary_conditions (:2990-2992): three draws per inlet
+ * cell in (j, k) order, mapped to [-1, 1]; non-inlet entries are left untouched. */
+void les_inflow_noise(les_rng* g, const int* attr, int ny, int nz, double* noise) {
+    const size_t np = (size_t)ny * nz;
+    for (int j = 0; j < ny; j++)
+        for (int k = 0; k < nz; k++) {
+            size_t p = (size_t)j * nz + k;
+            if (attr[p] != 1) continue;
+            noise[p] = ((double)les_rng_next(g) / LES_RAND_MAX) * 2.0 - 1.0;
+            noise[np + p] = ((double)les_rng_next(g) / LES_RAND_MAX) * 2.0 - 1.0;
+            noise[2 * np + p] = ((double)les_rng_next(g) / LES_RAND_MAX) * 2.0 - 1.0;
+        }
+}
+
+double les_dt(const lesgpu_config* c, double umax, double numax, double alphamax) {
+    double dx = c->lx / (double)c->nx;
+    double dt_conv = c->courant * dx / (umax + 1e-10);
+    double dt_nu = c->courant_diffusion * (dx * dx) / (numax + 1e-10);
+    double dt_al = c->courant_diffusion * (dx * dx) / (alphamax + 1e-10);
+    return fmin(dt_conv, fmin(dt_nu, dt_al));
+}
+
+/* initialize() + setting() (:1085-1285): attribute map (symmetry code 5 on j = 0) and the
+ * initial burnt/unburnt state with rho from the equation of state. */
+int les_initial_state(const lesgpu_config* c, const lesgpu_species* sp, int* attr, double* const* f) {
+    if (!c || !sp || !attr || !f) return LESGPU_EINVAL;
+    const int nx = c->nx, ny = c->ny, nz = c->nz;
+    const double dy = c->ly / (double)ny, dz = c->lz / (double)nz;
+    /* inlet composition and stoichiometry (:4101-4120) */
+    double inletYk[LESGPU_NSP], ambientYk[LESGPU_NSP] = {0.0, 0.232, 0.768, 0.0, 0.0};
+    const double phi = c->equivalence_ratio;
+    double m_f = 1.0, m_o2 = 5.0 / phi, m_n2 = m_o2 * 3.76;
+    double mass_total = m_f * sp->mw[0] + m_o2 * sp->mw[1] + m_n2 * sp->mw[2];
+    inletYk[0] = (m_f * sp->mw[0]) / mass_total;
+    inletYk[1] = (m_o2 * sp->mw[1]) / mass_total;
+    inletYk[2] = (m_n2 * sp->mw[2]) / mass_total;
+    inletYk[3] = 0.0; inletYk[4] = 0.0;
+    const double st_o2 = (5.0 * sp->mw[1]) / sp->mw[0];
+    const double st_co2 = (3.0 * sp->mw[3]) / sp->mw[0];
+    const double st_h2o = (4.0 * sp->mw[4]) / sp->mw[0];
+    const double icy = 0.0, icz = c->lz / 2.0;
+#define CIDX(i, j, k) (((size_t)(i) * (size_t)ny + (size_t)(j)) * (size_t)nz + (size_t)(k))
+    for (int i = 0; i < nx; i++)
+        for (int j = 0; j < ny; j++)
+            for (int k = 0; k < nz; k++) {
+                int a;
+                if (i == 0) {
+                    double y = j * dy, z = k * dz;
+                    double d2 = pow(y - icy, 2) + pow(z - icz, 2);
+                    if (d2 <= pow(c->inlet_radius, 2)) a = 1;
+                    else if (d2 <= pow(c->rim_outer_radius, 2)) a = 6;
+                    else a = 4;
+                } else if (i == nx - 1) a = 2;
+                else if (j == 0) a = 5;
+                else if (j == ny - 1 || k == 0 || k == nz - 1) a = 4;
+                else a = 3;
+                attr[CIDX(i, j, k)] = a;
+            }
+    double *u = f[0], *v = f[1], *w = f[2], *T = f[3], *G = f[4], *rho = f[5];
+    double* const* Y = f + 6;
+    for (int i = 0; i < nx; i++)
+        for (int j = 0; j < ny; j++)
+            for (int k = 0; k < nz; k++) {
+                size_t id = CIDX(i, j, k);
+                u[id] = v[id] = w[id] = 0.0;
+                T[id] = 0.0; G[id] = 0.0;
+                for (int q = 0; q < LESGPU_NSP; q++) Y[q][id] = 0.0;
+                switch (attr[id]) {
+                    case 1:
+                        u[id] = c->inlet_velocity;
+                        T[id] = c->inlet_temperature;
+                        for (int q = 0; q < LESGPU_NSP; q++) Y[q][id] = inletYk[q];
+                        break;
+                    case 4:
+                    case 2:
+                        T[id] = c->ambient_temperature;
+                        for (int q = 0; q < LESGPU_NSP; q++) Y[q][id] = ambientYk[q];
+                        break;
+                    case 5:
+                    case 3:
+                        if (i <= c->initial_flame_front_i) {
+                            G[id] = 1.0;
+                            T[id] = c->burnt_gas_temperature;
+                            double cons = inletYk[0];
+                            Y[0][id] = inletYk[0] - cons;
+                            Y[1][id] = inletYk[1] - cons * st_o2;
+                            Y[2][id] = inletYk[2];
+                            Y[3][id] = inletYk[3] + cons * st_co2;
+                            Y[4][id] = inletYk[4] + cons * st_h2o;
+                        } else {
+                            T[id] = c->inlet_temperature;
+                            for (int q = 0; q < LESGPU_NSP; q++) Y[q][id] = inletYk[q];
+                        }
+                        break;
+                    default:
+                        break;
+                }
+                double syw = 0.0;
+                for (int q = 0; q < LESGPU_NSP; q++) syw += Y[q][id] / (sp->mw[q] / 1000.0);
+                if (syw > 1e-10 && T[id] > 1.0) {
+                    double W = 1.0 / syw;
+                    double Rm = 8.314462 / W;
+                    rho[id] = 101325.0 / (Rm * T[id]);
+                } else {
+                    rho[id] = 1.2;
+                }
+            }
+#undef CIDX
+    return LESGPU_OK;
+}
+
+static int alloc_fields(size_t n, double** f) {
+    for (int q = 0; q < LESGPU_NSTATE; q++) {
+        f[q] = (double*)malloc(n * sizeof(double));
+        if (!f[q]) {
+            for (int r = 0; r < q; r++) free(f[r]);
+            return -1;
+        }
+    }
+    return 0;
+}
+
+static void free_fields(double** f) {
+    for (int q = 0; q < LESGPU_NSTATE; q++) free(f[q]);
+}
+
+int les_solver_create(const lesgpu_config* cfg, const char* chem_path, const char* tran_path, int start_step,
+                      les_solver** out) {
+    if (!cfg || !chem_path || !tran_path || !out) return LESGPU_EINVAL;
+    *out = NULL;
+    les_solver* s = (les_solver*)calloc(1, sizeof(les_solver));
+    if (!s) return LESGPU_ENOMEM;
+    s->cfg = *cfg;
+    int rc = lesgpu_load_species(chem_path, tran_path, &s->sp);
+    if (rc) { free(s); return rc; }
+    s->nx = cfg->nx; s->ny = cfg->ny; s->nz = cfg->nz;
+    s->n = (size_t)s->nx * s->ny * s->nz;
+    s->dx = cfg->lx / (double)cfg->nx;
+    s->dy = cfg->ly / (double)cfg->ny;
+    s->dz = cfg->lz / (double)cfg->nz;
+    /* inlet composition and stoichiometry (:4101-4120) */
+    const double phi = cfg->equivalence_ratio;
+    double m_f = 1.0, m_o2 = 5.0 / phi, m_n2 = m_o2 * 3.76;
+    double mass_total = m_f * s->sp.mw[0] + m_o2 * s->sp.mw[1] + m_n2 * s->sp.mw[2];
+    s->inletYk[0] = (m_f * s->sp.mw[0]) / mass_total;
+    s->inletYk[1] = (m_o2 * s->sp.mw[1]) / mass_total;
+    s->inletYk[2] = (m_n2 * s->sp.mw[2]) / mass_total;
+    s->inletYk[3] = 0.0; s->inletYk[4] = 0.0;
+    s->ambientYk[0] = 0.0; s->ambientYk[1] = 0.232; s->ambientYk[2] = 0.768; s->ambientYk[3] = 0.0; s->ambientYk[4] = 0.0;
+    s->stoich_o2 = (5.0 * s->sp.mw[1]) / s->sp.mw[0];
+    s->stoich_co2 = (3.0 * s->sp.mw[3]) / s->sp.mw[0];
+    s->stoich_h2o = (4.0 * s->sp.mw[4]) / s->sp.mw[0];
+    s->attr = (int*)malloc(s->n * sizeof(int));
+    s->vort = (double*)calloc(cfg->num_vortices > 0 ? (size_t)cfg->num_vortices * 7 : 7, sizeof(double));
+    s->noise = (double*)calloc(3 * (size_t)s->ny * s->nz, sizeof(double));
+    s->probe_buf = (double*)malloc(7 * (size_t)s->ny * 6 * sizeof(double));
+    if (!s->attr || !s->vort || !s->noise || !s->probe_buf) {
+        les_solver_destroy(s);
+        return LESGPU_ENOMEM;
+    }
+    double* f[LESGPU_NSTATE];
+    if (alloc_fields(s->n, f)) { les_solver_destroy(s); return LESGPU_ENOMEM; }
+    les_initial_state(cfg, &s->sp, s->attr, f);
+    rc = lesgpu_create(cfg, &s->sp, &s->ctx);
+    if (rc == LESGPU_OK) rc = lesgpu_upload_attribute(s->ctx, s->attr);
+    if (rc == LESGPU_OK) rc = lesgpu_upload_state(s->ctx, (const double* const*)f, LESGPU_NSTATE);
+    free_fields(f);
+    if (rc) {
+        if (s->ctx) snprintf(s->err, sizeof(s->err), "%s", lesgpu_last_error(s->ctx));
+        les_solver_destroy(s);
+        return rc;
+    }
+    /* srand(seed) + initialize_vortices (:4085, :4360) and the inlet mask (:4366-4367) */
+    les_rng_seed(&s->rng, cfg->seed);
+    les_vortices_init(&s->rng, cfg, s->vort);
+    for (int q = 0; q < 7; q++) s->probe_i[q] = (int)(PROBE_X[q] / s->dx);
+    s->t_loop = start_step;
+    *out = s;
+    return LESGPU_OK;
+}
+
+void les_solver_destroy(les_solver* s) {
+    if (!s) return;
+    if (s->ctx) lesgpu_destroy(s->ctx);
+    free(s->attr); free(s->vort); free(s->noise); free(s->probe_buf);
+    free(s);
+}
+
+lesgpu_ctx* les_solver_ctx(les_solver* s) { return s ? s->ctx : NULL; }
+const char* les_solver_last_error(const les_solver* s) { return s ? s->err : "null solver"; }
+int les_solver_t_loop(const les_solver* s) { return s ? s->t_loop : -1; }
+double les_solver_last_dt(const les_solver* s) { return s ? s->dt : 0.0; }
+double les_solver_last_umax(const les_solver* s) { return s ? s->umax : 0.0; }
+unsigned long long les_solver_rng_draws(const les_solver* s) { return s ? s->rng.n : 0; }
+
+int les_solver_attribute(const les_solver* s, int* out) {
+    if (!s || !out) return LESGPU_EINVAL;
+    memcpy(out, s->attr, s->n * sizeof(int));
+    return LESGPU_OK;
+}
+
+int les_solver_vortices(const les_solver* s, double* out) {
+    if (!s || !out) return LESGPU_EINVAL;
+    memcpy(out, s->vort, (size_t)s->cfg.num_vortices * 7 * sizeof(double));
+    return s->cfg.num_vortices;
+}
+
+static void join_path(char* dst, size_t cap, const char* dir, const char* name) {
+    snprintf(dst, cap, "%s/%s", dir, name);
+}
+
+int les_solver_set_outputs(les_solver* s, const char* dir, int flags) {
+    if (!s || (flags && !dir)) return LESGPU_EINVAL;
+    s->out_flags = flags;
+    if (!dir) return LESGPU_OK;
+    snprintf(s->out_dir, sizeof(s->out_dir), "%s", dir);
+    if (flags & LES_OUT_PROBES) {
+        for (int n = 0; n < 7; n++) {
+            char name[128], path[1200];
+            snprintf(name, sizeof(name), "probe_data_flame_region_loc%d.csv", n);
+            join_path(path, sizeof(path), s->out_dir, name);
+            remove(path);
+            FILE* fp = fopen(path, "w");
+            if (!fp) return serr(s, LESGPU_EIO, "cannot create probe file");
+            fprintf(fp, "timestep,x_location,y_flame,y_physical,y_relative,u,v,w,G,nu_t,S_mag\n");
+            fclose(fp);
+        }
+    }
+    return LESGPU_OK;
+}
+
+/* record_flame_region_data (:3403-3471): the lower G = 0.5 crossing on the line k = NZ/2
+ * at each x-station, then every row within SAMPLING_RANGE (1.0 m, i.e. all rows). */
+static int write_probes(les_solver* s, int t_loop) {
+    int st[7], slot[7], m = 0;
+    for (int n = 0; n < 7; n++) {
+        int ip = s->probe_i[n];
+        if (ip <= 0 || ip >= s->nx - 1) continue;
+        st[m] = ip;
+        slot[m] = n;
+        m++;
+    }
+    if (m == 0) return LESGPU_OK;
+    const int kline = s->nz / 2;
+    int rc = lesgpu_probe_lines(s->ctx, st, m, kline, s->probe_buf);
+    if (rc) return rc;
+    for (int q = 0; q < m; q++) {
+        const double* row = s->probe_buf + (size_t)q * s->ny * 6;
+        double y_flame = -1.0;
+        for (int j = 0; j < s->ny - 1; j++) {
+            double G1 = row[6 * j + 3], G2 = row[6 * (j + 1) + 3];
+            if ((G1 - 0.5) * (G2 - 0.5) <= 0.0) {
+                double y1 = j * s->dy, y2 = (j + 1) * s->dy;
+                if (fabs(G2 - G1) < 1e-9) y_flame = y1;
+                else y_flame = y1 + (0.5 - G1) / (G2 - G1) * (y2 - y1);
+                break;
+            }
+        }
+        if (!(y_flame > 0.0)) continue;
+        char name[128], path[1200];
+        snprintf(name, sizeof(name), "probe_data_flame_region_loc%d.csv", slot[q]);
+        join_path(path, sizeof(path), s->out_dir, name);
+        FILE* fp = fopen(path, "a");
+        if (!fp) continue;
+        for (int j = 0; j < s->ny; j++) {
+            double yp = j * s->dy, yr = yp - y_flame;
+            if (fabs(yr) <= 1.000) {
+                const double* r = row + 6 * j;
+                fprintf(fp, "%d,%.3f,%.6f,%.6f,%.6f,%.6f,%.6f,%.6f,%.6f,%.6e,%.6e\n", t_loop, PROBE_X[slot[q]], y_flame, yp,
+                        yr, r[0], r[1], r[2], r[3], r[4], r[5]);
+            }
+        }
+        fclose(fp);
+    }
+    return LESGPU_OK;
+}
+
+/* write_monitor_log (:3874-3924), every 10 steps */
+static int write_monitor(les_solver* s, int step, double dt) {
+    if (step % 10 != 0) return LESGPU_OK;
+    double m[6];
+    int rc = lesgpu_monitor(s->ctx, m);
+    if (rc) return rc;
+    char path[1200];
+    join_path(path, sizeof(path), s->out_dir, "simulation_monitor.csv");
+    FILE* fp = fopen(path, "a");
+    if (!fp) return LESGPU_OK;
+    fseek(fp, 0, SEEK_END);
+    if (ftell(fp) == 0) fprintf(fp, "step,dt,total_mass,min_T,max_T,min_G,max_G,min_Y_C3H8\n");
+    fprintf(fp, "%d,%.6e,%.6e,%.2f,%.2f,%.4f,%.4f,%.2e\n", step, dt, m[0], m[1], m[2], m[3], m[4], m[5]);
+    fclose(fp);
+    return LESGPU_OK;
+}
+
+int les_solver_step(les_solver* s) {
+    if (!s) return LESGPU_EINVAL;
+    const lesgpu_config* c = &s->cfg;
+    /* dt (:4399-4411) */
+    double umax, numax, alphamax;
+    int rc = lesgpu_dt_inputs(s->ctx, &umax, &numax, &alphamax);
+    if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
+    double dt = les_dt(c, umax, numax, alphamax);
+    s->dt = dt;
+    s->umax = umax;
+    /* SEM vortices for this step, then the inflow noise drawn after the RK stages (:4414, :2990) */
+    les_vortices_update(&s->rng, c, s->vort, dt);
+    les_inflow_noise(&s->rng, s->attr, s->ny, s->nz, s->noise);
+    rc = lesgpu_set_inflow(s->ctx, s->vort, c->num_vortices, s->noise);
+    if (rc == LESGPU_OK) rc = lesgpu_step(s->ctx, dt, s->t_loop);
+    if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
+    if ((s->out_flags & LES_OUT_PROBES) && s->out_dir[0]) {
+        rc = write_probes(s, s->t_loop);
+        if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
+    }
+    if ((s->out_flags & LES_OUT_CHECKPOINT) && s->out_dir[0] && s->t_loop > 0 && s->t_loop % 50 == 0) {
+        char path[1200];
+        join_path(path, sizeof(path), s->out_dir, "checkpoint.bin");
+        rc = les_solver_save_checkpoint(s, path, s->t_loop);
+        if (rc) return rc;
+    }
+    if ((s->out_flags & LES_OUT_MONITOR) && s->out_dir[0]) {
+        rc = write_monitor(s, s->t_loop, dt);
+        if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
+    }
+    s->t_loop++;
+    return LESGPU_OK;
+}
+
+int les_solver_run(les_solver* s, int nsteps) {
+    for (int q = 0; q < nsteps; q++) {
+        int rc = les_solver_step(s);
+        if (rc) return rc;
+    }
+    return lesgpu_sync(s->ctx);
+}
+
+int les_solver_save_checkpoint(les_solver* s, const char* path, int t) {
+    if (!s || !path) return LESGPU_EINVAL;
+    double* f[LESGPU_NSTATE];
+    if (alloc_fields(s->n, f)) return LESGPU_ENOMEM;
+    int rc = lesgpu_download_state(s->ctx, (double* const*)f, LESGPU_NSTATE);
+    if (rc) { free_fields(f); return serr(s, rc, lesgpu_last_error(s->ctx)); }
+    FILE* fp = fopen(path, "wb");
+    if (!fp) { free_fields(f); return serr(s, LESGPU_EIO, "cannot open checkpoint for writing"); }
+    int ok = fwrite(&t, sizeof(int), 1, fp) == 1;
+    for (int q = 0; q < LESGPU_NSTATE && ok; q++) ok = fwrite(f[q], sizeof(double), s->n, fp) == s->n;
+    fclose(fp);
+    free_fields(f);
+    if (!ok) return serr(s, LESGPU_EIO, "short checkpoint write");
+    /* restart_info.txt next to the checkpoint (:3691-3697) */
+    char info[1200];
+    snprintf(info, sizeof(info), "%s", path);
+    char* slash = strrchr(info, '/');
+    if (slash) snprintf(slash + 1, sizeof(info) - (size_t)(slash + 1 - info), "restart_info.txt");
+    else snprintf(info, sizeof(info), "restart_info.txt");
+    FILE* fi = fopen(info, "w");
+    if (fi) {
+        fprintf(fi, "BINARY\n%d\n", t);
+        fclose(fi);
+    }
+    return LESGPU_OK;
+}
+
+int les_solver_load_checkpoint(les_solver* s, const char* path, int* t_out) {
+    if (!s || !path) return LESGPU_EINVAL;
+    FILE* fp = fopen(path, "rb");
+    if (!fp) return serr(s, LESGPU_EIO, "cannot open checkpoint");
+    fseek(fp, 0, SEEK_END);
+    long sz = ftell(fp);
+    fseek(fp, 0, SEEK_SET);
+    long want = (long)sizeof(int) + (long)(LESGPU_NSTATE * s->n * sizeof(double));
+    if (sz != want) { fclose(fp); return serr(s, LESGPU_EIO, "checkpoint size does not match the grid"); }
+    int t = 0;
+    double* f[LESGPU_NSTATE];
+    if (alloc_fields(s->n, f)) { fclose(fp); return LESGPU_ENOMEM; }
+    int ok = fread(&t, sizeof(int), 1, fp) == 1;
+    for (int q = 0; q < LESGPU_NSTATE && ok; q++) ok = fread(f[q], sizeof(double), s->n, fp) == s->n;
+    fclose(fp);
+    if (!ok) { free_fields(f); return serr(s, LESGPU_EIO, "short checkpoint read"); }
+    for (int q = 0; q < LESGPU_NSTATE && ok; q++)
+        for (size_t i = 0; i < s->n; i++)
+            if (!isfinite(f[q][i])) { ok = 0; break; }
+    if (!ok) { free_fields(f); return serr(s, LESGPU_ENONFINITE, "checkpoint holds non-finite values"); }
+    int rc = lesgpu_upload_state(s->ctx, (const double* const*)f, LESGPU_NSTATE);
+    free_fields(f);
+    if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
+    if (t_out) *t_out = t;
+    return LESGPU_OK;
+}

@@ -1,0 +1,363 @@
+"""ctypes binding of ``liblesgpu.so`` (include/les_gpu.h and include/les_solver.h).
+
+The library is built in-tree by ``build.py``.  There is no fallback: if the shared
+library is missing or a CUDA call fails, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Dict, Optional, Sequence
+
+import numpy as np
+
+from .config import SolverConfig
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "liblesgpu.so")
+DATA_DIR = os.path.join(PKG_DIR, "data")
+CHEM_BIN = os.path.join(DATA_DIR, "chem.bin")
+TRAN_BIN = os.path.join(DATA_DIR, "tran.bin")
+
+FP64, FP32 = 0, 1
+STATE_NAMES = ["u", "v", "w", "T", "G", "rho", "Y0", "Y1", "Y2", "Y3", "Y4"]
+FIELD_IDS: Dict[str, int] = {name: q for q, name in enumerate(STATE_NAMES)}
+FIELD_IDS.update({"nu_t": 11, "S_mag": 12})
+_INSPECT = (["u_f", "v_f", "w_f", "T_f", "G_f", "rho_f"] + [f"Y{k}_f" for k in range(5)]
+            + ["nu", "mu_mix", "ST", "Cp", "lambda", "alpha"] + [f"D{k}" for k in range(5)]
+            + ["k_rhou", "k_rhov", "k_rhow", "k_T", "k_G"] + [f"k_Y{k}" for k in range(5)])
+FIELD_IDS.update({name: 100 + q for q, name in enumerate(_INSPECT)})
+
+ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "EIO", -5: "ESTATE", -6: "ENONFINITE"}
+
+LES_OUT_PROBES, LES_OUT_MONITOR, LES_OUT_CHECKPOINT = 1, 2, 4
+
+
+class LesgpuError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class LesgpuConfig(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("num_vortices", C.c_int),
+                ("initial_flame_front_i", C.c_int), ("weno_transition_step", C.c_int),
+                ("seed", C.c_uint), ("flame_accel", C.c_int),
+                ("lx", C.c_double), ("ly", C.c_double), ("lz", C.c_double),
+                ("inlet_radius", C.c_double), ("rim_outer_radius", C.c_double),
+                ("inlet_velocity", C.c_double), ("inlet_temperature", C.c_double),
+                ("ambient_temperature", C.c_double), ("turbulence_intensity", C.c_double),
+                ("length_scale", C.c_double), ("s_l", C.c_double),
+                ("burnt_gas_temperature", C.c_double), ("pr_t", C.c_double), ("sc_t", C.c_double),
+                ("d3", C.c_double), ("courant", C.c_double), ("courant_diffusion", C.c_double),
+                ("cs_unburned", C.c_double), ("cs_burnt", C.c_double), ("cs_flame_boost", C.c_double),
+                ("accel_strength", C.c_double), ("accel_width", C.c_double),
+                ("accel_center", C.c_double), ("relax", C.c_double), ("nu_unburnt", C.c_double),
+                ("rho_unburnt_approx", C.c_double), ("rho_burnt_approx", C.c_double),
+                ("equivalence_ratio", C.c_double), ("precision", C.c_int), ("device", C.c_int)]
+
+    @classmethod
+    def from_config(cls, cfg: SolverConfig, precision: int = FP64, device: int = 0) -> "LesgpuConfig":
+        c = cls()
+        d = cfg.as_dict()
+        for name, _t in cls._fields_:
+            if name in d:
+                setattr(c, name, d[name])
+        c.precision = precision
+        c.device = device
+        return c
+
+
+class LesgpuSpecies(C.Structure):
+    _fields_ = [("mw", C.c_double * 5), ("t_mid", C.c_double * 5),
+                ("nasa_high", (C.c_double * 7) * 5), ("nasa_low", (C.c_double * 7) * 5),
+                ("lam", (C.c_double * 4) * 5), ("eta", (C.c_double * 4) * 5),
+                ("dcoef", ((C.c_double * 4) * 5) * 5)]
+
+
+class LesRng(C.Structure):
+    _fields_ = [("r", C.c_int * 34), ("f", C.c_int), ("b", C.c_int), ("n", C.c_ulonglong)]
+
+
+_lib = None
+
+
+def _sig(L, name, res, args):
+    fn = getattr(L, name)
+    fn.restype = res
+    fn.argtypes = args
+
+
+def lib():
+    """Load ``liblesgpu.so``; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(f"{LIB_PATH} is missing: run `python build.py` in {PKG_DIR}")
+        L = C.CDLL(LIB_PATH)
+        vp, ip, dp = C.c_void_p, C.POINTER(C.c_int), C.c_void_p
+        _sig(L, "lesgpu_load_species", C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(LesgpuSpecies)])
+        _sig(L, "lesgpu_create", C.c_int, [C.POINTER(LesgpuConfig), C.POINTER(LesgpuSpecies), C.POINTER(vp)])
+        _sig(L, "lesgpu_destroy", None, [vp])
+        _sig(L, "lesgpu_last_error", C.c_char_p, [vp])
+        _sig(L, "lesgpu_upload_attribute", C.c_int, [vp, vp])
+        _sig(L, "lesgpu_upload_state", C.c_int, [vp, C.POINTER(C.c_void_p), C.c_int])
+        _sig(L, "lesgpu_download_state", C.c_int, [vp, C.POINTER(C.c_void_p), C.c_int])
+        _sig(L, "lesgpu_get_field", C.c_int, [vp, C.c_int, dp])
+        _sig(L, "lesgpu_dt_inputs", C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                               C.POINTER(C.c_double)])
+        _sig(L, "lesgpu_set_inflow", C.c_int, [vp, dp, C.c_int, dp])
+        _sig(L, "lesgpu_step", C.c_int, [vp, C.c_double, C.c_int])
+        _sig(L, "lesgpu_probe_lines", C.c_int, [vp, vp, C.c_int, C.c_int, dp])
+        _sig(L, "lesgpu_monitor", C.c_int, [vp, dp])
+        _sig(L, "lesgpu_check_finite", C.c_int, [vp, C.c_int])
+        _sig(L, "lesgpu_set_debug", C.c_int, [vp, C.c_int])
+        _sig(L, "lesgpu_eval_rhs", C.c_int, [vp, C.c_int])
+        _sig(L, "lesgpu_sync", C.c_int, [vp])
+        _sig(L, "lesgpu_device_bytes", C.c_size_t, [vp])
+        _sig(L, "lesgpu_bytes_for_grid", C.c_size_t, [C.c_int, C.c_int, C.c_int, C.c_int])
+        _sig(L, "les_rng_seed", None, [C.POINTER(LesRng), C.c_uint])
+        _sig(L, "les_rng_next", C.c_int, [C.POINTER(LesRng)])
+        _sig(L, "les_initial_state", C.c_int, [C.POINTER(LesgpuConfig), C.POINTER(LesgpuSpecies), vp,
+                                               C.POINTER(C.c_void_p)])
+        _sig(L, "les_vortices_init", None, [C.POINTER(LesRng), C.POINTER(LesgpuConfig), dp])
+        _sig(L, "les_vortices_update", None, [C.POINTER(LesRng), C.POINTER(LesgpuConfig), dp, C.c_double])
+        _sig(L, "les_inflow_noise", None, [C.POINTER(LesRng), vp, C.c_int, C.c_int, dp])
+        _sig(L, "les_dt", C.c_double, [C.POINTER(LesgpuConfig), C.c_double, C.c_double, C.c_double])
+        _sig(L, "les_solver_create", C.c_int, [C.POINTER(LesgpuConfig), C.c_char_p, C.c_char_p, C.c_int,
+                                               C.POINTER(vp)])
+        _sig(L, "les_solver_destroy", None, [vp])
+        _sig(L, "les_solver_ctx", vp, [vp])
+        _sig(L, "les_solver_last_error", C.c_char_p, [vp])
+        _sig(L, "les_solver_set_outputs", C.c_int, [vp, C.c_char_p, C.c_int])
+        _sig(L, "les_solver_step", C.c_int, [vp])
+        _sig(L, "les_solver_run", C.c_int, [vp, C.c_int])
+        _sig(L, "les_solver_t_loop", C.c_int, [vp])
+        _sig(L, "les_solver_last_dt", C.c_double, [vp])
+        _sig(L, "les_solver_last_umax", C.c_double, [vp])
+        _sig(L, "les_solver_attribute", C.c_int, [vp, vp])
+        _sig(L, "les_solver_save_checkpoint", C.c_int, [vp, C.c_char_p, C.c_int])
+        _sig(L, "les_solver_load_checkpoint", C.c_int, [vp, C.c_char_p, C.POINTER(C.c_int)])
+        _sig(L, "les_solver_vortices", C.c_int, [vp, dp])
+        _sig(L, "les_solver_rng_draws", C.c_ulonglong, [vp])
+        _lib = L
+    return _lib
+
+
+def load_species(chem: str = CHEM_BIN, tran: str = TRAN_BIN) -> LesgpuSpecies:
+    sp = LesgpuSpecies()
+    rc = lib().lesgpu_load_species(chem.encode(), tran.encode(), C.byref(sp))
+    if rc != 0:
+        raise LesgpuError(rc, f"cannot load species from {chem}, {tran}")
+    return sp
+
+
+def _ptrs(arrs: Sequence[np.ndarray]):
+    return (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+
+
+class Rng:
+    """The glibc rand() stream (srand/rand) with private state."""
+
+    def __init__(self, seed: int):
+        self._s = LesRng()
+        lib().les_rng_seed(C.byref(self._s), seed)
+
+    def next(self) -> int:
+        return lib().les_rng_next(C.byref(self._s))
+
+    @property
+    def draws(self) -> int:
+        return self._s.n
+
+
+def initial_state(cfg: SolverConfig, species: Optional[LesgpuSpecies] = None):
+    """Attribute map and state of a fresh run (the reference's initialize()+setting())."""
+    sp = species or load_species()
+    shape = (cfg.nx, cfg.ny, cfg.nz)
+    attr = np.empty(shape, dtype=np.int32)
+    fields = [np.empty(shape, dtype=np.float64) for _ in STATE_NAMES]
+    c = LesgpuConfig.from_config(cfg)
+    rc = lib().les_initial_state(C.byref(c), C.byref(sp), attr.ctypes.data, _ptrs(fields))
+    if rc != 0:
+        raise LesgpuError(rc, "les_initial_state")
+    return attr, dict(zip(STATE_NAMES, fields))
+
+
+class Context:
+    """One ``lesgpu_ctx``: device arena of one grid driven through the C ABI."""
+
+    def __init__(self, cfg: SolverConfig, precision: int = FP64, species: Optional[LesgpuSpecies] = None,
+                 device: int = 0):
+        self.cfg = cfg
+        self.shape = (cfg.nx, cfg.ny, cfg.nz)
+        self._sp = species or load_species()
+        self._c = LesgpuConfig.from_config(cfg, precision, device)
+        h = C.c_void_p()
+        rc = lib().lesgpu_create(C.byref(self._c), C.byref(self._sp), C.byref(h))
+        if rc != 0:
+            raise LesgpuError(rc, "lesgpu_create failed")
+        self._h = h
+
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            raise LesgpuError(rc, f"{what}: {lib().lesgpu_last_error(self._h).decode()}")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().lesgpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload_attribute(self, attr: np.ndarray):
+        a = np.ascontiguousarray(attr, dtype=np.int32)
+        assert a.shape == self.shape
+        self._check(lib().lesgpu_upload_attribute(self._h, a.ctypes.data), "upload_attribute")
+
+    def upload_state(self, state: Dict[str, np.ndarray]):
+        arrs = [np.ascontiguousarray(state[k], dtype=np.float64) for k in STATE_NAMES]
+        for a in arrs:
+            assert a.shape == self.shape
+        self._check(lib().lesgpu_upload_state(self._h, _ptrs(arrs), len(arrs)), "upload_state")
+
+    def download_state(self) -> Dict[str, np.ndarray]:
+        arrs = [np.empty(self.shape, dtype=np.float64) for _ in STATE_NAMES]
+        self._check(lib().lesgpu_download_state(self._h, _ptrs(arrs), len(arrs)), "download_state")
+        return dict(zip(STATE_NAMES, arrs))
+
+    def field(self, name: str) -> np.ndarray:
+        out = np.empty(self.shape, dtype=np.float64)
+        self._check(lib().lesgpu_get_field(self._h, FIELD_IDS[name], out.ctypes.data), f"get_field({name})")
+        return out
+
+    def dt_inputs(self):
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        self._check(lib().lesgpu_dt_inputs(self._h, C.byref(a), C.byref(b), C.byref(c)), "dt_inputs")
+        return a.value, b.value, c.value
+
+    def set_inflow(self, vortices: np.ndarray, noise: np.ndarray):
+        v = np.ascontiguousarray(vortices, dtype=np.float64)
+        n = np.ascontiguousarray(noise, dtype=np.float64)
+        self._check(lib().lesgpu_set_inflow(self._h, v.ctypes.data, v.shape[0], n.ctypes.data), "set_inflow")
+
+    def step(self, dt: float, t_loop: int):
+        self._check(lib().lesgpu_step(self._h, dt, t_loop), "step")
+
+    def eval_rhs(self, t_loop: int):
+        self._check(lib().lesgpu_eval_rhs(self._h, t_loop), "eval_rhs")
+
+    def set_debug(self, on: bool = True):
+        self._check(lib().lesgpu_set_debug(self._h, 1 if on else 0), "set_debug")
+
+    def probe_lines(self, stations: Sequence[int], k_line: int) -> np.ndarray:
+        st = np.ascontiguousarray(stations, dtype=np.int32)
+        out = np.empty((len(st), self.shape[1], 6), dtype=np.float64)
+        self._check(lib().lesgpu_probe_lines(self._h, st.ctypes.data, len(st), k_line, out.ctypes.data),
+                    "probe_lines")
+        return out
+
+    def monitor(self) -> np.ndarray:
+        out = np.empty(6, dtype=np.float64)
+        self._check(lib().lesgpu_monitor(self._h, out.ctypes.data), "monitor")
+        return out
+
+    def check_finite(self, name: str = "u") -> bool:
+        rc = lib().lesgpu_check_finite(self._h, FIELD_IDS[name])
+        if rc == -6:
+            return False
+        self._check(rc, "check_finite")
+        return True
+
+    def sync(self):
+        self._check(lib().lesgpu_sync(self._h), "sync")
+
+    @property
+    def device_bytes(self) -> int:
+        return lib().lesgpu_device_bytes(self._h)
+
+
+class Solver:
+    """``les_solver``: the reference's time loop with the step body on the GPU."""
+
+    def __init__(self, cfg: SolverConfig, precision: int = FP64, start_step: int = 0, chem: str = CHEM_BIN,
+                 tran: str = TRAN_BIN, device: int = 0):
+        self.cfg = cfg
+        self.shape = (cfg.nx, cfg.ny, cfg.nz)
+        self._c = LesgpuConfig.from_config(cfg, precision, device)
+        h = C.c_void_p()
+        rc = lib().les_solver_create(C.byref(self._c), chem.encode(), tran.encode(), start_step, C.byref(h))
+        if rc != 0:
+            raise LesgpuError(rc, "les_solver_create failed")
+        self._h = h
+        self.ctx = Context.__new__(Context)
+        self.ctx.cfg = cfg
+        self.ctx.shape = self.shape
+        self.ctx._h = C.c_void_p(lib().les_solver_ctx(h))
+
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            raise LesgpuError(rc, f"{what}: {lib().les_solver_last_error(self._h).decode()}")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.ctx._h = None
+            lib().les_solver_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_outputs(self, directory: Optional[str], flags: int):
+        self._check(lib().les_solver_set_outputs(self._h, directory.encode() if directory else None, flags),
+                    "set_outputs")
+
+    def step(self, n: int = 1):
+        for _ in range(n):
+            self._check(lib().les_solver_step(self._h), "step")
+
+    def run(self, n: int):
+        self._check(lib().les_solver_run(self._h, n), "run")
+
+    @property
+    def t_loop(self) -> int:
+        return lib().les_solver_t_loop(self._h)
+
+    @property
+    def last_dt(self) -> float:
+        return lib().les_solver_last_dt(self._h)
+
+    @property
+    def rng_draws(self) -> int:
+        return lib().les_solver_rng_draws(self._h)
+
+    def vortices(self) -> np.ndarray:
+        out = np.empty((self.cfg.num_vortices, 7), dtype=np.float64)
+        lib().les_solver_vortices(self._h, out.ctypes.data)
+        return out
+
+    def attribute(self) -> np.ndarray:
+        out = np.empty(self.shape, dtype=np.int32)
+        self._check(lib().les_solver_attribute(self._h, out.ctypes.data), "attribute")
+        return out
+
+    def state(self) -> Dict[str, np.ndarray]:
+        return self.ctx.download_state()
+
+    def field(self, name: str) -> np.ndarray:
+        return self.ctx.field(name)
+
+    def save_checkpoint(self, path: str, t: int):
+        self._check(lib().les_solver_save_checkpoint(self._h, path.encode(), t), "save_checkpoint")
+
+    def load_checkpoint(self, path: str) -> int:
+        t = C.c_int()
+        self._check(lib().les_solver_load_checkpoint(self._h, path.encode(), C.byref(t)), "load_checkpoint")
+        return t.value

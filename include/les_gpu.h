@@ -1,0 +1,161 @@
+/*
+ * les_gpu.h -- C ABI of the B200 solver step for the premixed-flame LES of
+ * les_combustion_solver.c (naist15421/Combustion-LES-Optimization).
+ *
+ * The reference has no plugin or FFI layer: its time loop (les_combustion_solver.c:4390-4603)
+ * mutates global Grid3D arrays through direct calls.  This header is the boundary that
+ * replaces the body of that loop -- the dt reductions (:4399-4411), the SEM inflow plane
+ * (:965-1074), the RK4 stages with calculate_RHS (:4420-4544) and
+ * apply_boundary_conditions (:4555) -- with calls into a CUDA library, while the caller
+ * keeps the host-side pieces (glibc-compatible rand() draws, probe/monitor/checkpoint files).
+ *
+ * Conventions
+ *  - Every field crossing the boundary is a host array of NX*NY*NZ doubles in the
+ *    reference's [i][j][k] order (k fastest, les_combustion_solver.c:286).
+ *  - State field order is the checkpoint.bin order (:3671-3698):
+ *    u, v, w, T, G, rho, Y[C3H8], Y[O2], Y[N2], Y[CO2], Y[H2O].
+ *  - The library owns all device memory; host arrays are only read/written during a call.
+ *  - Calls return LESGPU_OK (0) or a negative LESGPU_E* code and never exit the process;
+ *    lesgpu_last_error() returns a message for the last failure on a context.
+ *  - A context is bound to one CUDA device and one stream and is driven by one host thread.
+ *    Calls are synchronous unless their comment says otherwise.
+ */
+#ifndef LES_GPU_H
+#define LES_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LESGPU_OK 0
+#define LESGPU_EINVAL -1     /* bad argument (null pointer, size mismatch, unknown id) */
+#define LESGPU_ECUDA -2      /* a CUDA runtime call failed */
+#define LESGPU_ENOMEM -3     /* device allocation failed or over the configured budget */
+#define LESGPU_EIO -4        /* file could not be read or has the wrong record layout */
+#define LESGPU_ESTATE -5     /* call out of order (e.g. step before a state was uploaded) */
+#define LESGPU_ENONFINITE -6 /* a NaN/Inf was found where the reference would abort */
+
+#define LESGPU_NSP 5          /* C3H8, O2, N2, CO2, H2O (les_combustion_solver.c:129-133) */
+#define LESGPU_NSTATE 11      /* u v w T G rho Y0..Y4 */
+
+#define LESGPU_FP64 0         /* plain form: everything in double precision */
+#define LESGPU_FP32 1         /* precision form: fp32 bulk, fp64 global sums/reductions */
+
+/* Run-time replacement for the reference's compile-time #defines (:46-83, :136-262) and
+ * function-local constants (:2701-2703, :2834, :4101). */
+typedef struct lesgpu_config {
+    int nx, ny, nz, num_vortices;
+    int initial_flame_front_i, weno_transition_step;
+    unsigned int seed;
+    int flame_accel;                  /* USE_FLAME_ACCEL_MODEL (:208) */
+    double lx, ly, lz;
+    double inlet_radius, rim_outer_radius;
+    double inlet_velocity, inlet_temperature, ambient_temperature;
+    double turbulence_intensity, length_scale;
+    double s_l, burnt_gas_temperature, pr_t, sc_t, d3;
+    double courant, courant_diffusion;
+    double cs_unburned, cs_burnt, cs_flame_boost;
+    double accel_strength, accel_width, accel_center, relax;
+    double nu_unburnt, rho_unburnt_approx, rho_burnt_approx, equivalence_ratio;
+    int precision;                    /* LESGPU_FP64 or LESGPU_FP32 */
+    int device;                       /* CUDA device ordinal */
+} lesgpu_config;
+
+/* Species data as the reference's SpeciesData (:292-305) plus the binary-diffusion fits. */
+typedef struct lesgpu_species {
+    double mw[LESGPU_NSP];            /* g/mol */
+    double t_mid[LESGPU_NSP];
+    double nasa_high[LESGPU_NSP][7];
+    double nasa_low[LESGPU_NSP][7];
+    double lambda[LESGPU_NSP][4];     /* ln-polynomial fits, CGS */
+    double eta[LESGPU_NSP][4];
+    double dcoef[LESGPU_NSP][LESGPU_NSP][4];
+} lesgpu_species;
+
+typedef struct lesgpu_ctx lesgpu_ctx;
+
+/* Field ids for lesgpu_get_field: the 11 state fields, then per-step diagnostics. */
+enum {
+    LESGPU_F_U = 0, LESGPU_F_V, LESGPU_F_W, LESGPU_F_T, LESGPU_F_G, LESGPU_F_RHO,
+    LESGPU_F_Y0, LESGPU_F_Y1, LESGPU_F_Y2, LESGPU_F_Y3, LESGPU_F_Y4,
+    LESGPU_F_NU_T = 11,               /* eddy viscosity of the last RHS evaluation */
+    LESGPU_F_S_MAG = 12,              /* |S| of the last RHS evaluation */
+    /* intermediates of the last RHS evaluation (filtered fields, properties, k-arrays) */
+    LESGPU_F_U_F = 100, LESGPU_F_V_F, LESGPU_F_W_F, LESGPU_F_T_F, LESGPU_F_G_F, LESGPU_F_RHO_F,
+    LESGPU_F_Y0_F, LESGPU_F_Y1_F, LESGPU_F_Y2_F, LESGPU_F_Y3_F, LESGPU_F_Y4_F,
+    LESGPU_F_NU, LESGPU_F_MU_MIX, LESGPU_F_ST, LESGPU_F_CP, LESGPU_F_LAMBDA, LESGPU_F_ALPHA,
+    LESGPU_F_D0, LESGPU_F_D1, LESGPU_F_D2, LESGPU_F_D3, LESGPU_F_D4,
+    LESGPU_F_K_RHOU, LESGPU_F_K_RHOV, LESGPU_F_K_RHOW, LESGPU_F_K_T, LESGPU_F_K_G,
+    LESGPU_F_K_Y0, LESGPU_F_K_Y1, LESGPU_F_K_Y2, LESGPU_F_K_Y3, LESGPU_F_K_Y4
+};
+
+/* Replaces load_chem_bin + load_tran_bin (:324-382): read the two Fortran-record files. */
+int lesgpu_load_species(const char* chem_path, const char* tran_path, lesgpu_species* out);
+
+/* Allocates the device field arena for one grid (replaces the ALLOC_GRID block, :4023-4080). */
+int lesgpu_create(const lesgpu_config* cfg, const lesgpu_species* sp, lesgpu_ctx** out);
+void lesgpu_destroy(lesgpu_ctx* ctx);
+const char* lesgpu_last_error(const lesgpu_ctx* ctx);
+
+/* Cell attribute codes (:1151-1181): 1 inlet, 2 outlet, 3 fluid, 4 wall/free, 5 symmetry,
+ * 6 rim.  NX*NY*NZ ints in [i][j][k] order. */
+int lesgpu_upload_attribute(lesgpu_ctx* ctx, const int* attr);
+
+/* Replaces the state half of load_quick_checkpoint (:3701-3726): nfields (<= 11) host
+ * arrays in checkpoint order; rho*u momentum is derived as the reference does (:3717).
+ * Resets the dt-reduction inputs as a restart does (nu/alpha are not part of the state). */
+int lesgpu_upload_state(lesgpu_ctx* ctx, const double* const* fields, int nfields);
+int lesgpu_download_state(lesgpu_ctx* ctx, double* const* fields, int nfields);
+int lesgpu_get_field(lesgpu_ctx* ctx, int field_id, double* out);
+
+/* The three maxima feeding dt (:1472-1485, :4399-4408): max |u| over inlet+fluid cells
+ * (INLET_VELOCITY when below 1e-10) and max nu / alpha over fluid cells from the last
+ * RHS evaluation (0 before the first step). */
+int lesgpu_dt_inputs(lesgpu_ctx* ctx, double* umax, double* numax, double* alphamax);
+
+/* SEM inflow for the next step (:943-1075 and the white noise of :2987-2997).
+ * vortices: nv x {x, y, z, radius, strength_u, strength_v, strength_w} after the host's
+ *           update_vortices (:900-939) for this step's dt;
+ * noise:    3 x NY x NZ planes of the rand()-derived r1, r2, r3 in [-1, 1] (only inlet
+ *           cells are read), drawn in the reference's (j, k) order after the vortex draws. */
+int lesgpu_set_inflow(lesgpu_ctx* ctx, const double* vortices, int nv, const double* noise);
+
+/* One time step with the given dt: SEM plane, four RK4 stages of calculate_RHS with the
+ * stage updates, the final combine and apply_boundary_conditions.  t_loop selects the
+ * central/WENO5 G-gradient switch (:2740-2780).  Asynchronous on the context's stream. */
+int lesgpu_step(lesgpu_ctx* ctx, double dt, int t_loop);
+
+/* Probe lines for record_flame_region_data (:3403-3471) and the point buffer (:4558-4569):
+ * for each of n x-stations, NY rows of {u, v, w, G, nu_t, S_mag} on the line k = k_line.
+ * out holds n * NY * 6 doubles. */
+int lesgpu_probe_lines(lesgpu_ctx* ctx, const int* i_stations, int n, int k_line, double* out);
+
+/* Monitor reductions of write_monitor_log (:3874-3918): out[0] total mass (sum of
+ * rho*DX*DY*DZ), out[1..2] min/max T, out[3..4] min/max G, out[5] min Y[C3H8]. */
+int lesgpu_monitor(lesgpu_ctx* ctx, double out[6]);
+
+/* check_for_nan (:1289-1305) without exit(): returns LESGPU_ENONFINITE if any u is not finite. */
+int lesgpu_check_finite(lesgpu_ctx* ctx, int field_id);
+
+/* Inspection support (no reference counterpart; the reference exposes these intermediates
+ * as globals, :457-612).  lesgpu_set_debug(ctx, 1) makes every step keep Cp, lambda,
+ * alpha and the stage-1 k-arrays for lesgpu_get_field; lesgpu_eval_rhs evaluates one
+ * calculate_RHS (:2494) at the current state, filling all intermediates, without
+ * advancing the state. */
+int lesgpu_set_debug(lesgpu_ctx* ctx, int enable);
+int lesgpu_eval_rhs(lesgpu_ctx* ctx, int t_loop);
+
+/* Block until all work queued on the context's stream has finished. */
+int lesgpu_sync(lesgpu_ctx* ctx);
+
+/* Bytes of device memory the context holds (for admission by memory budget). */
+size_t lesgpu_device_bytes(const lesgpu_ctx* ctx);
+size_t lesgpu_bytes_for_grid(int nx, int ny, int nz, int precision);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LES_GPU_H */

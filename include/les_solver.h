@@ -1,0 +1,88 @@
+/*
+ * les_solver.h -- C host driver around les_gpu.h: the reference's main() time loop
+ * (les_combustion_solver.c:4016-4632) with the step body on the GPU.
+ *
+ * The host keeps what the reference keeps on the host and must stay bit-identical to it:
+ * the glibc rand() stream (vortex recycling and inflow white noise, drawn in the reference's
+ * order), the SEM vortex positions, the dt formula, and the probe / monitor / checkpoint
+ * files in the reference's formats.  Each solver owns an independent rand() state, so many
+ * solvers can run in one process (ensembles, serving).
+ */
+#ifndef LES_SOLVER_H
+#define LES_SOLVER_H
+
+#include "les_gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* glibc random_r TYPE_3 generator (the algorithm behind srand/rand), one state per user. */
+typedef struct les_rng {
+    int r[34];
+    int f, b;                 /* ring positions of the two taps */
+    unsigned long long n;     /* draws so far */
+} les_rng;
+
+void les_rng_seed(les_rng* g, unsigned int seed);     /* srand(seed) */
+int les_rng_next(les_rng* g);                          /* rand(), 0 .. 2^31-1 */
+#define LES_RAND_MAX 2147483647
+
+/* Host-side pieces of the time loop, usable without a solver object.
+ * vort is nv x {x, y, z, radius, strength_u, strength_v, strength_w}. */
+/* initialize() + setting() (:1085-1285): attribute map and the 11 state fields. */
+int les_initial_state(const lesgpu_config* cfg, const lesgpu_species* sp, int* attr, double* const* fields);
+/* initialize_vortices (:861-897) and update_vortices (:900-939) on a private rand() stream. */
+void les_vortices_init(les_rng* g, const lesgpu_config* cfg, double* vort);
+void les_vortices_update(les_rng* g, const lesgpu_config* cfg, double* vort, double dt);
+/* Inflow white noise (:2990-2992): 3 draws per inlet cell of attr's i = 0 face, (j,k) order. */
+void les_inflow_noise(les_rng* g, const int* attr, int ny, int nz, double* noise);
+/* dt formula (:4400-4411) from the three maxima returned by lesgpu_dt_inputs. */
+double les_dt(const lesgpu_config* cfg, double umax, double numax, double alphamax);
+
+typedef struct les_solver les_solver;
+
+/* Output switches for les_solver_set_outputs. */
+#define LES_OUT_PROBES 1       /* probe_data_flame_region_loc*.csv every step (:4572-4574) */
+#define LES_OUT_MONITOR 2      /* simulation_monitor.csv every 10 steps (:4592) */
+#define LES_OUT_CHECKPOINT 4   /* checkpoint.bin + restart_info.txt every 50 steps (:4583-4589) */
+
+/* Load the species files, create the GPU context, build the attribute map and the initial
+ * state exactly as initialize()+setting() (:1085-1285), seed rand() and place the SEM
+ * vortices (initialize_vortices, :861-897).  t_loop starts at start_step. */
+int les_solver_create(const lesgpu_config* cfg, const char* chem_path, const char* tran_path, int start_step,
+                      les_solver** out);
+void les_solver_destroy(les_solver* s);
+lesgpu_ctx* les_solver_ctx(les_solver* s);
+const char* les_solver_last_error(const les_solver* s);
+
+/* Directory (must exist) and LES_OUT_* flags; creates the probe files with their header
+ * as initialize_probe_file does (:3373-3398). */
+int les_solver_set_outputs(les_solver* s, const char* dir, int flags);
+
+/* One iteration of the time loop (:4390-4603): dt from the GPU maxima, vortex update and
+ * noise draws with rand(), the GPU step, then the enabled outputs. */
+int les_solver_step(les_solver* s);
+int les_solver_run(les_solver* s, int nsteps);
+
+int les_solver_t_loop(const les_solver* s);
+double les_solver_last_dt(const les_solver* s);
+double les_solver_last_umax(const les_solver* s);
+
+/* Host copies of the attribute map and the initial state fields (checkpoint order). */
+int les_solver_attribute(const les_solver* s, int* out);
+
+/* checkpoint.bin in the reference layout (:3671-3698): int t, then u v w T G rho Y0..Y4.
+ * load also restores rho*u momentum as load_quick_checkpoint does (:3716-3726). */
+int les_solver_save_checkpoint(les_solver* s, const char* path, int t);
+int les_solver_load_checkpoint(les_solver* s, const char* path, int* t_out);
+
+/* Vortex table (nv x 7) and rand() draw count, for inspection. */
+int les_solver_vortices(const les_solver* s, double* out);
+unsigned long long les_solver_rng_draws(const les_solver* s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LES_SOLVER_H */
