@@ -1,0 +1,372 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 solver step: cell-steps/s on the 256x128x128 plain-FP64 case.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c2] [--precision fp64|fp32]
+
+A "step" is one iteration of the solver's time loop (les_combustion_solver.c:4390-4603):
+dt from the device maxima, SEM vortex update and inflow noise from the host rand() stream,
+the SEM plane, four RK4 stages and the boundary conditions.  Inputs are seeded synthetic
+data (the reference's own initial condition with a fixed srand seed and placeholder
+species properties).
+
+* value       -- cell-steps/s of K steps with the state resident in HBM, timed with CUDA
+                 events on the solver's stream (max over ranks).
+* e2e         -- the same through the public solver API with host buffers: the state is
+                 uploaded from pinned host memory, every step reads back its dt inputs and
+                 the seven probe lines, and the final state is downloaded, all timed.
+* roofline    -- the dominant kernel class: algorithmic bytes per launch / average launch
+                 time (CUDA events on the solver's stream) against the measured HBM peak.
+* cpu_baseline-- the reference solver itself (oracle/_ref, built from its source) on this
+                 host's cores, for a bounded number of steps of the same workload.
+
+Multi-GPU: one process per GPU under torchrun; each rank advances an independent replica
+of the workload (the solve does not shard), value = all cells x steps / max rank time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import signal
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "combustion-les-optimization_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "cell-steps/s: FP64 plain vs FP32/batched at ≤1e-3 profile err; p50/p99 latency"
+UNIT = "cell-steps/s"
+WORKLOADS = {
+    "c2": "plain FP64 drop-in, 256x128x128 grid over 0.128x0.064x0.064 m, 800 SEM eddies (10%), "
+          "flame plane at x=0.03 m, CFL 0.3",
+    "c1": "64x32x32 grid over 0.128x0.064x0.064 m, 200 SEM eddies (10%), flame plane at x=0.03 m, CFL 0.3",
+    "c3": "512x256x256 grid, 3000 SEM eddies (15%), flame plane at x=0.03 m, CFL 0.3",
+}
+# Algorithmic bytes per cell for one launch of each kernel class, 8-byte fields (each
+# field the kernel must read or write touched once; halos and intermediates in L2 free).
+KERNEL_BYTES_PER_CELL = {
+    "filter_props": (11 + 11 + 8) * 8,        # read stage state, write filtered + properties
+    "strain": (7 + 4) * 8,                    # read u v w G rho mu nu (filtered), write nu_t S ST mu_eff
+    "rhs_combine": (11 + 9 + 11 + 10 + 10 + 11) * 8,   # F, props, Phi_n, acc in/out, stage state
+    "bc": (9 + 6) * 8,                        # EOS pass over all cells dominates the BC class
+    "sem": 0,
+}
+STEP_BYTES_PER_CELL = 1664                    # SURVEY 8(d) convention, FP64, per cell-step
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _traffic_table():
+    """DRAM bytes per cell per launch from the committed ncu summaries (profiles/*.md lines
+    of the form `traffic <kernel> <workload> <bytes_per_cell>`)."""
+    out = {}
+    pd = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(pd):
+        return out
+    for fn in sorted(os.listdir(pd)):
+        if not fn.endswith((".md", ".txt")):
+            continue
+        with open(os.path.join(pd, fn)) as f:
+            for line in f:
+                parts = line.strip().strip("`").split()
+                if len(parts) == 4 and parts[0] == "traffic":
+                    try:
+                        out[(parts[1], parts[2])] = float(parts[3])
+                    except ValueError:
+                        pass
+    return out
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+        os.close(fd)
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                     stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.send_signal(signal.SIGTERM)
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    sm.append(float(p[1]))
+                    smax = max(smax, float(p[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, p[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        os.remove(self.path)
+        if not sm:
+            return None
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist():
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1 and not dist.is_initialized():
+        import datetime
+        backend = "nccl"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, local, world
+
+
+def _max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_reference_rate(workload: str, max_steps: int, budget_s: float, threads: int):
+    """Time the reference solver (oracle/_ref/<workload>/les_ref) on the host cores.
+    Returns (cell-steps/s, steps timed, cores, kind, sample description) or None."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from lesgpu.config import preset
+    cfg = preset(workload)
+    exe = os.path.join(ROOT, "oracle", "_ref", workload, "les_ref")
+    if os.path.exists(exe):
+        work = tempfile.mkdtemp(prefix="lesref_bench_")
+        for fn in ("chem.bin", "tran.bin"):
+            shutil.copyfile(os.path.join(ROOT, "oracle", "_ref", workload, fn), os.path.join(work, fn))
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads), LES_REF_STEPS=str(max_steps), LES_REF_SEED=str(cfg.seed),
+                   LES_REF_NOVTK="1", LES_REF_DUMP_EVERY="0")
+        p = subprocess.Popen([exe], cwd=work, env=env, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE, text=True)
+        steps = []
+        t0 = time.time()
+        try:
+            for line in p.stderr:
+                if line.startswith("LESREF_STEP"):
+                    steps.append(float(line.split()[3]))
+                    if len(steps) >= max_steps or time.time() - t0 > budget_s:
+                        break
+        finally:
+            p.kill()
+            p.wait()
+            shutil.rmtree(work, ignore_errors=True)
+        if not steps:
+            return None
+        timed = steps[1:] if len(steps) > 1 else steps      # the first step pays page faults
+        per = sum(timed) / len(timed)
+        return (cfg.cells / per, len(timed), threads, "reference",
+                f"{len(timed)} of {len(steps)} steps of the {cfg.nx}x{cfg.ny}x{cfg.nz} case, "
+                f"OMP_NUM_THREADS={threads}, wall time per step from omp_get_wtime")
+    # restated oracle fallback (1 thread) on the same workload
+    import oracle
+    orc = oracle.Oracle(cfg.as_dict())
+    orc.step(1)
+    t0 = time.time()
+    n = 0
+    while n < max_steps and time.time() - t0 < budget_s:
+        orc.step(1)
+        n += 1
+    per = (time.time() - t0) / max(n, 1)
+    orc.close()
+    return (cfg.cells / per, n, 1, "port", f"{n} steps of the {cfg.nx}x{cfg.ny}x{cfg.nz} case, serial oracle")
+
+
+def run_reference_arm(args):
+    rank, _local, world = int(os.environ.get("RANK", "0")), 0, int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    steps = max(2, args.warmup + args.steps)
+    r = cpu_reference_rate(args.workload, min(steps, 40), budget_s=150.0, threads=threads)
+    if r is None:
+        print(json.dumps({"impl": "reference", "unavailable": "compiled reference produced no timed steps"}))
+        return 0
+    rate, n, cores, kind, sample = r
+    from lesgpu.config import preset
+    cfg = preset(args.workload)
+    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world,
+            "steps": n, "warmup": 1, "ms_per_step": cfg.cells / rate * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOADS.get(args.workload, args.workload), "grid": [cfg.nx, cfg.ny, cfg.nz]},
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    rank, local, world = _dist()
+    torch.cuda.set_device(local)
+    from lesgpu import native as N
+    from lesgpu.config import preset
+    cfg = preset(args.workload)
+    prec = N.FP32 if args.precision == "fp32" else N.FP64
+    esz = 4 if prec == N.FP32 else 8
+    sol = N.Solver(cfg, precision=prec, device=local)
+    ctx = sol.ctx
+    per_step_launches = (2 if True else 0) + 12 + 4
+
+    # ---- warm-up
+    sol.step(args.warmup)
+    ctx.sync()
+    torch.cuda.synchronize()
+
+    # ---- value: K device-resident steps
+    clocks = Clocks(local) if rank == 0 else None
+    _barrier(world)
+    torch.cuda.synchronize()
+    ctx.sync()
+    if clocks:
+        clocks.start()
+    ctx.mark(0)
+    sol.step(args.steps)
+    ctx.mark(1)
+    ms = ctx.elapsed_ms(0, 1)
+    torch.cuda.synchronize()
+    clk = clocks.stop() if clocks else None
+    _barrier(world)
+    ms_max = _max_over_ranks(ms, world)
+    value = world * cfg.cells * args.steps / (ms_max / 1e3)
+
+    # ---- roofline: per-kernel-class device time over a few further steps
+    ctx.kernel_timing(True)
+    nprof = max(2, min(args.steps, 4))
+    sol.step(nprof)
+    kt = ctx.kernel_times()
+    ctx.kernel_timing(False)
+    cls = max((k for k in kt if kt[k][1] > 0), key=lambda k: kt[k][0])
+    avg_ms = kt[cls][0] / kt[cls][1]
+    bytes_launch = KERNEL_BYTES_PER_CELL[cls] * cfg.cells * esz / 8
+    peak, peak_kind = _peaks()
+    achieved = bytes_launch / (avg_ms / 1e3) / 1e9
+    traffic = _traffic_table().get((cls, args.workload))
+    step_ms = ms_max / args.steps
+    roofline = {"bound": "hbm", "kernel": cls, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind,
+                "traffic": (traffic * cfg.cells if traffic is not None else None),
+                "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": avg_ms,
+                "kernel_share": {k: (v[0] / max(sum(x[0] for x in kt.values()), 1e-30)) for k, v in kt.items()},
+                "step_achieved_gbs": STEP_BYTES_PER_CELL * esz / 8 * cfg.cells / (step_ms / 1e3) / 1e9}
+
+    # ---- e2e: public API with host buffers (pinned), copies inside the timed region
+    st = sol.state()
+    pinned = {k: torch.empty(v.shape, dtype=torch.float64, pin_memory=True) for k, v in st.items()}
+    for k, v in st.items():
+        pinned[k].numpy()[...] = v
+    host_state = {k: t.numpy() for k, t in pinned.items()}
+    stations = [int(x / (cfg.lx / cfg.nx)) for x in (0.010, 0.015, 0.020, 0.025, 0.030, 0.035, 0.040)]
+    stations = [i for i in stations if 0 < i < cfg.nx - 1]
+    _barrier(world)
+    ctx.sync()
+    ctx.mark(2)
+    ctx.upload_state(host_state)
+    for _ in range(args.steps):
+        sol.step(1)
+        ctx.probe_lines(stations, cfg.nz // 2)
+    out = ctx.download_state()
+    ctx.mark(3)
+    e2e_ms = _max_over_ranks(ctx.elapsed_ms(2, 3), world)
+    e2e_value = world * cfg.cells * args.steps / (e2e_ms / 1e3)
+    state_bytes = 11 * cfg.cells * 8
+    n_inlet = int((sol.attribute()[0] == 1).sum())
+    h2d = state_bytes / args.steps + cfg.num_vortices * 7 * 8 + n_inlet * 3 * 8
+    d2h = state_bytes / args.steps + 64 + len(stations) * cfg.ny * 6 * 8
+    del out
+
+    result = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            r = cpu_reference_rate(args.workload, 4, budget_s=60.0, threads=os.cpu_count() or 1)
+            if r is not None:
+                rate, n, cores, kind, sample = r
+                cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+        result = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == N.FP64 else "f32",
+            "data": "synthetic: the reference's initial flame state, seeded SEM inflow, placeholder species properties",
+            "config": {"workload": WORKLOADS.get(args.workload, args.workload), "grid": [cfg.nx, cfg.ny, cfg.nz],
+                       "cells": cfg.cells, "precision": args.precision, "parallelism": f"replicas x{world}",
+                       "l2": f"inputs larger than L2 ({ctx.device_bytes / 2**30:.2f} GiB resident per replica)"},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": per_step_launches * args.steps,
+            "clocks": clk,
+        }
+        print(json.dumps(result))
+    sol.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="c2")
+    ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

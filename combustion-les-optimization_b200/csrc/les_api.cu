@@ -127,6 +127,45 @@ size_t fields_for_precision() { return 55; }
 
 }  // namespace
 
+namespace les {
+
+int tmark_begin(DevCtx& c, int cls) {
+    if (!c.timing) return -1;
+    const int slot = c.ev_used;
+    if (2 * (slot + 1) > (int)c.ev_pool.size()) {
+        for (int q = 0; q < 2; q++) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return -1;
+            c.ev_pool.push_back(e);
+        }
+    }
+    if ((int)c.ev_cls.size() <= slot) c.ev_cls.resize(slot + 1);
+    c.ev_cls[slot] = cls;
+    cudaEventRecord(c.ev_pool[2 * slot], c.stream);
+    c.ev_used++;
+    return slot;
+}
+
+void tmark_end(DevCtx& c, int slot) {
+    if (slot < 0) return;
+    cudaEventRecord(c.ev_pool[2 * slot + 1], c.stream);
+}
+
+void tmark_flush(DevCtx& c) {
+    if (!c.timing || c.ev_used == 0) return;
+    cudaStreamSynchronize(c.stream);
+    for (int q = 0; q < c.ev_used; q++) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, c.ev_pool[2 * q], c.ev_pool[2 * q + 1]) == cudaSuccess) {
+            c.kms[c.ev_cls[q]] += ms;
+            c.kcount[c.ev_cls[q]] += 1;
+        }
+    }
+    c.ev_used = 0;
+}
+
+}  // namespace les
+
 extern "C" {
 
 int lesgpu_load_species(const char* chem_path, const char* tran_path, lesgpu_species* out) {
@@ -282,6 +321,9 @@ void lesgpu_destroy(lesgpu_ctx* ctx) {
     for (int q = 0; q < les::NACC; q++)
         if (d.kd[q]) cudaFree(d.kd[q]);
     if (d.h_pinned) cudaFreeHost(d.h_pinned);
+    for (cudaEvent_t e : d.ev_pool) cudaEventDestroy(e);
+    for (int q = 0; q < 16; q++)
+        if (d.marks[q]) cudaEventDestroy(d.marks[q]);
     if (d.stream) cudaStreamDestroy(d.stream);
     delete ctx;
 }
@@ -553,6 +595,44 @@ int lesgpu_check_finite(lesgpu_ctx* ctx, int field_id) {
     CK(cudaMemcpyAsync(&h, d.flag, sizeof(int), cudaMemcpyDeviceToHost, d.stream));
     CK(cudaStreamSynchronize(d.stream));
     if (h) return fail(ctx, LESGPU_ENONFINITE, "non-finite value found");
+    return LESGPU_OK;
+}
+
+int lesgpu_kernel_timing(lesgpu_ctx* ctx, int enable) {
+    if (!ctx) return LESGPU_EINVAL;
+    ctx->d.timing = enable != 0;
+    for (int q = 0; q < 8; q++) { ctx->d.kms[q] = 0.0; ctx->d.kcount[q] = 0; }
+    return LESGPU_OK;
+}
+
+int lesgpu_mark(lesgpu_ctx* ctx, int slot) {
+    if (!ctx || slot < 0 || slot >= 16) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    if (!d.marks[slot]) CK(cudaEventCreate(&d.marks[slot]));
+    CK(cudaEventRecord(d.marks[slot], d.stream));
+    return LESGPU_OK;
+}
+
+int lesgpu_elapsed_ms(lesgpu_ctx* ctx, int a, int b, double* ms) {
+    if (!ctx || !ms || a < 0 || b < 0 || a >= 16 || b >= 16) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    if (!d.marks[a] || !d.marks[b]) return fail(ctx, LESGPU_ESTATE, "marker not recorded");
+    CK(cudaEventSynchronize(d.marks[b]));
+    float f = 0.f;
+    CK(cudaEventElapsedTime(&f, d.marks[a], d.marks[b]));
+    *ms = f;
+    return LESGPU_OK;
+}
+
+int lesgpu_kernel_times(lesgpu_ctx* ctx, double* ms, long long* launches, int n) {
+    if (!ctx || !ms || !launches || n < 0) return LESGPU_EINVAL;
+    les::tmark_flush(ctx->d);
+    for (int q = 0; q < n && q < LESGPU_NK; q++) {
+        ms[q] = ctx->d.kms[q];
+        launches[q] = ctx->d.kcount[q];
+        ctx->d.kms[q] = 0.0;
+        ctx->d.kcount[q] = 0;
+    }
     return LESGPU_OK;
 }
 

@@ -58,8 +58,21 @@ struct DevCtx {
     double* h_pinned = nullptr;         // pinned staging for small transfers
     size_t h_pinned_len = 0;
     bool have_attr = false, have_state = false, have_inflow = false;
+    // kernel timing: event pairs recorded around each kernel class during a step
+    bool timing = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<int> ev_cls;            // class of each recorded pair
+    int ev_used = 0;
+    cudaEvent_t marks[16] = {};
+    double kms[8] = {0};
+    long long kcount[8] = {0};
     std::string err;
 };
+
+// Kernel-timing helpers (les_api.cu): tmark_begin returns a pair slot or -1.
+int tmark_begin(DevCtx& c, int cls);
+void tmark_end(DevCtx& c, int slot);
+void tmark_flush(DevCtx& c);
 
 // Per-precision entry points (les_f64.cu / les_f32.cu).
 cudaError_t sem_inflow(DevCtx& c);

@@ -49,16 +49,25 @@ cudaError_t step_impl(DevCtx& c, double dt, int t_loop) {
     for (int q = 0; q < NACC; q++) knone.p[q] = nullptr;
 
     // SEM inflow plane (:943-1075)
+    int tm = tmark_begin(c, 0);
     sem_inflow(c);
+    tmark_end(c, tm);
     // four RK4 stages (:4428-4544)
     for (int s = 0; s < 4; s++) {
         F11<R> in = (s == 0) ? S : St;
+        tm = tmark_begin(c, 1);
         k_filter_props<R><<<g, b, 0, st>>>(c.dC, c.attr, in, F, P, c.part, c.dS, s == 3 ? 1 : 0);
+        tmark_end(c, tm);
+        tm = tmark_begin(c, 2);
         k_strain<R><<<g, b, 0, st>>>(c.dC, c.attr, F, P);
+        tmark_end(c, tm);
         // the k-arrays of the first stage are kept for inspection when requested
+        tm = tmark_begin(c, 3);
         k_rhs_combine<R><<<g, b, 0, st>>>(c.dC, c.attr, F, P, S, St, acc, s == 0 ? kd : knone, c.dS, dt, s, t_loop);
+        tmark_end(c, tm);
     }
     // apply_boundary_conditions (:2967-3161)
+    tm = tmark_begin(c, 4);
     {
         const int tpb = 128;
         k_bc_iface<R><<<dim3((c.nz + tpb - 1) / tpb, c.ny), tpb, 0, st>>>(c.dC, c.attr, S, c.plane, c.noise,
@@ -69,6 +78,8 @@ cudaError_t step_impl(DevCtx& c, double dt, int t_loop) {
         }
         k_bc_eos<R><<<g, b, 0, st>>>(c.dC, c.attr, S, c.part, c.dS);
     }
+    tmark_end(c, tm);
+    tmark_flush(c);
     return cudaGetLastError();
 }
 

@@ -114,6 +114,10 @@ def lib():
         _sig(L, "lesgpu_set_debug", C.c_int, [vp, C.c_int])
         _sig(L, "lesgpu_eval_rhs", C.c_int, [vp, C.c_int])
         _sig(L, "lesgpu_sync", C.c_int, [vp])
+        _sig(L, "lesgpu_kernel_timing", C.c_int, [vp, C.c_int])
+        _sig(L, "lesgpu_kernel_times", C.c_int, [vp, dp, dp, C.c_int])
+        _sig(L, "lesgpu_mark", C.c_int, [vp, C.c_int])
+        _sig(L, "lesgpu_elapsed_ms", C.c_int, [vp, C.c_int, C.c_int, C.POINTER(C.c_double)])
         _sig(L, "lesgpu_device_bytes", C.c_size_t, [vp])
         _sig(L, "lesgpu_bytes_for_grid", C.c_size_t, [C.c_int, C.c_int, C.c_int, C.c_int])
         _sig(L, "les_rng_seed", None, [C.POINTER(LesRng), C.c_uint])
@@ -275,6 +279,25 @@ class Context:
 
     def sync(self):
         self._check(lib().lesgpu_sync(self._h), "sync")
+
+    def mark(self, slot: int):
+        self._check(lib().lesgpu_mark(self._h, slot), "mark")
+
+    def elapsed_ms(self, a: int, b: int) -> float:
+        v = C.c_double()
+        self._check(lib().lesgpu_elapsed_ms(self._h, a, b, C.byref(v)), "elapsed_ms")
+        return v.value
+
+    KERNEL_CLASSES = ["sem", "filter_props", "strain", "rhs_combine", "bc"]
+
+    def kernel_timing(self, on: bool = True):
+        self._check(lib().lesgpu_kernel_timing(self._h, 1 if on else 0), "kernel_timing")
+
+    def kernel_times(self) -> Dict[str, tuple]:
+        ms = np.zeros(5)
+        cnt = np.zeros(5, dtype=np.int64)
+        self._check(lib().lesgpu_kernel_times(self._h, ms.ctypes.data, cnt.ctypes.data, 5), "kernel_times")
+        return {k: (float(ms[q]), int(cnt[q])) for q, k in enumerate(self.KERNEL_CLASSES)}
 
     @property
     def device_bytes(self) -> int:

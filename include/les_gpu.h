@@ -147,6 +147,25 @@ int lesgpu_check_finite(lesgpu_ctx* ctx, int field_id);
 int lesgpu_set_debug(lesgpu_ctx* ctx, int enable);
 int lesgpu_eval_rhs(lesgpu_ctx* ctx, int t_loop);
 
+/* Kernel timing (observability; the reference only prints a per-step line, :4601).
+ * With timing enabled every step records CUDA events around each kernel class on the
+ * context's stream and accumulates their durations; lesgpu_kernel_times returns the
+ * totals (ms) and launch counts per class and resets them.  Classes: */
+enum {
+    LESGPU_K_SEM = 0,        /* SEM inflow plane + normalisation */
+    LESGPU_K_FILTER = 1,     /* box filter + mixture properties (4 launches per step) */
+    LESGPU_K_STRAIN = 2,     /* strain, nu_t, S_T (4 per step) */
+    LESGPU_K_RHS = 3,        /* right-hand sides + RK4 stage update (4 per step) */
+    LESGPU_K_BC = 4,         /* boundary faces + EOS/renormalisation */
+    LESGPU_NK = 5
+};
+int lesgpu_kernel_timing(lesgpu_ctx* ctx, int enable);
+/* Device-time markers on the context's stream (slots 0..15): lesgpu_mark records a CUDA
+ * event, lesgpu_elapsed_ms waits for slot b and returns the time between two markers. */
+int lesgpu_mark(lesgpu_ctx* ctx, int slot);
+int lesgpu_elapsed_ms(lesgpu_ctx* ctx, int slot_a, int slot_b, double* ms);
+int lesgpu_kernel_times(lesgpu_ctx* ctx, double* ms, long long* launches, int n);
+
 /* Block until all work queued on the context's stream has finished. */
 int lesgpu_sync(lesgpu_ctx* ctx);
 

@@ -1,0 +1,47 @@
+"""The C-ABI library loads on a CPU-only machine and exports every entry point that
+include/*.h declares (no compute calls are made here)."""
+import ctypes
+import glob
+import os
+import re
+
+from conftest import ROOT
+
+DECL = re.compile(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b((?:lesgpu|les)_\w+)\s*\(", re.M)
+
+
+def declared_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        with open(h) as f:
+            txt = f.read()
+        txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+        for m in DECL.finditer(txt):
+            names.add(m.group(1))
+    return names
+
+
+def test_headers_declare_the_boundary():
+    names = declared_functions()
+    for want in ["lesgpu_create", "lesgpu_upload_state", "lesgpu_dt_inputs", "lesgpu_set_inflow", "lesgpu_step",
+                 "lesgpu_probe_lines", "lesgpu_monitor", "lesgpu_download_state", "lesgpu_last_error",
+                 "lesgpu_destroy", "les_solver_create", "les_solver_step", "les_rng_next"]:
+        assert want in names
+
+
+def test_library_exports_every_declared_symbol(lesgpu_native):
+    lib = ctypes.CDLL(lesgpu_native.LIB_PATH)
+    missing = [n for n in sorted(declared_functions()) if not hasattr(lib, n)]
+    assert not missing, f"declared but not exported: {missing}"
+
+
+def test_missing_library_fails_loudly(tmp_path, monkeypatch):
+    from lesgpu import native
+    monkeypatch.setattr(native, "_lib", None)
+    monkeypatch.setattr(native, "LIB_PATH", str(tmp_path / "liblesgpu.so"))
+    try:
+        native.lib()
+    except FileNotFoundError as e:
+        assert "build.py" in str(e)
+    else:
+        raise AssertionError("expected FileNotFoundError")
