@@ -136,6 +136,21 @@ int lesgpu_probe_lines(lesgpu_ctx* ctx, const int* i_stations, int n, int k_line
  * rho*DX*DY*DZ), out[1..2] min/max T, out[3..4] min/max G, out[5] min Y[C3H8]. */
 int lesgpu_monitor(lesgpu_ctx* ctx, double out[6]);
 
+/* lesgpu_monitor_noalloc -- no counterpart in the reference.  The same six monitor values
+ * as lesgpu_monitor, computed from caller-owned device arrays (n FP64 cells each of rho,
+ * T, G and Y[C3H8]) into a caller-owned device buffer out[6], asynchronously on `stream`
+ * (a cudaStream_t, or NULL for the default stream).  It allocates nothing: for callers that
+ * cannot call cudaMalloc -- a serving loop whose HBM is fully handed out to request slots,
+ * or a latency-bound path that must not take cudaMalloc's device-wide synchronisation.
+ * Its scratch is a fixed 3 MiB __device__ array that every GPU loading the library holds
+ * until exit, so n is limited to LESGPU_NOALLOC_MAX_CELLS; larger n returns LESGPU_EINVAL.
+ * The first call on a device looks up that array's device address and should come before
+ * any stream capture.  All calls share the array: calls that overlap on the GPU race and
+ * must be serialised by the caller. */
+#define LESGPU_NOALLOC_MAX_CELLS 16777216
+int lesgpu_monitor_noalloc(const double* rho, const double* T, const double* G, const double* Y0, size_t n,
+                           double dx, double dy, double dz, double* out, void* stream);
+
 /* check_for_nan (:1289-1305) without exit(): returns LESGPU_ENONFINITE if any u is not finite. */
 int lesgpu_check_finite(lesgpu_ctx* ctx, int field_id);
 
