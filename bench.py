@@ -52,7 +52,8 @@ WORKLOADS = {
 KERNEL_BYTES_PER_CELL = {
     "filter_props": (11 + 11 + 8) * 8,        # read stage state, write filtered + properties
     "strain": (7 + 4) * 8,                    # read u v w G rho mu nu (filtered), write nu_t S ST mu_eff
-    "rhs_combine": (11 + 9 + 11 + 10 + 10 + 11) * 8,   # F, props, Phi_n, acc in/out, stage state
+    "rhs_flow": (8 + 4) * 8,                  # read u v w G rho mu_eff nu_t ST, write 4 k-values
+    "rhs_scalar": (10 + 7 + 4 + 11 + 10 + 10 + 11) * 8,   # F, props, k-flow, Phi_n, acc in/out, stage state
     "bc": (9 + 6) * 8,                        # EOS pass over all cells dominates the BC class
     "sem": 0,
 }

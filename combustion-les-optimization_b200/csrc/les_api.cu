@@ -109,6 +109,20 @@ void build_consts(const lesgpu_config& g, const lesgpu_species& sp, les::Consts&
     C.u_in = g.inlet_velocity;
     C.noise_amp = 0.10 * g.inlet_velocity;                              // :2987
     C.ti_rms = g.inlet_velocity * g.turbulence_intensity;              // :1050
+    auto dc = [](double c) { les::DC d; d.c = c; d.r = 1.0 / c; return d; };
+    C.d_dx = dc(C.dx); C.d_dy = dc(C.dy); C.d_dz = dc(C.dz);
+    C.d_2dx = dc(C.two_dx); C.d_2dy = dc(C.two_dy); C.d_2dz = dc(C.two_dz);
+    C.d_dxx = dc(C.dxx); C.d_dyy = dc(C.dyy); C.d_dzz = dc(C.dzz);
+    C.d_six = dc(6.0);
+    C.d_filter = dc(6.0 + 50.0);
+    C.d_sct2 = dc(C.sc_t2); C.d_prt2 = dc(C.pr_t2);
+    C.d_ramp = dc(0.03);
+    C.d_w2 = dc(C.two_w2);
+    C.d_tau_sl = dc(C.tau_sl > 0 ? C.tau_sl : 1.0);
+    for (int a = 0; a < les::NSP; a++) {
+        C.d_mwk[a] = dc(C.mwk[a]);
+        for (int b = 0; b < les::NSP; b++) C.d_wden[a][b] = dc(C.wden[a][b]);
+    }
 }
 
 unsigned char* read_record(FILE* fp, int* len) {
@@ -123,7 +137,7 @@ unsigned char* read_record(FILE* fp, int* len) {
     return b;
 }
 
-size_t fields_for_precision() { return 55; }
+size_t fields_for_precision() { return 59; }
 
 }  // namespace
 
@@ -272,6 +286,7 @@ int lesgpu_create(const lesgpu_config* cfg, const lesgpu_species* sp, lesgpu_ctx
     for (int s = 0; s < les::NSP; s++) d.D[s] = take();
     d.aT = take(); d.nu_t = take(); d.S_mag = take(); d.ST = take(); d.mu_eff = take();
     for (int q = 0; q < les::NACC; q++) d.acc[q] = take();
+    for (int q = 0; q < 4; q++) d.kflow[q] = take();
     size_t nb = ((size_t)(d.nz + les::BX - 1) / les::BX) * ((d.ny + les::BY - 1) / les::BY) * d.nx;
     d.part_len = 6 * nb + 64;
     size_t planes = (size_t)d.ny * d.nz;
@@ -634,6 +649,12 @@ int lesgpu_kernel_times(lesgpu_ctx* ctx, double* ms, long long* launches, int n)
         ctx->d.kcount[q] = 0;
     }
     return LESGPU_OK;
+}
+
+int lesgpu_selfcheck_division(const double* divisors, int nd, size_t n, unsigned long long seed,
+                              unsigned long long* mismatches) {
+    if (!divisors || nd <= 0 || !mismatches) return LESGPU_EINVAL;
+    return les::selfcheck_division(divisors, nd, n, seed, mismatches);
 }
 
 int lesgpu_sync(lesgpu_ctx* ctx) {

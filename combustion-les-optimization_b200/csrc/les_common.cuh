@@ -29,9 +29,17 @@ constexpr double FORCE_LIMIT = 500.0;
 constexpr double RAMP_DIST = 0.03;
 constexpr double SSR_A = 0.2340, SSR_B = 0.2187;
 
-// Per-context constants, resident in device memory and read through the L1/constant path
-// (every access is warp-uniform).  All derived values are computed on the host with the
-// same operations the reference applies to its macros, so they are bit-identical.
+// A divisor with its reciprocal rounded to nearest.  x / c is evaluated as q = x*r followed
+// by one fma correction q + (x - q*c)*r (Markstein's iteration), which returns the
+// correctly rounded quotient for normal operands -- the same bits as IEEE division -- in
+// 3 FP64 operations instead of a division sequence.
+struct DC {
+    double c, r;
+};
+
+// Per-context constants, passed to every kernel by value (__grid_constant__), so reads go
+// through the constant bank.  All derived values are computed on the host with the same
+// operations the reference applies to its macros, so they are bit-identical.
 struct Consts {
     int nx, ny, nz, flame_accel;
     int weno_step, dco_sym, n_inlet, pad0;
@@ -49,6 +57,11 @@ struct Consts {
     int eta_zero[NSP], lam_zero[NSP], dco_zero[NSP][NSP];
     double wpow[NSP][NSP];              // pow(M_j/M_i, 0.25)           [i][j]
     double wden[NSP][NSP];              // sqrt(8.0)*sqrt(1.0 + M_i/M_j) [i][j]
+    // divisors of the reference's divisions by constants, with reciprocals
+    DC d_dx, d_dy, d_dz, d_2dx, d_2dy, d_2dz, d_dxx, d_dyy, d_dzz;
+    DC d_six, d_filter, d_sct2, d_prt2, d_ramp, d_w2, d_tau_sl;
+    DC d_mwk[NSP];
+    DC d_wden[NSP][NSP];
     // model (:257-262, :2834, :2700-2704)
     double cs_u, cs_b, cs_boost;
     double accel_strength, accel_center, two_w2;   // two_w2 = 2.0*W*W
@@ -77,6 +90,13 @@ struct Scalars {
 __device__ __forceinline__ size_t cid(int i, int j, int k, int ny, int nz) {
     return ((size_t)i * (size_t)ny + (size_t)j) * (size_t)nz + (size_t)k;
 }
+
+__device__ __forceinline__ double cdv(double x, const DC& d) {
+    double q = x * d.r;
+    double e = fma(-q, d.c, x);
+    return fma(e, d.r, q);
+}
+__device__ __forceinline__ float cdv(float x, const DC& d) { return x * (float)d.r; }
 
 // x^3 and x^4 rounded once: glibc pow() returns the correctly rounded power for these
 // arguments, while a plain product rounds twice.  The exact square is split with fma,

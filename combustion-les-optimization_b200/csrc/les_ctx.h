@@ -31,6 +31,7 @@ struct DevCtx {
     void* ST = nullptr;
     void* mu_eff = nullptr;
     void* acc[NACC] = {};
+    void* kflow[4] = {};                // momentum and G right-hand sides of the stage
     void* dbg_cp = nullptr;             // optional inspection buffers (lesgpu_get_field)
     void* dbg_lam = nullptr;
     void* dbg_alpha = nullptr;
@@ -76,6 +77,7 @@ void tmark_flush(DevCtx& c);
 
 // Per-precision entry points (les_f64.cu / les_f32.cu).
 cudaError_t sem_inflow(DevCtx& c);
+int selfcheck_division(const double* divisors, int nd, size_t n, unsigned long long seed, unsigned long long* bad);
 cudaError_t step_f64(DevCtx& c, double dt, int t_loop);
 cudaError_t umax_f64(DevCtx& c);
 cudaError_t monitor_f64(DevCtx& c);

@@ -2,18 +2,23 @@
 // plain form, float for the precision form).  Global sums and maxima are always
 // accumulated in double.
 //
-// One RK4 stage is three passes over the grid:
+// One RK4 stage is four passes over the grid:
 //   A  k_filter_props : 7-point box filter of the 11 stage fields (apply_box_filter,
 //                       les_combustion_solver.c:1307-1470) and the cell-local mixture
 //                       properties (update_nu_mix :1489, update_Dk :1684, update_Cp_mix
 //                       :1762, update_lambda_mix_alpha :1798); partial sums for <rho_f>.
 //   B  k_strain       : resolved strain, G-dependent Smagorinsky nu_t (calculate_nu_t
 //                       :1569), SSR-SGS flame speed (:1913) and mu_eff = mu + rho_f nu_t.
-//   C  k_rhs_combine  : momentum / G / species / temperature right-hand sides
-//                       (calculate_RHS :2552-2962) fused with the RK4 stage update
-//                       (:4432-4455) or the final combine (:4517-4544).
+//   C1 k_rhs_flow     : momentum and G right-hand sides (calculate_RHS :2552-2825).
+//   C2 k_rhs_scalar   : species and temperature right-hand sides (:2837-2962) fused with
+//                       the RK4 stage update (:4432-4455) or the final combine (:4517-4544).
 // After the fourth stage the boundary kernels replay apply_boundary_conditions
 // (:2967-3161) in the reference's face order.
+//
+// Every kernel takes the constant table by value (__grid_constant__): divisors, their
+// reciprocals and the species data are read from the constant bank.  Divisions by
+// constants use cdv() (correctly rounded, see les_common.cuh); divisions by per-cell
+// values are IEEE divisions.
 #pragma once
 
 #include "les_common.cuh"
@@ -46,6 +51,12 @@ template <typename R>
 struct KDbg {                // optional (nullptr): the stage's k-arrays for inspection
     R* p[NACC];
 };
+template <typename R>
+struct KFlow {               // momentum and G right-hand sides handed from C1 to C2
+    R* p[4];                 // k_rhou k_rhov k_rhow k_G
+};
+
+#define LES_KERNEL_CONSTS const __grid_constant__ Consts C
 
 // ---------------------------------------------------------------------------- helpers
 
@@ -59,11 +70,11 @@ __device__ __forceinline__ R fit_prop(const double co[4], int zero, R L, R L2, R
 }
 
 template <typename R>
-__device__ __forceinline__ R eos_rho(const Consts* __restrict__ C, R T, const R Y[NSP], R fallback) {
+__device__ __forceinline__ R eos_rho(const Consts& C, R T, const R Y[NSP], R fallback) {
     // update_rho_from_EOS (:1894-1905)
     R syw = R(0);
 #pragma unroll
-    for (int s = 0; s < NSP; s++) syw += Y[s] / (R)C->mwk[s];
+    for (int s = 0; s < NSP; s++) syw += cdv(Y[s], C.d_mwk[s]);
     if (syw > R(1e-9) && T > R(1.0)) {
         R W = R(1.0) / syw;
         R Rm = (R)R_UNIV / W;
@@ -74,15 +85,17 @@ __device__ __forceinline__ R eos_rho(const Consts* __restrict__ C, R T, const R 
 
 // Cell-local mixture properties of one fluid cell (attr == 3).
 template <typename R>
-__device__ __forceinline__ void cell_props(const Consts* __restrict__ C, R Tl, const R Yf[NSP], R rhof,
-                                           R& mu_mix, R& nu, R D[NSP], R& aT, R& cp_out, R& lam_out,
-                                           R& alpha) {
+__device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP], R rhof, R& mu_mix, R& nu,
+                                           R D[NSP], R& aT, R& cp_out, R& lam_out, R& alpha) {
     R X[NSP];
     R syw = R(0);
     bool tpos = Tl > R(0);
+    R ym[NSP];
+#pragma unroll
+    for (int s = 0; s < NSP; s++) ym[s] = cdv(Yf[s], C.d_mwk[s]);
     if (tpos) {
 #pragma unroll
-        for (int s = 0; s < NSP; s++) syw += Yf[s] / (R)C->mwk[s];
+        for (int s = 0; s < NSP; s++) syw += ym[s];
     }
     bool ok = tpos && !(syw < R(1e-9));
     // Cp (:1772-1786) -- independent of the mole fractions
@@ -94,10 +107,10 @@ __device__ __forceinline__ void cell_props(const Consts* __restrict__ C, R Tl, c
         R cp = R(0);
 #pragma unroll
         for (int s = 0; s < NSP; s++) {
-            const double* a = (Tl > (R)C->t_mid[s]) ? C->nasa_high[s] : C->nasa_low[s];
+            const double* a = (Tl > (R)C.t_mid[s]) ? C.nasa_high[s] : C.nasa_low[s];
             R cpr = (R)a[0] + (R)a[1] * Tl + (R)a[2] * T2 + (R)a[3] * T3 + (R)a[4] * T4;
             R cpm = cpr * (R)R_UNIV;
-            R cpk = (C->mwk[s] < 1e-9) ? R(1000.0) : cpm / (R)C->mwk[s];
+            R cpk = (C.mwk[s] < 1e-9) ? R(1000.0) : cdv(cpm, C.d_mwk[s]);
             cp += Yf[s] * cpk;
         }
         Cp = fmax(R(100.0), cp);
@@ -115,7 +128,7 @@ __device__ __forceinline__ void cell_props(const Consts* __restrict__ C, R Tl, c
         return;
     }
 #pragma unroll
-    for (int s = 0; s < NSP; s++) X[s] = (Yf[s] / (R)C->mwk[s]) / syw;
+    for (int s = 0; s < NSP; s++) X[s] = ym[s] / syw;
     const R L = log(Tl);
     const R L2 = L * L;
     const R L3 = pow3_rn(L);
@@ -123,8 +136,8 @@ __device__ __forceinline__ void cell_props(const Consts* __restrict__ C, R Tl, c
     R muk[NSP], lamk[NSP];
 #pragma unroll
     for (int s = 0; s < NSP; s++) {
-        muk[s] = fit_prop<R>(C->eta[s], C->eta_zero[s], L, L2, L3) * R(0.1);
-        lamk[s] = fit_prop<R>(C->lam[s], C->lam_zero[s], L, L2, L3) * R(1e-5);
+        muk[s] = fit_prop<R>(C.eta[s], C.eta_zero[s], L, L2, L3) * R(0.1);
+        lamk[s] = fit_prop<R>(C.lam[s], C.lam_zero[s], L, L2, L3) * R(1e-5);
     }
     // Wilke (:1530-1546) and Wassiljew (:1842-1863) share the same phi_ij, the same skip
     // rule and the same summation order, so one denominator per species serves both.
@@ -137,8 +150,8 @@ __device__ __forceinline__ void cell_props(const Consts* __restrict__ C, R Tl, c
         for (int b = 0; b < NSP; b++) {
             if (X[b] < R(1e-12)) continue;
             R sr = sqrt(muk[a] / muk[b]);
-            R t = R(1.0) + sr * (R)C->wpow[a][b];
-            R ph = (t * t) / (R)C->wden[a][b];
+            R t = R(1.0) + sr * (R)C.wpow[a][b];
+            R ph = cdv(t * t, C.d_wden[a][b]);
             den += X[b] * ph;
         }
         if (den > R(1e-9)) {
@@ -159,14 +172,14 @@ __device__ __forceinline__ void cell_props(const Consts* __restrict__ C, R Tl, c
     // Hirschfelder-Curtiss (:1716-1749).  Binary coefficients D_kj are evaluated once per
     // unordered pair when the fit table is symmetric.
     R Dm[NSP][NSP];
-    if (C->dco_sym) {
+    if (C.dco_sym) {
 #pragma unroll
         for (int a = 0; a < NSP; a++)
 #pragma unroll
             for (int b = a + 1; b < NSP; b++) {
                 R v = R(0);
                 if (X[a] > R(1e-12) || X[b] > R(1e-12))
-                    v = fit_prop<R>(C->dco[a][b], C->dco_zero[a][b], L, L2, L3) * R(1e-4);
+                    v = fit_prop<R>(C.dco[a][b], C.dco_zero[a][b], L, L2, L3) * R(1e-4);
                 Dm[a][b] = v;
                 Dm[b][a] = v;
             }
@@ -176,7 +189,7 @@ __device__ __forceinline__ void cell_props(const Consts* __restrict__ C, R Tl, c
 #pragma unroll
             for (int b = 0; b < NSP; b++) {
                 R v = R(0);
-                if (a != b && X[b] > R(1e-12)) v = fit_prop<R>(C->dco[a][b], C->dco_zero[a][b], L, L2, L3) * R(1e-4);
+                if (a != b && X[b] > R(1e-12)) v = fit_prop<R>(C.dco[a][b], C.dco_zero[a][b], L, L2, L3) * R(1e-4);
                 Dm[a][b] = v;
             }
     }
@@ -194,7 +207,7 @@ __device__ __forceinline__ void cell_props(const Consts* __restrict__ C, R Tl, c
         R Dv;
         if (fabs(R(1.0) - X[a]) < R(1e-9)) {
             int o = (a != N2) ? N2 : O2;
-            Dv = fit_prop<R>(C->dco[a][o], C->dco_zero[a][o], L, L2, L3) * R(1e-4);
+            Dv = fit_prop<R>(C.dco[a][o], C.dco_zero[a][o], L, L2, L3) * R(1e-4);
         } else if (sx > R(1e-12)) {
             Dv = (R(1.0) - X[a]) / sx;
         } else {
@@ -209,17 +222,17 @@ __device__ __forceinline__ void cell_props(const Consts* __restrict__ C, R Tl, c
 // ------------------------------------------------------------------ pass A: filter + props
 
 template <typename R>
-__global__ void __launch_bounds__(NT) k_filter_props(const Consts* __restrict__ C, const uint8_t* __restrict__ attr,
-                                                     F11<R> in, F11<R> F, PropBuf<R> P, double* __restrict__ part,
-                                                     Scalars* __restrict__ S, int want_max) {
+__global__ void __launch_bounds__(NT, 2)
+    k_filter_props(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> in, F11<R> F, PropBuf<R> P,
+                   double* __restrict__ part, Scalars* __restrict__ S, int want_max) {
     __shared__ double sh[NT / 32];
     __shared__ bool last;
-    const int nx = C->nx, ny = C->ny, nz = C->nz;
+    const int nx = C.nx, ny = C.ny, nz = C.nz;
     const int k = blockIdx.x * BX + threadIdx.x;
     const int j = blockIdx.y * BY + threadIdx.y;
     const int i = blockIdx.z;
     const int tid = threadIdx.y * BX + threadIdx.x;
-    const size_t sI = (size_t)ny * nz, sJ = (size_t)nz;
+    const ptrdiff_t sI = (ptrdiff_t)ny * nz, sJ = (ptrdiff_t)nz;
     double mass = 0.0, mnu = 0.0, mal = 0.0;
     if (k < nz && j < ny) {
         const size_t id = cid(i, j, k, ny, nz);
@@ -228,16 +241,15 @@ __global__ void __launch_bounds__(NT) k_filter_props(const Consts* __restrict__ 
         R f[NSTATE];
 #pragma unroll
         for (int q = 0; q < NSTATE; q++) {
-            const R* __restrict__ x = in.p[q];
+            const R* __restrict__ x = in.p[q] + id;
             if (filt) {
-                f[q] = (x[id - sI] + x[id - sJ] + x[id - 1] + R(FILTER_W) * x[id] + x[id + 1] + x[id + sJ] + x[id + sI]) /
-                       R(6.0 + FILTER_W);
+                f[q] = cdv(x[-sI] + x[-sJ] + x[-1] + R(FILTER_W) * x[0] + x[1] + x[sJ] + x[sI], C.d_filter);
             } else {
-                f[q] = x[id];
+                f[q] = x[0];
             }
             F.p[q][id] = f[q];
         }
-        if (a == 1 || a == 2 || a == 3 || a == 5) mass = (((double)f[5] * C->dx) * C->dy) * C->dz;
+        if (a == 1 || a == 2 || a == 3 || a == 5) mass = (((double)f[5] * C.dx) * C.dy) * C.dz;
         if (a == 3) {
             R mu_mix, nu, D[NSP], aT, cp, lam, alpha;
             cell_props<R>(C, f[3], &f[6], f[5], mu_mix, nu, D, aT, cp, lam, alpha);
@@ -249,13 +261,15 @@ __global__ void __launch_bounds__(NT) k_filter_props(const Consts* __restrict__ 
             if (P.dbg_cp) { P.dbg_cp[id] = cp; P.dbg_lam[id] = lam; P.dbg_alpha[id] = alpha; }
             mnu = (double)nu;
             mal = (double)alpha;
-        } else {
+        } else if (P.dbg_cp) {
+            // property values of non-fluid cells are never read by the step; they are filled
+            // only for inspection, with the reference's defaults
             P.mu_mix[id] = R(1.8e-5);
             P.nu[id] = R(1.5e-5);
 #pragma unroll
             for (int s = 0; s < NSP; s++) P.D[s][id] = R(0);
             P.aT[id] = R(0);
-            if (P.dbg_cp) { P.dbg_cp[id] = R(1000.0); P.dbg_lam[id] = R(0); P.dbg_alpha[id] = R(0); }
+            P.dbg_cp[id] = R(1000.0); P.dbg_lam[id] = R(0); P.dbg_alpha[id] = R(0);
         }
     }
     // partial sums for the stage's <rho_f> (:2536-2550) and, on the last stage, the
@@ -286,7 +300,7 @@ __global__ void __launch_bounds__(NT) k_filter_props(const Consts* __restrict__ 
         s = block_sum<NT>(s, sh, tid);
         if (want_max) { mn = block_max<NT>(mn, sh, tid); ma = block_max<NT>(ma, sh, tid); }
         if (tid == 0) {
-            S->rho_avg = (C->total_volume > 0) ? (s / C->total_volume) : 1.2;
+            S->rho_avg = (C.total_volume > 0) ? (s / C.total_volume) : 1.2;
             if (want_max) { S->numax = mn; S->alphamax = ma; }
             S->counter[0] = 0u;
         }
@@ -296,31 +310,30 @@ __global__ void __launch_bounds__(NT) k_filter_props(const Consts* __restrict__ 
 // ------------------------------------------------------------------ pass B: strain + nu_t + S_T
 
 template <typename R>
-__global__ void __launch_bounds__(NT) k_strain(const Consts* __restrict__ C, const uint8_t* __restrict__ attr,
-                                               F11<R> F, PropBuf<R> P) {
-    const int nx = C->nx, ny = C->ny, nz = C->nz;
+__global__ void __launch_bounds__(NT, 3)
+    k_strain(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> F, PropBuf<R> P) {
+    const int nx = C.nx, ny = C.ny, nz = C.nz;
     const int k = blockIdx.x * BX + threadIdx.x;
     const int j = blockIdx.y * BY + threadIdx.y;
     const int i = blockIdx.z;
     if (k >= nz || j >= ny) return;
-    const size_t sI = (size_t)ny * nz, sJ = (size_t)nz;
+    const ptrdiff_t sI = (ptrdiff_t)ny * nz, sJ = (ptrdiff_t)nz;
     const size_t id = cid(i, j, k, ny, nz);
     const bool interior = i >= 1 && i < nx - 1 && j >= 1 && j < ny - 1 && k >= 1 && k < nz - 1;
     const int a = attr[id];
     if (interior && a == 3) {
-        const R* __restrict__ uf = F.p[0];
-        const R* __restrict__ vf = F.p[1];
-        const R* __restrict__ wf = F.p[2];
-        const R tdx = (R)C->two_dx, tdy = (R)C->two_dy, tdz = (R)C->two_dz;
-        R du_dx = (uf[id + sI] - uf[id - sI]) / tdx;
-        R dv_dy = (vf[id + sJ] - vf[id - sJ]) / tdy;
-        R dw_dz = (wf[id + 1] - wf[id - 1]) / tdz;
-        R du_dy = (uf[id + sJ] - uf[id - sJ]) / tdy;
-        R du_dz = (uf[id + 1] - uf[id - 1]) / tdz;
-        R dv_dx = (vf[id + sI] - vf[id - sI]) / tdx;
-        R dv_dz = (vf[id + 1] - vf[id - 1]) / tdz;
-        R dw_dx = (wf[id + sI] - wf[id - sI]) / tdx;
-        R dw_dy = (wf[id + sJ] - wf[id - sJ]) / tdy;
+        const R* __restrict__ uf = F.p[0] + id;
+        const R* __restrict__ vf = F.p[1] + id;
+        const R* __restrict__ wf = F.p[2] + id;
+        R du_dx = cdv(uf[sI] - uf[-sI], C.d_2dx);
+        R dv_dy = cdv(vf[sJ] - vf[-sJ], C.d_2dy);
+        R dw_dz = cdv(wf[1] - wf[-1], C.d_2dz);
+        R du_dy = cdv(uf[sJ] - uf[-sJ], C.d_2dy);
+        R du_dz = cdv(uf[1] - uf[-1], C.d_2dz);
+        R dv_dx = cdv(vf[sI] - vf[-sI], C.d_2dx);
+        R dv_dz = cdv(vf[1] - vf[-1], C.d_2dz);
+        R dw_dx = cdv(wf[sI] - wf[-sI], C.d_2dx);
+        R dw_dy = cdv(wf[sJ] - wf[-sJ], C.d_2dy);
         R S11 = du_dx, S22 = dv_dy, S33 = dw_dz;
         R S12 = R(0.5) * (du_dy + dv_dx), S13 = R(0.5) * (du_dz + dw_dx), S23 = R(0.5) * (dv_dz + dw_dy);
         R Sij = R(2.0) * (S12 * S12 + S13 * S13 + S23 * S23) + S11 * S11 + S22 * S22 + S33 * S33;
@@ -329,9 +342,9 @@ __global__ void __launch_bounds__(NT) k_strain(const Consts* __restrict__ C, con
         R g = F.p[4][id];
         if (g < R(0.0)) g = R(0.0);
         if (g > R(1.0)) g = R(1.0);
-        R cs = (R)C->cs_u + ((R)C->cs_b - (R)C->cs_u) * g;
-        cs += (R)C->cs_boost * R(4.0) * g * (R(1.0) - g);
-        const R dx = (R)C->dx;
+        R cs = (R)C.cs_u + ((R)C.cs_b - (R)C.cs_u) * g;
+        cs += (R)C.cs_boost * R(4.0) * g * (R(1.0) - g);
+        const R dx = (R)C.dx;
         R nut = (cs * dx) * (cs * dx) * Smag;
         P.nu_t[id] = nut;
         P.S_mag[id] = Smag;
@@ -339,7 +352,7 @@ __global__ void __launch_bounds__(NT) k_strain(const Consts* __restrict__ C, con
         // SSR-SGS turbulent flame speed (:1926-1957)
         R nul = P.nu[id];
         R num = Sij - (div * div) * R(1.0 / 3.0);
-        R X = ((R)C->dx4 / (nul * nul)) * num;
+        R X = ((R)C.dx4 / (nul * nul)) * num;
         R d_eta;
         if (X < R(SMALL)) {
             d_eta = R(1.0);
@@ -350,28 +363,27 @@ __global__ void __launch_bounds__(NT) k_strain(const Consts* __restrict__ C, con
         }
         R eta = dx / (d_eta + R(SMALL));
         R Dce = R(8.0) * eta;
-        R asf = R(8.0) * exp((R)C->ssr_cdF / (Dce + R(SMALL)));
-        R base = asf * eta / dx;
-        R wr = pow(base, (R)(2.0 - C->d3));
+        R asf = R(8.0) * exp((R)C.ssr_cdF / (Dce + R(SMALL)));
+        R base = cdv(asf * eta, C.d_dx);
+        R wr = pow(base, (R)(2.0 - C.d3));
         R te = R(0.0);
-        if (C->tau_sl > SMALL) te = dx * fmax(R(0.0), div) / (R)C->tau_sl;
+        if (C.tau_sl > SMALL) te = cdv(dx * fmax(R(0.0), div), C.d_tau_sl);
         R ratio = wr + te;
-        R st = (R)C->s_l * fmax(R(0.0), ratio);
-        P.ST[id] = fmax((R)C->s_l, st);
+        R st = (R)C.s_l * fmax(R(0.0), ratio);
+        P.ST[id] = fmax((R)C.s_l, st);
     } else {
         P.nu_t[id] = R(0);
         P.S_mag[id] = R(0);
-        P.ST[id] = interior ? (R)C->s_l : R(0);
+        P.ST[id] = interior ? (R)C.s_l : R(0);
         P.mu_eff[id] = R(0);
     }
 }
 
-// ------------------------------------------------------------------ pass C: RHS + combine
+// ------------------------------------------------------------------ pass C: right-hand sides
 
-// One axis of the TENO5 G-advection (:2258-2295); q[0..6] = phi at offsets -3..+3.
+// teno5_reconstruct (:2190-2236)
 template <typename R>
-__device__ __forceinline__ R teno5_rec(R v0, R v1, R v2, R v3, R v4) {
-    // teno5_reconstruct (:2190-2236)
+__device__ __forceinline__ R teno5_rec(const Consts& C, R v0, R v1, R v2, R v3, R v4) {
     R a0 = v0 - R(2.0) * v1 + v2, b0 = v0 - R(4.0) * v1 + R(3.0) * v2;
     R a1 = v1 - R(2.0) * v2 + v3, b1 = v1 - v3;
     R a2 = v2 - R(2.0) * v3 + v4, b2 = R(3.0) * v2 - R(4.0) * v3 + v4;
@@ -379,9 +391,9 @@ __device__ __forceinline__ R teno5_rec(R v0, R v1, R v2, R v3, R v4) {
     R is1 = R(13.0 / 12.0) * (a1 * a1) + R(1.0 / 4.0) * (b1 * b1);
     R is2 = R(13.0 / 12.0) * (a2 * a2) + R(1.0 / 4.0) * (b2 * b2);
     int d0 = (is0 < R(TENO_CUT)) ? 1 : 0, d1 = (is1 < R(TENO_CUT)) ? 1 : 0, d2 = (is2 < R(TENO_CUT)) ? 1 : 0;
-    R p0 = (R(2.0) * v0 - R(7.0) * v1 + R(11.0) * v2) / R(6.0);
-    R p1 = (-v1 + R(5.0) * v2 + R(2.0) * v3) / R(6.0);
-    R p2 = (R(2.0) * v2 + R(5.0) * v3 - v4) / R(6.0);
+    R p0 = cdv(R(2.0) * v0 - R(7.0) * v1 + R(11.0) * v2, C.d_six);
+    R p1 = cdv(-v1 + R(5.0) * v2 + R(2.0) * v3, C.d_six);
+    R p2 = cdv(R(2.0) * v2 + R(5.0) * v3 - v4, C.d_six);
     if (d0 + d1 + d2 == 0) {
         if (is0 <= is1 && is0 <= is2) return p0;
         else if (is1 <= is0 && is1 <= is2) return p1;
@@ -393,18 +405,18 @@ __device__ __forceinline__ R teno5_rec(R v0, R v1, R v2, R v3, R v4) {
     return (w0 * p0 + w1 * p1 + w2 * p2) / ws;
 }
 
+// One axis of the TENO5 G-advection (:2258-2295).
 template <typename R>
-__device__ __forceinline__ R teno_axis(R vel, const R* __restrict__ phi, size_t id, size_t s, R d) {
-    R q0 = phi[id - 3 * s], q1 = phi[id - 2 * s], q2 = phi[id - s], q3 = phi[id], q4 = phi[id + s], q5 = phi[id + 2 * s],
-      q6 = phi[id + 3 * s];
+__device__ __forceinline__ R teno_axis(const Consts& C, R vel, const R* __restrict__ q, ptrdiff_t s, const DC& d) {
+    R q0 = q[-3 * s], q1 = q[-2 * s], q2 = q[-s], q3 = q[0], q4 = q[s], q5 = q[2 * s], q6 = q[3 * s];
     if (vel >= R(0.0)) {
-        R ph = teno5_rec<R>(q1, q2, q3, q4, q5);
-        R mh = teno5_rec<R>(q0, q1, q2, q3, q4);
-        return vel * (ph - mh) / d;
+        R ph = teno5_rec<R>(C, q1, q2, q3, q4, q5);
+        R mh = teno5_rec<R>(C, q0, q1, q2, q3, q4);
+        return cdv(vel * (ph - mh), d);
     } else {
-        R mh = teno5_rec<R>(q5, q4, q3, q2, q1);
-        R ph = teno5_rec<R>(q6, q5, q4, q3, q2);
-        return vel * (ph - mh) / d;
+        R mh = teno5_rec<R>(C, q5, q4, q3, q2, q1);
+        R ph = teno5_rec<R>(C, q6, q5, q4, q3, q2);
+        return cdv(vel * (ph - mh), d);
     }
 }
 
@@ -419,8 +431,8 @@ __device__ __forceinline__ void weno_is(R v1, R v2, R v3, R v4, R v5, R& is0, R&
     is2 = R(13.0 / 12.0) * (a2 * a2) + R(1.0 / 4.0) * (b2 * b2);
 }
 template <typename R>
-__device__ __forceinline__ R weno5_grad(const R* __restrict__ phi, size_t id, size_t s, R dx) {
-    R p0 = phi[id - 2 * s], p1 = phi[id - s], p2 = phi[id], p3 = phi[id + s], p4 = phi[id + 2 * s], p5 = phi[id + 3 * s];
+__device__ __forceinline__ R weno5_grad(const Consts& C, const R* __restrict__ q, ptrdiff_t s, const DC& dx) {
+    R p0 = q[-2 * s], p1 = q[-s], p2 = q[0], p3 = q[s], p4 = q[2 * s], p5 = q[3 * s];
     const R eps = R(1.0e-6);
     R i0, i1, i2;
     weno_is<R>(p1, p2, p3, p4, p5, i0, i1, i2);
@@ -428,20 +440,20 @@ __device__ __forceinline__ R weno5_grad(const R* __restrict__ phi, size_t id, si
     R a0 = R(3.0 / 10.0) / (e0 * e0), a1 = R(6.0 / 10.0) / (e1 * e1), a2 = R(1.0 / 10.0) / (e2 * e2);
     R sa = a0 + a1 + a2;
     R w0 = a0 / sa, w1 = a1 / sa, w2 = a2 / sa;
-    R s0 = (R(2.0) * p1 - R(7.0) * p2 + R(11.0) * p3) / R(6.0);
-    R s1 = (-p2 + R(5.0) * p3 + R(2.0) * p4) / R(6.0);
-    R s2 = (R(2.0) * p3 + R(5.0) * p4 - p5) / R(6.0);
+    R s0 = cdv(R(2.0) * p1 - R(7.0) * p2 + R(11.0) * p3, C.d_six);
+    R s1 = cdv(-p2 + R(5.0) * p3 + R(2.0) * p4, C.d_six);
+    R s2 = cdv(R(2.0) * p3 + R(5.0) * p4 - p5, C.d_six);
     R ph = w0 * s0 + w1 * s1 + w2 * s2;
     weno_is<R>(p0, p1, p2, p3, p4, i0, i1, i2);
     e0 = eps + i0; e1 = eps + i1; e2 = eps + i2;
     a0 = R(1.0 / 10.0) / (e0 * e0); a1 = R(6.0 / 10.0) / (e1 * e1); a2 = R(3.0 / 10.0) / (e2 * e2);
     sa = a0 + a1 + a2;
     w0 = a0 / sa; w1 = a1 / sa; w2 = a2 / sa;
-    R m0 = (-p0 + R(5.0) * p1 + R(2.0) * p2) / R(6.0);
-    R m1 = (R(2.0) * p1 + R(5.0) * p2 - p3) / R(6.0);
-    R m2 = (R(11.0) * p2 - R(7.0) * p3 + R(2.0) * p4) / R(6.0);
+    R m0 = cdv(-p0 + R(5.0) * p1 + R(2.0) * p2, C.d_six);
+    R m1 = cdv(R(2.0) * p1 + R(5.0) * p2 - p3, C.d_six);
+    R m2 = cdv(R(11.0) * p2 - R(7.0) * p3 + R(2.0) * p4, C.d_six);
     R mh = w0 * m0 + w1 * m1 + w2 * m2;
-    return (ph - mh) / dx;
+    return cdv(ph - mh, dx);
 }
 
 // superbee_limiter (:2017-2028)
@@ -455,7 +467,7 @@ __device__ __forceinline__ R superbee(R r) {
 
 // MUSCL-superbee along one axis (:2058-2094); values at offsets -2..+2.
 template <typename R>
-__device__ __forceinline__ R muscl_axis(R vel, R pm2, R pm1, R p0, R pp1, R pp2, R d) {
+__device__ __forceinline__ R muscl_axis(R vel, R pm2, R pm1, R p0, R pp1, R pp2, const DC& d) {
     if (vel >= R(0.0)) {
         R dup_im = pm1 - pm2, ddn_im = p0 - pm1;
         R r_im = (fabs(ddn_im) < R(SMALL)) ? R(1e9) : dup_im / ddn_im;
@@ -463,7 +475,7 @@ __device__ __forceinline__ R muscl_axis(R vel, R pm2, R pm1, R p0, R pp1, R pp2,
         R dup_i = p0 - pm1, ddn_i = pp1 - p0;
         R r_i = (fabs(ddn_i) < R(SMALL)) ? R(1e9) : dup_i / ddn_i;
         R phi_iph = p0 + R(0.5) * superbee<R>(r_i) * ddn_i;
-        return vel * (phi_iph - phi_imh) / d;
+        return cdv(vel * (phi_iph - phi_imh), d);
     } else {
         R dup_i = pp1 - p0, ddn_i = p0 - pm1;
         R r_i = (fabs(ddn_i) < R(SMALL)) ? R(1e9) : dup_i / ddn_i;
@@ -471,72 +483,246 @@ __device__ __forceinline__ R muscl_axis(R vel, R pm2, R pm1, R p0, R pp1, R pp2,
         R dup_ip = pp2 - pp1, ddn_ip = pp1 - p0;
         R r_ip = (fabs(ddn_ip) < R(SMALL)) ? R(1e9) : dup_ip / ddn_ip;
         R phi_iph = pp1 - R(0.5) * superbee<R>(r_ip) * ddn_ip;
-        return vel * (phi_iph - phi_imh) / d;
+        return cdv(vel * (phi_iph - phi_imh), d);
     }
 }
 
 // First-order upwind fallback used by the non-conservative schemes near faces
 // (:642-651, :2043-2052).
 template <typename R>
-__device__ __forceinline__ R upwind3(const R* __restrict__ phi, size_t id, size_t sI, size_t sJ, R u, R v, R w, R dx,
-                                     R dy, R dz) {
+__device__ __forceinline__ R upwind3(const Consts& C, const R* __restrict__ q, ptrdiff_t sI, ptrdiff_t sJ, R u, R v,
+                                     R w) {
     R f;
-    if (u >= R(0.0)) f = u * (phi[id] - phi[id - sI]) / dx;
-    else f = u * (phi[id + sI] - phi[id]) / dx;
-    if (v >= R(0.0)) f += v * (phi[id] - phi[id - sJ]) / dy;
-    else f += v * (phi[id + sJ] - phi[id]) / dy;
-    if (w >= R(0.0)) f += w * (phi[id] - phi[id - 1]) / dz;
-    else f += w * (phi[id + 1] - phi[id]) / dz;
+    if (u >= R(0.0)) f = cdv(u * (q[0] - q[-sI]), C.d_dx);
+    else f = cdv(u * (q[sI] - q[0]), C.d_dx);
+    if (v >= R(0.0)) f += cdv(v * (q[0] - q[-sJ]), C.d_dy);
+    else f += cdv(v * (q[sJ] - q[0]), C.d_dy);
+    if (w >= R(0.0)) f += cdv(w * (q[0] - q[-1]), C.d_dz);
+    else f += cdv(w * (q[1] - q[0]), C.d_dz);
     return f;
 }
 
 // calculate_convection_muscl (:2037-2159)
 template <typename R>
-__device__ __forceinline__ R conv_muscl(const R* __restrict__ phi, size_t id, size_t sI, size_t sJ, bool band2, R u, R v,
-                                        R w, R dx, R dy, R dz) {
-    if (band2) return upwind3<R>(phi, id, sI, sJ, u, v, w, dx, dy, dz);
-    R cx = muscl_axis<R>(u, phi[id - 2 * sI], phi[id - sI], phi[id], phi[id + sI], phi[id + 2 * sI], dx);
-    R cy = muscl_axis<R>(v, phi[id - 2 * sJ], phi[id - sJ], phi[id], phi[id + sJ], phi[id + 2 * sJ], dy);
-    R cz = muscl_axis<R>(w, phi[id - 2], phi[id - 1], phi[id], phi[id + 1], phi[id + 2], dz);
+__device__ __forceinline__ R conv_muscl(const Consts& C, const R* __restrict__ q, ptrdiff_t sI, ptrdiff_t sJ, bool band2,
+                                        R u, R v, R w) {
+    if (band2) return upwind3<R>(C, q, sI, sJ, u, v, w);
+    R cx = muscl_axis<R>(u, q[-2 * sI], q[-sI], q[0], q[sI], q[2 * sI], C.d_dx);
+    R cy = muscl_axis<R>(v, q[-2 * sJ], q[-sJ], q[0], q[sJ], q[2 * sJ], C.d_dy);
+    R cz = muscl_axis<R>(w, q[-2], q[-1], q[0], q[1], q[2], C.d_dz);
     return cx + cy + cz;
 }
 
 // Face-averaged SGS diffusion div((nu_t/Sc) grad phi) (:2751-2760, :2853-2860, :2932-2939).
+// The six face coefficients depend only on nu_t, so they are computed once per cell.
 template <typename R>
-__device__ __forceinline__ R sgs_div(const R* __restrict__ phi, const R* __restrict__ nut, size_t id, size_t sI, size_t sJ,
-                                     R c2, R dx, R dy, R dz) {
-    R n0 = nut[id];
-    R g_iph = (nut[id + sI] + n0) / c2, g_imh = (n0 + nut[id - sI]) / c2;
-    R g_jph = (nut[id + sJ] + n0) / c2, g_jmh = (n0 + nut[id - sJ]) / c2;
-    R g_kph = (nut[id + 1] + n0) / c2, g_kmh = (n0 + nut[id - 1]) / c2;
-    R p0 = phi[id];
-    R sx = (g_iph * (phi[id + sI] - p0) / dx - g_imh * (p0 - phi[id - sI]) / dx) / dx;
-    R sy = (g_jph * (phi[id + sJ] - p0) / dy - g_jmh * (p0 - phi[id - sJ]) / dy) / dy;
-    R sz = (g_kph * (phi[id + 1] - p0) / dz - g_kmh * (p0 - phi[id - 1]) / dz) / dz;
+struct SgsFaces {
+    R iph, imh, jph, jmh, kph, kmh;
+};
+template <typename R>
+__device__ __forceinline__ SgsFaces<R> sgs_faces(const R* __restrict__ nut, ptrdiff_t sI, ptrdiff_t sJ, const DC& c2) {
+    R n0 = nut[0];
+    SgsFaces<R> g;
+    g.iph = cdv(nut[sI] + n0, c2); g.imh = cdv(n0 + nut[-sI], c2);
+    g.jph = cdv(nut[sJ] + n0, c2); g.jmh = cdv(n0 + nut[-sJ], c2);
+    g.kph = cdv(nut[1] + n0, c2); g.kmh = cdv(n0 + nut[-1], c2);
+    return g;
+}
+template <typename R>
+__device__ __forceinline__ R sgs_div(const Consts& C, const R* __restrict__ q, const SgsFaces<R>& g, ptrdiff_t sI,
+                                     ptrdiff_t sJ) {
+    R p0 = q[0];
+    R sx = cdv(cdv(g.iph * (q[sI] - p0), C.d_dx) - cdv(g.imh * (p0 - q[-sI]), C.d_dx), C.d_dx);
+    R sy = cdv(cdv(g.jph * (q[sJ] - p0), C.d_dy) - cdv(g.jmh * (p0 - q[-sJ]), C.d_dy), C.d_dy);
+    R sz = cdv(cdv(g.kph * (q[1] - p0), C.d_dz) - cdv(g.kmh * (p0 - q[-1]), C.d_dz), C.d_dz);
     return sx + sy + sz;
 }
 
 template <typename R>
-__device__ __forceinline__ R lap3(const R* __restrict__ phi, size_t id, size_t sI, size_t sJ, R dxx, R dyy, R dzz) {
-    R p0 = phi[id];
-    R a = (phi[id + sI] - R(2.0) * p0 + phi[id - sI]) / dxx;
-    R b = (phi[id + sJ] - R(2.0) * p0 + phi[id - sJ]) / dyy;
-    R c = (phi[id + 1] - R(2.0) * p0 + phi[id - 1]) / dzz;
+__device__ __forceinline__ R lap3(const Consts& C, const R* __restrict__ q, ptrdiff_t sI, ptrdiff_t sJ) {
+    R p0 = q[0];
+    R a = cdv(q[sI] - R(2.0) * p0 + q[-sI], C.d_dxx);
+    R b = cdv(q[sJ] - R(2.0) * p0 + q[-sJ], C.d_dyy);
+    R c = cdv(q[1] - R(2.0) * p0 + q[-1], C.d_dzz);
     return a + b + c;
 }
 
-// stage: 0,1,2 -> intermediate stage with coefficient 0.5/0.5/1.0, 3 -> final combine.
+// C1: momentum (:2552-2697) with calculate_convection_conservative (:683-727) and the G
+// equation (:2706-2825).  Writes k_rhou, k_rhov, k_rhow, k_G of fluid cells.
 template <typename R>
-__global__ void __launch_bounds__(NT) k_rhs_combine(const Consts* __restrict__ C, const uint8_t* __restrict__ attr,
-                                                    F11<R> F, PropBuf<R> P, F11<R> S0, F11<R> St, AccBuf<R> acc,
-                                                    KDbg<R> kd, const Scalars* __restrict__ Sc, double dt, int stage,
-                                                    int t_loop) {
-    const int nx = C->nx, ny = C->ny, nz = C->nz;
+__global__ void __launch_bounds__(NT, 2)
+    k_rhs_flow(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> F, PropBuf<R> P, KFlow<R> kf,
+               KDbg<R> kd, const Scalars* __restrict__ Sc, int t_loop) {
+    const int nx = C.nx, ny = C.ny, nz = C.nz;
     const int k = blockIdx.x * BX + threadIdx.x;
     const int j = blockIdx.y * BY + threadIdx.y;
     const int i = blockIdx.z;
     if (k >= nz || j >= ny) return;
-    const size_t sI = (size_t)ny * nz, sJ = (size_t)nz;
+    const ptrdiff_t sI = (ptrdiff_t)ny * nz, sJ = (ptrdiff_t)nz;
+    const size_t id = cid(i, j, k, ny, nz);
+    if (attr[id] != 3) return;
+    const R* __restrict__ uf = F.p[0] + id;
+    const R* __restrict__ vf = F.p[1] + id;
+    const R* __restrict__ wf = F.p[2] + id;
+    const R* __restrict__ Gf = F.p[4] + id;
+    const R* __restrict__ rf = F.p[5] + id;
+    const R u0 = uf[0], v0 = vf[0], w0 = wf[0];
+    const bool band2 = (i < 2 || i >= nx - 2 || j < 2 || j >= ny - 2 || k < 2 || k >= nz - 2);
+    const bool band3 = (i < 3 || i >= nx - 3 || j < 3 || j >= ny - 3 || k < 3 || k >= nz - 3);
+    R kmom[3];
+    {
+        const R r0 = rf[0];
+        // face mass fluxes; in the near-face band the reference writes 0.5*(a+b)*0.5*(c+d),
+        // in the interior (0.5*(a+b))*(0.5*(c+d)) -- equal values, since scaling by 0.5 is exact
+        R mf_iph = (R(0.5) * (rf[sI] + r0)) * (R(0.5) * (uf[sI] + u0));
+        R mf_imh = (R(0.5) * (r0 + rf[-sI])) * (R(0.5) * (u0 + uf[-sI]));
+        R mf_jph = (R(0.5) * (rf[sJ] + r0)) * (R(0.5) * (vf[sJ] + v0));
+        R mf_jmh = (R(0.5) * (r0 + rf[-sJ])) * (R(0.5) * (v0 + vf[-sJ]));
+        R mf_kph = (R(0.5) * (rf[1] + r0)) * (R(0.5) * (wf[1] + w0));
+        R mf_kmh = (R(0.5) * (r0 + rf[-1])) * (R(0.5) * (w0 + wf[-1]));
+        const R mu_eff = P.mu_eff[id];
+        const R* comps[3] = {uf, vf, wf};
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            const R* __restrict__ ph = comps[q];
+            R pc = ph[0];
+            R p_iph, p_imh, p_jph, p_jmh, p_kph, p_kmh;
+            if (band2) {
+                p_iph = (mf_iph > R(0)) ? pc : ph[sI];
+                p_imh = (mf_imh > R(0)) ? ph[-sI] : pc;
+                p_jph = (mf_jph > R(0)) ? pc : ph[sJ];
+                p_jmh = (mf_jmh > R(0)) ? ph[-sJ] : pc;
+                p_kph = (mf_kph > R(0)) ? pc : ph[1];
+                p_kmh = (mf_kmh > R(0)) ? ph[-1] : pc;
+            } else {
+                // With the reference's face coefficients UW2 = 0, UW1 = DW1 = 0.5 (:164-166)
+                // both upwind branches give 0.5*phi_L + 0.5*phi_R, so no branch is taken.
+                p_iph = R(0.5) * pc + R(0.5) * ph[sI];
+                p_imh = R(0.5) * ph[-sI] + R(0.5) * pc;
+                p_jph = R(0.5) * pc + R(0.5) * ph[sJ];
+                p_jmh = R(0.5) * ph[-sJ] + R(0.5) * pc;
+                p_kph = R(0.5) * pc + R(0.5) * ph[1];
+                p_kmh = R(0.5) * ph[-1] + R(0.5) * pc;
+            }
+            R conv = cdv(mf_iph * p_iph - mf_imh * p_imh, C.d_dx) + cdv(mf_jph * p_jph - mf_jmh * p_jmh, C.d_dy) +
+                     cdv(mf_kph * p_kph - mf_kmh * p_kmh, C.d_dz);
+            kmom[q] = -conv + mu_eff * lap3<R>(C, ph, sI, sJ);
+        }
+        R grav = (r0 - (R)Sc->rho_avg) * R(G_GRAVITY);
+        R fx = R(0), fy = R(0), fz = R(0);
+        if (C.flame_accel) {
+            R Gl = Gf[0];
+            if (Gl > R(0.01) && Gl < R(0.99)) {
+                R dGx = cdv(Gf[sI] - Gf[-sI], C.d_2dx);
+                R dGy = cdv(Gf[sJ] - Gf[-sJ], C.d_2dy);
+                R dGz = cdv(Gf[1] - Gf[-1], C.d_2dz);
+                if (dGx < R(0.0)) dGx = R(0.0);
+                if (dGy < R(0.0)) dGy = R(0.0);
+                R zrel = ((R)k * (R)C.dz) - (R)C.inlet_center_z;
+                if (zrel > R(0.0)) {
+                    if (dGz < R(0.0)) dGz = R(0.0);
+                } else {
+                    if (dGz > R(0.0)) dGz = R(0.0);
+                }
+                R df = Gl - (R)C.accel_center;
+                R window = exp(cdv(-(df * df), C.d_w2));
+                // tip_mask is the literal 1.0 in the momentum source (:2638)
+                R cf = (R)C.accel_strength * r0 * window * R(1.0);
+                fx = cf * dGx * R(0.05);
+                fy = cf * dGy * R(1.0);
+                fz = cf * dGz * R(1.0);
+                R zp = (R)k * (R)C.dz, ramp = R(1.0);
+                if (zp < R(RAMP_DIST)) ramp = cdv(zp, C.d_ramp);
+                fx *= ramp; fy *= ramp; fz *= ramp;
+            }
+        }
+        const R lim = R(FORCE_LIMIT);
+        if (fx > lim) fx = lim;
+        if (fx < -lim) fx = -lim;
+        if (fy > lim) fy = lim;
+        if (fy < -lim) fy = -lim;
+        if (fz > lim) fz = lim;
+        if (fz < -lim) fz = -lim;
+        kmom[0] = kmom[0] + grav + fx;
+        kmom[1] = kmom[1] + fy;
+        kmom[2] = kmom[2] + fz;
+    }
+    R kG;
+    {
+        R conv;
+        if (band3) {
+            if (band2) {
+                conv = upwind3<R>(C, Gf, sI, sJ, u0, v0, w0);
+            } else {
+                // calculate_convection_non_conservative interior branch (:652-677); the
+                // zero UW2 coefficient again makes both upwind branches identical.
+                R pc = Gf[0];
+                R p_iph = R(0.5) * pc + R(0.5) * Gf[sI], p_imh = R(0.5) * Gf[-sI] + R(0.5) * pc;
+                R p_jph = R(0.5) * pc + R(0.5) * Gf[sJ], p_jmh = R(0.5) * Gf[-sJ] + R(0.5) * pc;
+                R p_kph = R(0.5) * pc + R(0.5) * Gf[1], p_kmh = R(0.5) * Gf[-1] + R(0.5) * pc;
+                R cx = cdv(u0 * (p_iph - p_imh), C.d_dx);
+                R cy = cdv(v0 * (p_jph - p_jmh), C.d_dy);
+                R cz = cdv(w0 * (p_kph - p_kmh), C.d_dz);
+                conv = cx + cy + cz;
+            }
+        } else {
+            R fxa = teno_axis<R>(C, u0, Gf, sI, C.d_dx);
+            R fya = teno_axis<R>(C, v0, Gf, sJ, C.d_dy);
+            R fza = teno_axis<R>(C, w0, Gf, 1, C.d_dz);
+            conv = fxa + fya + fza;
+        }
+        SgsFaces<R> gf = sgs_faces<R>(P.nu_t + id, sI, sJ, C.d_sct2);
+        R sgs = sgs_div<R>(C, Gf, gf, sI, sJ);
+        R gx, gy, gz;
+        if (t_loop >= C.weno_step && !band3) {
+            gx = weno5_grad<R>(C, Gf, sI, C.d_dx);
+            gy = weno5_grad<R>(C, Gf, sJ, C.d_dy);
+            gz = weno5_grad<R>(C, Gf, 1, C.d_dz);
+        } else {
+            gx = cdv(Gf[sI] - Gf[-sI], C.d_2dx);
+            gy = cdv(Gf[sJ] - Gf[-sJ], C.d_2dy);
+            gz = cdv(Gf[1] - Gf[-1], C.d_2dz);
+        }
+        R gmag = sqrt(gx * gx + gy * gy + gz * gz);
+        R prop = P.ST[id] * gmag;
+        R art = R(0);
+        if (C.flame_accel) {
+            R Gl = Gf[0];
+            if (Gl > R(0.1) && Gl < R(0.99)) {
+                R df = Gl - (R)C.accel_center;
+                R window = exp(cdv(-(df * df), C.d_w2));
+                // tip_mask = 1 - exp(-r^2 / 0^2) is exactly 1 for every fluid cell (j >= 1)
+                // because TIP_PROTECTION_RADIUS is 0.0 (:234, :2806-2807).
+                R adc = R(5.0) * (P.nu_t[id] + R(1.0e-5)) * window * R(1.0);
+                art = adc * lap3<R>(C, Gf, sI, sJ);
+            }
+        }
+        kG = -conv + prop + sgs + art;
+    }
+    kf.p[0][id] = kmom[0];
+    kf.p[1][id] = kmom[1];
+    kf.p[2][id] = kmom[2];
+    kf.p[3][id] = kG;
+    if (kd.p[0]) {
+        kd.p[0][id] = kmom[0];
+        kd.p[1][id] = kmom[1];
+        kd.p[2][id] = kmom[2];
+        kd.p[4][id] = kG;
+    }
+}
+
+// C2: species (:2837-2904) and temperature (:2912-2962), then the RK4 bookkeeping.
+// stage: 0,1,2 -> intermediate stage with coefficient 0.5/0.5/1.0, 3 -> final combine.
+template <typename R>
+__global__ void __launch_bounds__(NT, 2)
+    k_rhs_scalar(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> F, PropBuf<R> P, F11<R> S0, F11<R> St,
+                 AccBuf<R> acc, KFlow<R> kf, KDbg<R> kd, double dt, int stage) {
+    const int nx = C.nx, ny = C.ny, nz = C.nz;
+    const int k = blockIdx.x * BX + threadIdx.x;
+    const int j = blockIdx.y * BY + threadIdx.y;
+    const int i = blockIdx.z;
+    if (k >= nz || j >= ny) return;
+    const ptrdiff_t sI = (ptrdiff_t)ny * nz, sJ = (ptrdiff_t)nz;
     const size_t id = cid(i, j, k, ny, nz);
     const int a = attr[id];
 
@@ -565,232 +751,68 @@ __global__ void __launch_bounds__(NT) k_rhs_combine(const Consts* __restrict__ C
         return;
     }
 
-    const R dx = (R)C->dx, dy = (R)C->dy, dz = (R)C->dz;
-    const R dxx = (R)C->dxx, dyy = (R)C->dyy, dzz = (R)C->dzz;
-    const R* __restrict__ uf = F.p[0];
-    const R* __restrict__ vf = F.p[1];
-    const R* __restrict__ wf = F.p[2];
-    const R* __restrict__ Tf = F.p[3];
-    const R* __restrict__ Gf = F.p[4];
-    const R* __restrict__ rf = F.p[5];
-    const R* __restrict__ nut = P.nu_t;
-    const R u0 = uf[id], v0 = vf[id], w0 = wf[id];
+    const R u0 = F.p[0][id], v0 = F.p[1][id], w0 = F.p[2][id];
     const bool band2 = (i < 2 || i >= nx - 2 || j < 2 || j >= ny - 2 || k < 2 || k >= nz - 2);
-    const bool band3 = (i < 3 || i >= nx - 3 || j < 3 || j >= ny - 3 || k < 3 || k >= nz - 3);
     R kv[NACC];
-
-    // ---- momentum (:2552-2697) with calculate_convection_conservative (:683-727)
-    {
-        const R r0 = rf[id];
-        R cu, cv, cw;
-        if (band2) {
-            R mf_iph = R(0.5) * (rf[id + sI] + r0) * R(0.5) * (uf[id + sI] + u0);
-            R mf_imh = R(0.5) * (r0 + rf[id - sI]) * R(0.5) * (u0 + uf[id - sI]);
-            R mf_jph = R(0.5) * (rf[id + sJ] + r0) * R(0.5) * (vf[id + sJ] + v0);
-            R mf_jmh = R(0.5) * (r0 + rf[id - sJ]) * R(0.5) * (v0 + vf[id - sJ]);
-            R mf_kph = R(0.5) * (rf[id + 1] + r0) * R(0.5) * (wf[id + 1] + w0);
-            R mf_kmh = R(0.5) * (r0 + rf[id - 1]) * R(0.5) * (w0 + wf[id - 1]);
-            R cc[3];
-#pragma unroll
-            for (int q = 0; q < 3; q++) {
-                const R* __restrict__ ph = F.p[q];
-                R pc = ph[id];
-                R p_iph = (mf_iph > R(0)) ? pc : ph[id + sI];
-                R p_imh = (mf_imh > R(0)) ? ph[id - sI] : pc;
-                R p_jph = (mf_jph > R(0)) ? pc : ph[id + sJ];
-                R p_jmh = (mf_jmh > R(0)) ? ph[id - sJ] : pc;
-                R p_kph = (mf_kph > R(0)) ? pc : ph[id + 1];
-                R p_kmh = (mf_kmh > R(0)) ? ph[id - 1] : pc;
-                cc[q] = (mf_iph * p_iph - mf_imh * p_imh) / dx + (mf_jph * p_jph - mf_jmh * p_jmh) / dy +
-                        (mf_kph * p_kph - mf_kmh * p_kmh) / dz;
-            }
-            cu = cc[0]; cv = cc[1]; cw = cc[2];
-        } else {
-            R u_iph = R(0.5) * (uf[id + sI] + u0), u_imh = R(0.5) * (u0 + uf[id - sI]);
-            R v_jph = R(0.5) * (vf[id + sJ] + v0), v_jmh = R(0.5) * (v0 + vf[id - sJ]);
-            R w_kph = R(0.5) * (wf[id + 1] + w0), w_kmh = R(0.5) * (w0 + wf[id - 1]);
-            R r_iph = R(0.5) * (rf[id + sI] + r0), r_imh = R(0.5) * (r0 + rf[id - sI]);
-            R r_jph = R(0.5) * (rf[id + sJ] + r0), r_jmh = R(0.5) * (r0 + rf[id - sJ]);
-            R r_kph = R(0.5) * (rf[id + 1] + r0), r_kmh = R(0.5) * (r0 + rf[id - 1]);
-            R mf_iph = r_iph * u_iph, mf_imh = r_imh * u_imh;
-            R mf_jph = r_jph * v_jph, mf_jmh = r_jmh * v_jmh;
-            R mf_kph = r_kph * w_kph, mf_kmh = r_kmh * w_kmh;
-            R cc[3];
-#pragma unroll
-            for (int q = 0; q < 3; q++) {
-                const R* __restrict__ ph = F.p[q];
-                // With the reference's face coefficients UW2 = 0, UW1 = DW1 = 0.5 (:164-166)
-                // both upwind branches give 0.5*phi_L + 0.5*phi_R, so no branch is taken.
-                R pc = ph[id];
-                R p_iph = R(0.5) * pc + R(0.5) * ph[id + sI];
-                R p_imh = R(0.5) * ph[id - sI] + R(0.5) * pc;
-                R p_jph = R(0.5) * pc + R(0.5) * ph[id + sJ];
-                R p_jmh = R(0.5) * ph[id - sJ] + R(0.5) * pc;
-                R p_kph = R(0.5) * pc + R(0.5) * ph[id + 1];
-                R p_kmh = R(0.5) * ph[id - 1] + R(0.5) * pc;
-                cc[q] = (mf_iph * p_iph - mf_imh * p_imh) / dx + (mf_jph * p_jph - mf_jmh * p_jmh) / dy +
-                        (mf_kph * p_kph - mf_kmh * p_kmh) / dz;
-            }
-            cu = cc[0]; cv = cc[1]; cw = cc[2];
-        }
-        const R mu_eff = P.mu_eff[id];
-        R diff_u = mu_eff * lap3<R>(uf, id, sI, sJ, dxx, dyy, dzz);
-        R diff_v = mu_eff * lap3<R>(vf, id, sI, sJ, dxx, dyy, dzz);
-        R diff_w = mu_eff * lap3<R>(wf, id, sI, sJ, dxx, dyy, dzz);
-        R grav = (r0 - (R)Sc->rho_avg) * R(G_GRAVITY);
-        R fx = R(0), fy = R(0), fz = R(0);
-        if (C->flame_accel) {
-            R Gl = Gf[id];
-            if (Gl > R(0.01) && Gl < R(0.99)) {
-                R dGx = (Gf[id + sI] - Gf[id - sI]) / (R)C->two_dx;
-                R dGy = (Gf[id + sJ] - Gf[id - sJ]) / (R)C->two_dy;
-                R dGz = (Gf[id + 1] - Gf[id - 1]) / (R)C->two_dz;
-                if (dGx < R(0.0)) dGx = R(0.0);
-                if (dGy < R(0.0)) dGy = R(0.0);
-                R zrel = ((R)k * dz) - (R)C->inlet_center_z;
-                if (zrel > R(0.0)) {
-                    if (dGz < R(0.0)) dGz = R(0.0);
-                } else {
-                    if (dGz > R(0.0)) dGz = R(0.0);
-                }
-                R df = Gl - (R)C->accel_center;
-                R window = exp(-(df * df) / (R)C->two_w2);
-                // tip_mask is the literal 1.0 in the momentum source (:2638)
-                R cf = (R)C->accel_strength * r0 * window * R(1.0);
-                fx = cf * dGx * R(0.05);
-                fy = cf * dGy * R(1.0);
-                fz = cf * dGz * R(1.0);
-                R zp = (R)k * dz, ramp = R(1.0);
-                if (zp < R(RAMP_DIST)) ramp = zp / R(RAMP_DIST);
-                fx *= ramp; fy *= ramp; fz *= ramp;
-            }
-        }
-        const R lim = R(FORCE_LIMIT);
-        if (fx > lim) fx = lim;
-        if (fx < -lim) fx = -lim;
-        if (fy > lim) fy = lim;
-        if (fy < -lim) fy = -lim;
-        if (fz > lim) fz = lim;
-        if (fz < -lim) fz = -lim;
-        kv[0] = -cu + diff_u + grav + fx;
-        kv[1] = -cv + diff_v + fy;
-        kv[2] = -cw + diff_w + fz;
-    }
-
-    // ---- G equation (:2706-2825)
-    {
-        R conv;
-        if (band3) {
-            if (band2) {
-                conv = upwind3<R>(Gf, id, sI, sJ, u0, v0, w0, dx, dy, dz);
-            } else {
-                // calculate_convection_non_conservative interior branch (:652-677); the
-                // zero UW2 coefficient again makes both upwind branches identical.
-                R pc = Gf[id];
-                R p_iph = R(0.5) * pc + R(0.5) * Gf[id + sI], p_imh = R(0.5) * Gf[id - sI] + R(0.5) * pc;
-                R p_jph = R(0.5) * pc + R(0.5) * Gf[id + sJ], p_jmh = R(0.5) * Gf[id - sJ] + R(0.5) * pc;
-                R p_kph = R(0.5) * pc + R(0.5) * Gf[id + 1], p_kmh = R(0.5) * Gf[id - 1] + R(0.5) * pc;
-                R cx = u0 * (p_iph - p_imh) / dx;
-                R cy = v0 * (p_jph - p_jmh) / dy;
-                R cz = w0 * (p_kph - p_kmh) / dz;
-                conv = cx + cy + cz;
-            }
-        } else {
-            R fxa = teno_axis<R>(u0, Gf, id, sI, dx);
-            R fya = teno_axis<R>(v0, Gf, id, sJ, dy);
-            R fza = teno_axis<R>(w0, Gf, id, 1, dz);
-            conv = fxa + fya + fza;
-        }
-        R sgs = sgs_div<R>(Gf, nut, id, sI, sJ, (R)C->sc_t2, dx, dy, dz);
-        R gx, gy, gz;
-        if (t_loop >= C->weno_step && !band3) {
-            gx = weno5_grad<R>(Gf, id, sI, dx);
-            gy = weno5_grad<R>(Gf, id, sJ, dy);
-            gz = weno5_grad<R>(Gf, id, 1, dz);
-        } else {
-            gx = (Gf[id + sI] - Gf[id - sI]) / (R)C->two_dx;
-            gy = (Gf[id + sJ] - Gf[id - sJ]) / (R)C->two_dy;
-            gz = (Gf[id + 1] - Gf[id - 1]) / (R)C->two_dz;
-        }
-        R gmag = sqrt(gx * gx + gy * gy + gz * gz);
-        R prop = P.ST[id] * gmag;
-        R art = R(0);
-        if (C->flame_accel) {
-            R Gl = Gf[id];
-            if (Gl > R(0.1) && Gl < R(0.99)) {
-                R df = Gl - (R)C->accel_center;
-                R window = exp(-(df * df) / (R)C->two_w2);
-                R d2x = (Gf[id + sI] - R(2.0) * Gl + Gf[id - sI]) / dxx;
-                R d2y = (Gf[id + sJ] - R(2.0) * Gl + Gf[id - sJ]) / dyy;
-                R d2z = (Gf[id + 1] - R(2.0) * Gl + Gf[id - 1]) / dzz;
-                // tip_mask = 1 - exp(-r^2 / 0^2) is exactly 1 for every fluid cell (j >= 1)
-                // because TIP_PROTECTION_RADIUS is 0.0 (:234, :2806-2807).
-                R adc = R(5.0) * (nut[id] + R(1.0e-5)) * window * R(1.0);
-                art = adc * (d2x + d2y + d2z);
-            }
-        }
-        kv[4] = -conv + prop + sgs + art;
-    }
-
-    // ---- species (:2837-2904) and temperature (:2912-2962)
-    R g = Gf[id];
+    R g = F.p[4][id];
     if (g < R(0.0)) g = R(0.0);
     if (g > R(1.0)) g = R(1.0);
-    {
-        const R relax = (R)C->relax;
+    const SgsFaces<R> gs = sgs_faces<R>(P.nu_t + id, sI, sJ, C.d_sct2);
+    const R relax = (R)C.relax;
 #pragma unroll
-        for (int s = 0; s < NSP; s++) {
-            const R* __restrict__ Yf = F.p[6 + s];
-            R conv = conv_muscl<R>(Yf, id, sI, sJ, band2, u0, v0, w0, dx, dy, dz);
-            R mol = P.D[s][id] * lap3<R>(Yf, id, sI, sJ, dxx, dyy, dzz);
-            R sgs = sgs_div<R>(Yf, nut, id, sI, sJ, (R)C->sc_t2, dx, dy, dz);
-            R tgt;
-            if (s == C3H8) tgt = (R)C->inletYk[C3H8] * (R(1.0) - g);
-            else if (s == O2) tgt = fmax(R(0.0), (R)C->inletYk[O2] - (R)C->cons_o2 * g);
-            else if (s == CO2) tgt = (R)C->inletYk[CO2] + (R)C->prod_co2 * g;
-            else if (s == H2O) tgt = (R)C->inletYk[H2O] + (R)C->prod_h2o * g;
-            else tgt = (R)C->inletYk[N2];
-            R nud = relax * (tgt - Yf[id]);
-            kv[5 + s] = -conv + mol + sgs + nud;
-        }
-        R conv = conv_muscl<R>(Tf, id, sI, sJ, band2, u0, v0, w0, dx, dy, dz);
-        R mol = P.aT[id] * lap3<R>(Tf, id, sI, sJ, dxx, dyy, dzz);
-        R sgs = sgs_div<R>(Tf, nut, id, sI, sJ, (R)C->pr_t2, dx, dy, dz);
-        R Tt = (R)C->t_in + g * (R)C->t_burnt_span;
-        R nud = relax * (Tt - Tf[id]);
+    for (int s = 0; s < NSP; s++) {
+        const R* __restrict__ Yf = F.p[6 + s] + id;
+        R conv = conv_muscl<R>(C, Yf, sI, sJ, band2, u0, v0, w0);
+        R mol = P.D[s][id] * lap3<R>(C, Yf, sI, sJ);
+        R sgs = sgs_div<R>(C, Yf, gs, sI, sJ);
+        R tgt;
+        if (s == C3H8) tgt = (R)C.inletYk[C3H8] * (R(1.0) - g);
+        else if (s == O2) tgt = fmax(R(0.0), (R)C.inletYk[O2] - (R)C.cons_o2 * g);
+        else if (s == CO2) tgt = (R)C.inletYk[CO2] + (R)C.prod_co2 * g;
+        else if (s == H2O) tgt = (R)C.inletYk[H2O] + (R)C.prod_h2o * g;
+        else tgt = (R)C.inletYk[N2];
+        R nud = relax * (tgt - Yf[0]);
+        kv[5 + s] = -conv + mol + sgs + nud;
+    }
+    {
+        const R* __restrict__ Tf = F.p[3] + id;
+        R conv = conv_muscl<R>(C, Tf, sI, sJ, band2, u0, v0, w0);
+        R mol = P.aT[id] * lap3<R>(C, Tf, sI, sJ);
+        const SgsFaces<R> gt = sgs_faces<R>(P.nu_t + id, sI, sJ, C.d_prt2);
+        R sgs = sgs_div<R>(C, Tf, gt, sI, sJ);
+        R Tt = (R)C.t_in + g * (R)C.t_burnt_span;
+        R nud = relax * (Tt - Tf[0]);
         kv[3] = -conv + mol + sgs + nud;
     }
+    kv[0] = kf.p[0][id];
+    kv[1] = kf.p[1][id];
+    kv[2] = kf.p[2][id];
+    kv[4] = kf.p[3][id];
     if (kd.p[0]) {
+        kd.p[3][id] = kv[3];
 #pragma unroll
-        for (int q = 0; q < NACC; q++) kd.p[q][id] = kv[q];
+        for (int s = 0; s < NSP; s++) kd.p[5 + s][id] = kv[5 + s];
     }
 
     // ---- RK4 bookkeeping.  acc holds k1, k1 + 2k2, (k1 + 2k2) + 2k3: exactly the
     // left-to-right partial sums of k1 + 2.0*k2 + 2.0*k3 + k4 (:4520).
-    R tot[NACC];
+    const bool fin = (stage == 3);
+    R incr[NACC];
     if (stage == 0) {
 #pragma unroll
-        for (int q = 0; q < NACC; q++) { tot[q] = kv[q]; acc.p[q][id] = kv[q]; }
+        for (int q = 0; q < NACC; q++) { incr[q] = kv[q]; acc.p[q][id] = kv[q]; }
     } else if (stage < 3) {
 #pragma unroll
-        for (int q = 0; q < NACC; q++) { tot[q] = acc.p[q][id] + R(2.0) * kv[q]; acc.p[q][id] = tot[q]; }
+        for (int q = 0; q < NACC; q++) { incr[q] = kv[q]; acc.p[q][id] = acc.p[q][id] + R(2.0) * kv[q]; }
     } else {
 #pragma unroll
-        for (int q = 0; q < NACC; q++) tot[q] = acc.p[q][id] + kv[q];
+        for (int q = 0; q < NACC; q++) incr[q] = acc.p[q][id] + kv[q];
     }
-    const R rho_n = S0.p[5][id];
-    const R T0 = S0.p[3][id], G0 = S0.p[4][id];
-    R mom0[3];
-#pragma unroll
-    for (int q = 0; q < 3; q++) mom0[q] = rho_n * S0.p[q][id];   // rhou = rho*u after the BC (:3146)
-    R Y[NSP];
-    const bool fin = (stage == 3);
     const R cdt = fin ? (R)(dt / 6.0) : (R)((stage == 2 ? 1.0 : 0.5) * dt);
-    R incr[NACC];
-#pragma unroll
-    for (int q = 0; q < NACC; q++) incr[q] = fin ? tot[q] : kv[q];
-    R Tn = T0 + cdt * incr[3];
-    R Gn = G0 + cdt * incr[4];
+    const R rho_n = S0.p[5][id];
+    R Tn = S0.p[3][id] + cdt * incr[3];
+    R Gn = S0.p[4][id] + cdt * incr[4];
+    R Y[NSP];
 #pragma unroll
     for (int s = 0; s < NSP; s++) Y[s] = S0.p[6 + s][id] + cdt * incr[5 + s];
     Tn = fmax(R(200.0), fmin(R(3000.0), Tn));
@@ -809,7 +831,7 @@ __global__ void __launch_bounds__(NT) k_rhs_combine(const Consts* __restrict__ C
     R vel[3];
 #pragma unroll
     for (int q = 0; q < 3; q++) {
-        R m = mom0[q] + cdt * incr[q];
+        R m = rho_n * S0.p[q][id] + cdt * incr[q];   // rhou = rho*u after the BC (:3146)
         vel[q] = (rn > R(SMALL)) ? m / rn : R(0);
     }
     R* const* out = fin ? S0.p : St.p;
@@ -835,18 +857,18 @@ __device__ __forceinline__ void copy_cell(F11<R>& S, size_t dst, size_t src) {
         if (q != 5) S.p[q][dst] = S.p[q][src];
 }
 template <typename R>
-__device__ __forceinline__ void ambient_cell(const Consts* __restrict__ C, F11<R>& S, size_t dst) {
+__device__ __forceinline__ void ambient_cell(const Consts& C, F11<R>& S, size_t dst) {
     S.p[0][dst] = R(0); S.p[1][dst] = R(0); S.p[2][dst] = R(0);
-    S.p[3][dst] = (R)C->t_amb; S.p[4][dst] = R(0);
+    S.p[3][dst] = (R)C.t_amb; S.p[4][dst] = R(0);
 #pragma unroll
-    for (int s = 0; s < NSP; s++) S.p[6 + s][dst] = (R)C->ambientYk[s];
+    for (int s = 0; s < NSP; s++) S.p[6 + s][dst] = (R)C.ambientYk[s];
 }
 
 template <typename R>
-__global__ void k_bc_iface(const Consts* __restrict__ C, const uint8_t* __restrict__ attr, F11<R> S,
+__global__ void k_bc_iface(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> S,
                            const double* __restrict__ plane, const double* __restrict__ noise,
                            const int* __restrict__ inlet_pos) {
-    const int nx = C->nx, ny = C->ny, nz = C->nz;
+    const int nx = C.nx, ny = C.ny, nz = C.nz;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
     if (k >= nz) return;
@@ -856,15 +878,15 @@ __global__ void k_bc_iface(const Consts* __restrict__ C, const uint8_t* __restri
         const size_t p = (size_t)j * nz + k;
         const size_t npl = (size_t)ny * nz;
         const int q = inlet_pos[p];
-        const R amp = (R)C->noise_amp;
+        const R amp = (R)C.noise_amp;
         R r1 = (R)noise[3 * q + 0], r2 = (R)noise[3 * q + 1], r3 = (R)noise[3 * q + 2];
-        S.p[0][i0] = fmax(R(0.0), (R)C->u_in + (R)plane[p] + amp * r1);
+        S.p[0][i0] = fmax(R(0.0), (R)C.u_in + (R)plane[p] + amp * r1);
         S.p[1][i0] = (R)plane[npl + p] + amp * r2;
         S.p[2][i0] = (R)plane[2 * npl + p] + amp * r3;
-        S.p[3][i0] = (R)C->t_in;
+        S.p[3][i0] = (R)C.t_in;
         S.p[4][i0] = R(0);
 #pragma unroll
-        for (int s = 0; s < NSP; s++) S.p[6 + s][i0] = (R)C->inletYk[s];
+        for (int s = 0; s < NSP; s++) S.p[6 + s][i0] = (R)C.inletYk[s];
     } else if (a0 == 4) {
         if (S.p[0][i1] < R(0)) ambient_cell<R>(C, S, i0);
         else copy_cell<R>(S, i0, i1);
@@ -880,8 +902,8 @@ __global__ void k_bc_iface(const Consts* __restrict__ C, const uint8_t* __restri
 }
 
 template <typename R>
-__global__ void k_bc_jface(const Consts* __restrict__ C, const uint8_t* __restrict__ attr, F11<R> S) {
-    const int ny = C->ny, nz = C->nz;
+__global__ void k_bc_jface(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> S) {
+    const int ny = C.ny, nz = C.nz;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = blockIdx.y + 1;
     if (k >= nz) return;
@@ -903,8 +925,8 @@ __global__ void k_bc_jface(const Consts* __restrict__ C, const uint8_t* __restri
 }
 
 template <typename R>
-__global__ void k_bc_kface(const Consts* __restrict__ C, const uint8_t* __restrict__ attr, F11<R> S) {
-    const int ny = C->ny, nz = C->nz;
+__global__ void k_bc_kface(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> S) {
+    const int ny = C.ny, nz = C.nz;
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = blockIdx.y + 1;
     if (j >= ny) return;
@@ -923,11 +945,11 @@ __global__ void k_bc_kface(const Consts* __restrict__ C, const uint8_t* __restri
 // EOS + renormalisation everywhere (:3130-3160) fused with the max-velocity reduction
 // over inlet/fluid cells for the next dt (:1472-1485).
 template <typename R>
-__global__ void __launch_bounds__(NT) k_bc_eos(const Consts* __restrict__ C, const uint8_t* __restrict__ attr, F11<R> S,
+__global__ void __launch_bounds__(NT) k_bc_eos(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> S,
                                                double* __restrict__ part, Scalars* __restrict__ Sc) {
     __shared__ double sh[NT / 32];
     __shared__ bool last;
-    const int ny = C->ny, nz = C->nz;
+    const int ny = C.ny, nz = C.nz;
     const int k = blockIdx.x * BX + threadIdx.x;
     const int j = blockIdx.y * BY + threadIdx.y;
     const int i = blockIdx.z;
@@ -942,7 +964,7 @@ __global__ void __launch_bounds__(NT) k_bc_eos(const Consts* __restrict__ C, con
         R T = S.p[3][id];
         R syw = R(0);
 #pragma unroll
-        for (int s = 0; s < NSP; s++) syw += Y[s] / (R)C->mwk[s];
+        for (int s = 0; s < NSP; s++) syw += cdv(Y[s], C.d_mwk[s]);
         R rho = (syw > R(1e-9) && T > R(1.0)) ? (R)P_CONST / ((R)R_UNIV / (R(1.0) / syw) * T) : R(1.2);
         S.p[5][id] = rho;
         if (a == 3 || a == 2 || a == 5) {
@@ -983,11 +1005,11 @@ __global__ void __launch_bounds__(NT) k_bc_eos(const Consts* __restrict__ C, con
 
 // Max velocity over inlet/fluid cells without touching the state (after an upload).
 template <typename R>
-__global__ void __launch_bounds__(NT) k_umax(const Consts* __restrict__ C, const uint8_t* __restrict__ attr, F11<R> S,
+__global__ void __launch_bounds__(NT) k_umax(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> S,
                                              double* __restrict__ part, Scalars* __restrict__ Sc) {
     __shared__ double sh[NT / 32];
     __shared__ bool last;
-    const int ny = C->ny, nz = C->nz;
+    const int ny = C.ny, nz = C.nz;
     const int k = blockIdx.x * BX + threadIdx.x;
     const int j = blockIdx.y * BY + threadIdx.y;
     const int i = blockIdx.z;
@@ -1026,7 +1048,7 @@ __global__ void __launch_bounds__(NT) k_umax(const Consts* __restrict__ C, const
 // ------------------------------------------------------------------ diagnostics
 
 template <typename R>
-__global__ void __launch_bounds__(NT) k_monitor(const Consts* __restrict__ C, F11<R> S, double* __restrict__ part,
+__global__ void __launch_bounds__(NT) k_monitor(LES_KERNEL_CONSTS, F11<R> S, double* __restrict__ part,
                                                 Scalars* __restrict__ Sc, size_t n) {
     // write_monitor_log (:3884-3897)
     __shared__ double sh[NT / 32];
@@ -1035,7 +1057,7 @@ __global__ void __launch_bounds__(NT) k_monitor(const Consts* __restrict__ C, F1
     double mass = 0.0, tmin = 1.0e9, tmax = -1.0e9, gmin = 1.0e9, gmax = -1.0e9, ymin = 1.0e9;
     for (size_t id = (size_t)blockIdx.x * NT + tid; id < n; id += (size_t)gridDim.x * NT) {
         double r = (double)S.p[5][id], T = (double)S.p[3][id], G = (double)S.p[4][id], Y = (double)S.p[6][id];
-        mass += ((r * C->dx) * C->dy) * C->dz;
+        mass += ((r * C.dx) * C.dy) * C.dz;
         tmin = fmin(tmin, T); tmax = fmax(tmax, T);
         gmin = fmin(gmin, G); gmax = fmax(gmax, G);
         ymin = fmin(ymin, Y);
@@ -1080,9 +1102,9 @@ __global__ void __launch_bounds__(NT) k_monitor(const Consts* __restrict__ C, F1
 }
 
 template <typename R>
-__global__ void k_probe(const Consts* __restrict__ C, F11<R> S, PropBuf<R> P, const int* __restrict__ st, int n,
-                        int kline, double* __restrict__ out) {
-    const int ny = C->ny, nz = C->nz;
+__global__ void k_probe(LES_KERNEL_CONSTS, F11<R> S, PropBuf<R> P, const int* __restrict__ st, int n, int kline,
+                        double* __restrict__ out) {
+    const int ny = C.ny, nz = C.nz;
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int q = blockIdx.y;
     if (j >= ny || q >= n) return;

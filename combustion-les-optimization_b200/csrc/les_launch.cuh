@@ -47,6 +47,8 @@ cudaError_t step_impl(DevCtx& c, double dt, int t_loop) {
     for (int q = 0; q < NACC; q++) kd.p[q] = c.debug ? (R*)c.kd[q] : nullptr;
     KDbg<R> knone;
     for (int q = 0; q < NACC; q++) knone.p[q] = nullptr;
+    KFlow<R> kf;
+    for (int q = 0; q < 4; q++) kf.p[q] = (R*)c.kflow[q];
 
     // SEM inflow plane (:943-1075)
     int tm = tmark_begin(c, 0);
@@ -56,27 +58,31 @@ cudaError_t step_impl(DevCtx& c, double dt, int t_loop) {
     for (int s = 0; s < 4; s++) {
         F11<R> in = (s == 0) ? S : St;
         tm = tmark_begin(c, 1);
-        k_filter_props<R><<<g, b, 0, st>>>(c.dC, c.attr, in, F, P, c.part, c.dS, s == 3 ? 1 : 0);
+        k_filter_props<R><<<g, b, 0, st>>>(c.hC, c.attr, in, F, P, c.part, c.dS, s == 3 ? 1 : 0);
         tmark_end(c, tm);
         tm = tmark_begin(c, 2);
-        k_strain<R><<<g, b, 0, st>>>(c.dC, c.attr, F, P);
+        k_strain<R><<<g, b, 0, st>>>(c.hC, c.attr, F, P);
         tmark_end(c, tm);
         // the k-arrays of the first stage are kept for inspection when requested
+        const KDbg<R>& kds = (s == 0) ? kd : knone;
         tm = tmark_begin(c, 3);
-        k_rhs_combine<R><<<g, b, 0, st>>>(c.dC, c.attr, F, P, S, St, acc, s == 0 ? kd : knone, c.dS, dt, s, t_loop);
+        k_rhs_flow<R><<<g, b, 0, st>>>(c.hC, c.attr, F, P, kf, kds, c.dS, t_loop);
+        tmark_end(c, tm);
+        tm = tmark_begin(c, 5);
+        k_rhs_scalar<R><<<g, b, 0, st>>>(c.hC, c.attr, F, P, S, St, acc, kf, kds, dt, s);
         tmark_end(c, tm);
     }
     // apply_boundary_conditions (:2967-3161)
     tm = tmark_begin(c, 4);
     {
         const int tpb = 128;
-        k_bc_iface<R><<<dim3((c.nz + tpb - 1) / tpb, c.ny), tpb, 0, st>>>(c.dC, c.attr, S, c.plane, c.noise,
+        k_bc_iface<R><<<dim3((c.nz + tpb - 1) / tpb, c.ny), tpb, 0, st>>>(c.hC, c.attr, S, c.plane, c.noise,
                                                                             c.inlet_pos);
         if (c.nx > 2) {
-            k_bc_jface<R><<<dim3((c.nz + tpb - 1) / tpb, c.nx - 2), tpb, 0, st>>>(c.dC, c.attr, S);
-            k_bc_kface<R><<<dim3((c.ny + tpb - 1) / tpb, c.nx - 2), tpb, 0, st>>>(c.dC, c.attr, S);
+            k_bc_jface<R><<<dim3((c.nz + tpb - 1) / tpb, c.nx - 2), tpb, 0, st>>>(c.hC, c.attr, S);
+            k_bc_kface<R><<<dim3((c.ny + tpb - 1) / tpb, c.nx - 2), tpb, 0, st>>>(c.hC, c.attr, S);
         }
-        k_bc_eos<R><<<g, b, 0, st>>>(c.dC, c.attr, S, c.part, c.dS);
+        k_bc_eos<R><<<g, b, 0, st>>>(c.hC, c.attr, S, c.part, c.dS);
     }
     tmark_end(c, tm);
     tmark_flush(c);
@@ -95,29 +101,32 @@ cudaError_t rhs_only_impl(DevCtx& c, int t_loop) {
     for (int q = 0; q < NACC; q++) acc.p[q] = (R*)c.acc[q];
     KDbg<R> kd;
     for (int q = 0; q < NACC; q++) kd.p[q] = (R*)c.kd[q];
-    k_filter_props<R><<<g, b, 0, st>>>(c.dC, c.attr, S, F, P, c.part, c.dS, 1);
-    k_strain<R><<<g, b, 0, st>>>(c.dC, c.attr, F, P);
-    k_rhs_combine<R><<<g, b, 0, st>>>(c.dC, c.attr, F, P, S, St, acc, kd, c.dS, 0.0, 0, t_loop);
+    KFlow<R> kf;
+    for (int q = 0; q < 4; q++) kf.p[q] = (R*)c.kflow[q];
+    k_filter_props<R><<<g, b, 0, st>>>(c.hC, c.attr, S, F, P, c.part, c.dS, 1);
+    k_strain<R><<<g, b, 0, st>>>(c.hC, c.attr, F, P);
+    k_rhs_flow<R><<<g, b, 0, st>>>(c.hC, c.attr, F, P, kf, kd, c.dS, t_loop);
+    k_rhs_scalar<R><<<g, b, 0, st>>>(c.hC, c.attr, F, P, S, St, acc, kf, kd, 0.0, 0);
     return cudaGetLastError();
 }
 
 template <typename R>
 cudaError_t umax_impl(DevCtx& c) {
-    k_umax<R><<<cell_grid(c), dim3(BX, BY), 0, c.stream>>>(c.dC, c.attr, f11<R>(c.S), c.part, c.dS);
+    k_umax<R><<<cell_grid(c), dim3(BX, BY), 0, c.stream>>>(c.hC, c.attr, f11<R>(c.S), c.part, c.dS);
     return cudaGetLastError();
 }
 
 template <typename R>
 cudaError_t monitor_impl(DevCtx& c) {
     const int nb = 592;   // 4 x 148 SMs
-    k_monitor<R><<<nb, NT, 0, c.stream>>>(c.dC, f11<R>(c.S), c.part, c.dS, c.n);
+    k_monitor<R><<<nb, NT, 0, c.stream>>>(c.hC, f11<R>(c.S), c.part, c.dS, c.n);
     return cudaGetLastError();
 }
 
 template <typename R>
 cudaError_t probe_impl(DevCtx& c, int n, int kline) {
     const int tpb = 64;
-    k_probe<R><<<dim3((c.ny + tpb - 1) / tpb, n), tpb, 0, c.stream>>>(c.dC, f11<R>(c.S), props<R>(c), c.probe_st, n,
+    k_probe<R><<<dim3((c.ny + tpb - 1) / tpb, n), tpb, 0, c.stream>>>(c.hC, f11<R>(c.S), props<R>(c), c.probe_st, n,
                                                                       kline, c.probe_out);
     return cudaGetLastError();
 }

@@ -117,6 +117,8 @@ def lib():
         _sig(L, "lesgpu_kernel_timing", C.c_int, [vp, C.c_int])
         _sig(L, "lesgpu_kernel_times", C.c_int, [vp, dp, dp, C.c_int])
         _sig(L, "lesgpu_mark", C.c_int, [vp, C.c_int])
+        _sig(L, "lesgpu_selfcheck_division", C.c_int, [dp, C.c_int, C.c_size_t, C.c_ulonglong,
+                                                       C.POINTER(C.c_ulonglong)])
         _sig(L, "lesgpu_elapsed_ms", C.c_int, [vp, C.c_int, C.c_int, C.POINTER(C.c_double)])
         _sig(L, "lesgpu_device_bytes", C.c_size_t, [vp])
         _sig(L, "lesgpu_bytes_for_grid", C.c_size_t, [C.c_int, C.c_int, C.c_int, C.c_int])
@@ -173,6 +175,16 @@ class Rng:
     @property
     def draws(self) -> int:
         return self._s.n
+
+
+def selfcheck_division(divisors: Sequence[float], n: int, seed: int = 12345) -> int:
+    """Number of quotients where the kernels' constant division differs from IEEE division."""
+    d = np.ascontiguousarray(divisors, dtype=np.float64)
+    bad = C.c_ulonglong(0)
+    rc = lib().lesgpu_selfcheck_division(d.ctypes.data, len(d), n, seed, C.byref(bad))
+    if rc != 0:
+        raise LesgpuError(rc, "selfcheck_division")
+    return int(bad.value)
 
 
 def initial_state(cfg: SolverConfig, species: Optional[LesgpuSpecies] = None):
@@ -288,15 +300,16 @@ class Context:
         self._check(lib().lesgpu_elapsed_ms(self._h, a, b, C.byref(v)), "elapsed_ms")
         return v.value
 
-    KERNEL_CLASSES = ["sem", "filter_props", "strain", "rhs_combine", "bc"]
+    KERNEL_CLASSES = ["sem", "filter_props", "strain", "rhs_flow", "bc", "rhs_scalar"]
 
     def kernel_timing(self, on: bool = True):
         self._check(lib().lesgpu_kernel_timing(self._h, 1 if on else 0), "kernel_timing")
 
     def kernel_times(self) -> Dict[str, tuple]:
-        ms = np.zeros(5)
-        cnt = np.zeros(5, dtype=np.int64)
-        self._check(lib().lesgpu_kernel_times(self._h, ms.ctypes.data, cnt.ctypes.data, 5), "kernel_times")
+        nk = len(self.KERNEL_CLASSES)
+        ms = np.zeros(nk)
+        cnt = np.zeros(nk, dtype=np.int64)
+        self._check(lib().lesgpu_kernel_times(self._h, ms.ctypes.data, cnt.ctypes.data, nk), "kernel_times")
         return {k: (float(ms[q]), int(cnt[q])) for q, k in enumerate(self.KERNEL_CLASSES)}
 
     @property

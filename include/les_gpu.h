@@ -170,9 +170,10 @@ enum {
     LESGPU_K_SEM = 0,        /* SEM inflow plane + normalisation */
     LESGPU_K_FILTER = 1,     /* box filter + mixture properties (4 launches per step) */
     LESGPU_K_STRAIN = 2,     /* strain, nu_t, S_T (4 per step) */
-    LESGPU_K_RHS = 3,        /* right-hand sides + RK4 stage update (4 per step) */
+    LESGPU_K_RHS_FLOW = 3,   /* momentum and G right-hand sides (4 per step) */
     LESGPU_K_BC = 4,         /* boundary faces + EOS/renormalisation */
-    LESGPU_NK = 5
+    LESGPU_K_RHS_SCALAR = 5, /* species/T right-hand sides + RK4 stage update (4 per step) */
+    LESGPU_NK = 6
 };
 int lesgpu_kernel_timing(lesgpu_ctx* ctx, int enable);
 /* Device-time markers on the context's stream (slots 0..15): lesgpu_mark records a CUDA
@@ -180,6 +181,13 @@ int lesgpu_kernel_timing(lesgpu_ctx* ctx, int enable);
 int lesgpu_mark(lesgpu_ctx* ctx, int slot);
 int lesgpu_elapsed_ms(lesgpu_ctx* ctx, int slot_a, int slot_b, double* ms);
 int lesgpu_kernel_times(lesgpu_ctx* ctx, double* ms, long long* launches, int n);
+
+/* Self-check of the constant-divisor division used by the kernels (x/c evaluated as a
+ * reciprocal product with one fma correction): n pseudo-random dividends spanning
+ * 2^-60..2^60 for each of nd divisors; *mismatches counts results whose bits differ from
+ * IEEE division.  Runs on the current device; allocates a few bytes of device memory. */
+int lesgpu_selfcheck_division(const double* divisors, int nd, size_t n, unsigned long long seed,
+                              unsigned long long* mismatches);
 
 /* Block until all work queued on the context's stream has finished. */
 int lesgpu_sync(lesgpu_ctx* ctx);

@@ -263,3 +263,18 @@ def test_fp32_precision_form_tracks_fp64(N):
         assert rel(sb[f], sa[f]) < 1e-3, f
     a.close()
     b.close()
+
+
+def test_constant_division_matches_ieee(N):
+    """The kernels evaluate divisions by constants as a reciprocal product with one fma
+    correction; it must give the same bits as IEEE division for the divisors they use."""
+    from lesgpu.config import preset
+    from lesgpu import props
+    divs = [6.0, 56.0, 1.6, 1.0, 0.03]
+    for name in ("c1", "c2", "c3", "tiny"):
+        c = preset(name)
+        for d in (c.lx / c.nx, c.ly / c.ny, c.lz / c.nz):
+            divs += [d, 2.0 * d, d * d]
+        divs.append(2.0 * c.accel_width * c.accel_width)
+    divs += [m / 1000.0 for m in props.synthetic_species().mw]
+    assert N.selfcheck_division(divs, 1 << 21) == 0
