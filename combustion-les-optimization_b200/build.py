@@ -71,18 +71,23 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(p) <= t for p in cu + c + hdr + [__file__])
 
 
-def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = False) -> str:
-    if not force and up_to_date():
+def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = False, defines=(), out: str = None,
+          build_dir: str = None) -> str:
+    """Compile the library.  ``defines`` (e.g. ``["LES_MINB_SCALAR=3"]``) and ``out`` build
+    a variant elsewhere; the default build goes to liblesgpu.so in-tree."""
+    lib_path = out or LIB
+    bdir = build_dir or BUILD
+    if not force and out is None and not defines and up_to_date():
         return LIB
     nvcc = _nvcc()
-    os.makedirs(BUILD, exist_ok=True)
+    os.makedirs(bdir, exist_ok=True)
     cu, c, _ = sources()
     objs = []
     for src in cu:
         name = os.path.splitext(os.path.basename(src))[0]
-        obj = os.path.join(BUILD, name + ".o")
+        obj = os.path.join(bdir, name + ".o")
         flags = [nvcc, "-c", src, "-o", obj, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
-                 "-I", INC, "-I", os.path.join(HERE, "csrc")] + ARCH
+                 "-I", INC, "-I", os.path.join(HERE, "csrc")] + ARCH + [f"-D{d}" for d in defines]
         flags += ["-fmad=false"] if name.endswith("_f64") else ["-fmad=true"]
         if ptxas_verbose:
             flags += ["-Xptxas", "-v"]
@@ -92,15 +97,15 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
         objs.append(obj)
     for src in c:
         name = os.path.splitext(os.path.basename(src))[0]
-        obj = os.path.join(BUILD, name + ".o")
+        obj = os.path.join(bdir, name + ".o")
         _run(["gcc", "-c", src, "-o", obj, "-O2", "-ffp-contract=off", "-fPIC", "-std=c11", "-Wall",
               "-I", INC, "-I", os.path.join(HERE, "host")], verbose)
         objs.append(obj)
-    tmp = LIB + ".tmp"
+    tmp = lib_path + ".tmp"
     _run([nvcc, "-shared", "-o", tmp] + objs + ARCH + ["-Xcompiler", "-fPIC", "-lcudart", "-lm",
                                                           "-L", _cuda_lib_dir(nvcc)], verbose)
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, lib_path)
+    return lib_path
 
 
 def main(argv=None) -> int:

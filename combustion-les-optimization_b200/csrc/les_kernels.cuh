@@ -58,6 +58,19 @@ struct KFlow {               // momentum and G right-hand sides handed from C1 t
 
 #define LES_KERNEL_CONSTS const __grid_constant__ Consts C
 
+// Minimum resident blocks per SM requested from the register allocator.  These kernels are
+// latency-bound; on B200 the 256x128x128 FP64 step was fastest with 4/4/3 (measured sweep
+// over 2..4: 13.4 ms at 2/2/2, 10.8 ms at 3/3/3, 10.5 ms at 4/4/4).
+#ifndef LES_MINB_FILTER
+#define LES_MINB_FILTER 4
+#endif
+#ifndef LES_MINB_FLOW
+#define LES_MINB_FLOW 4
+#endif
+#ifndef LES_MINB_SCALAR
+#define LES_MINB_SCALAR 3
+#endif
+
 // ---------------------------------------------------------------------------- helpers
 
 template <typename R>
@@ -222,7 +235,7 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
 // ------------------------------------------------------------------ pass A: filter + props
 
 template <typename R>
-__global__ void __launch_bounds__(NT, 2)
+__global__ void __launch_bounds__(NT, LES_MINB_FILTER)
     k_filter_props(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> in, F11<R> F, PropBuf<R> P,
                    double* __restrict__ part, Scalars* __restrict__ S, int want_max) {
     __shared__ double sh[NT / 32];
@@ -550,7 +563,7 @@ __device__ __forceinline__ R lap3(const Consts& C, const R* __restrict__ q, ptrd
 // C1: momentum (:2552-2697) with calculate_convection_conservative (:683-727) and the G
 // equation (:2706-2825).  Writes k_rhou, k_rhov, k_rhow, k_G of fluid cells.
 template <typename R>
-__global__ void __launch_bounds__(NT, 2)
+__global__ void __launch_bounds__(NT, LES_MINB_FLOW)
     k_rhs_flow(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> F, PropBuf<R> P, KFlow<R> kf,
                KDbg<R> kd, const Scalars* __restrict__ Sc, int t_loop) {
     const int nx = C.nx, ny = C.ny, nz = C.nz;
@@ -714,7 +727,7 @@ __global__ void __launch_bounds__(NT, 2)
 // C2: species (:2837-2904) and temperature (:2912-2962), then the RK4 bookkeeping.
 // stage: 0,1,2 -> intermediate stage with coefficient 0.5/0.5/1.0, 3 -> final combine.
 template <typename R>
-__global__ void __launch_bounds__(NT, 2)
+__global__ void __launch_bounds__(NT, LES_MINB_SCALAR)
     k_rhs_scalar(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> F, PropBuf<R> P, F11<R> S0, F11<R> St,
                  AccBuf<R> acc, KFlow<R> kf, KDbg<R> kd, double dt, int stage) {
     const int nx = C.nx, ny = C.ny, nz = C.nz;
