@@ -5,6 +5,7 @@
 // data), uploads/downloads in the reference's [i][j][k] order, and the stream-ordered step.
 #include <cuda_runtime.h>
 #include <math.h>
+#include <stddef.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -139,6 +140,8 @@ unsigned char* read_record(FILE* fp, int* len) {
 
 size_t fields_for_precision() { return 59; }
 
+void free_loop(DevCtx& d);
+
 }  // namespace
 
 namespace les {
@@ -179,6 +182,62 @@ void tmark_flush(DevCtx& c) {
 }
 
 }  // namespace les
+
+// ---------------------------------------------------------------- device-resident loop helpers
+
+namespace {
+
+// Rows J[m] (m = 0..rows-1) of the rand() jump-ahead: x[n+m] = sum_j J[m][j] * x[n-31+j]
+// (mod 2^32), from x[t] = x[t-31] + x[t-3] applied to coefficient vectors.
+std::vector<unsigned int> jump_table(int rows) {
+    std::vector<unsigned int> J((size_t)rows * 31, 0u);
+    auto row = [&](int t) -> const unsigned int* { return &J[(size_t)t * 31]; };
+    static unsigned int unit[31][31];
+    static bool init = false;
+    if (!init) {
+        for (int a = 0; a < 31; a++)
+            for (int b = 0; b < 31; b++) unit[a][b] = (a == b) ? 1u : 0u;
+        init = true;
+    }
+    for (int t = 0; t < rows; t++) {
+        const unsigned int* a = (t - 31 < 0) ? unit[t] : row(t - 31);         // x[t-31]
+        const unsigned int* b = (t - 3 < 0) ? unit[t + 28] : row(t - 3);     // x[t-3]
+        unsigned int* o = &J[(size_t)t * 31];
+        for (int j = 0; j < 31; j++) o[j] = a[j] + b[j];
+    }
+    return J;
+}
+
+void free_loop(DevCtx& d) {
+    if (d.graph) { cudaGraphExecDestroy(d.graph); d.graph = nullptr; }
+    d.graph_ok = false;
+    void* bufs[] = {d.J, d.dL, d.loop_st, d.hist_probe, d.hist_dt, d.hist_umax, d.hist_mon};
+    for (void* b : bufs)
+        if (b) cudaFree(b);
+    d.J = nullptr; d.dL = nullptr; d.loop_st = nullptr;
+    d.hist_probe = d.hist_dt = d.hist_umax = d.hist_mon = nullptr;
+    d.loop_ready = false;
+}
+
+int alloc_history(lesgpu_ctx* ctx, const int* st, int n, int kline, int cap) {
+    DevCtx& d = ctx->d;
+    if (d.graph) { cudaGraphExecDestroy(d.graph); d.graph = nullptr; }
+    d.graph_ok = false;
+    void* bufs[] = {d.loop_st, d.hist_probe, d.hist_dt, d.hist_umax, d.hist_mon};
+    for (void* b : bufs)
+        if (b) cudaFree(b);
+    d.loop_st = nullptr; d.hist_probe = d.hist_dt = d.hist_umax = d.hist_mon = nullptr;
+    d.loop_nst = n; d.loop_kline = kline; d.loop_cap = cap;
+    CK(cudaMalloc(&d.loop_st, (n > 0 ? n : 1) * sizeof(int)));
+    if (n > 0) CK(cudaMemcpy(d.loop_st, st, n * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&d.hist_probe, (size_t)cap * (n > 0 ? n : 1) * d.ny * 6 * sizeof(double)));
+    CK(cudaMalloc(&d.hist_dt, (size_t)cap * sizeof(double)));
+    CK(cudaMalloc(&d.hist_umax, (size_t)cap * sizeof(double)));
+    CK(cudaMalloc(&d.hist_mon, (size_t)cap * 6 * sizeof(double)));
+    return LESGPU_OK;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -243,6 +302,7 @@ size_t lesgpu_bytes_for_grid(int nx, int ny, int nz, int precision) {
     size_t n = (size_t)nx * ny * nz;
     size_t esz = (precision == LESGPU_FP32) ? 4 : 8;
     size_t nb = ((size_t)(nz + les::BX - 1) / les::BX) * ((ny + les::BY - 1) / les::BY) * nx;
+    if (nb < (size_t)les::MON_BLOCKS) nb = les::MON_BLOCKS;
     size_t planes = (size_t)ny * nz;
     return fields_for_precision() * n * esz + n +              // fields + attribute bytes
            (6 * nb + 64) * sizeof(double) +                       // reduction partials
@@ -287,8 +347,10 @@ int lesgpu_create(const lesgpu_config* cfg, const lesgpu_species* sp, lesgpu_ctx
     d.aT = take(); d.nu_t = take(); d.S_mag = take(); d.ST = take(); d.mu_eff = take();
     for (int q = 0; q < les::NACC; q++) d.acc[q] = take();
     for (int q = 0; q < 4; q++) d.kflow[q] = take();
+    // per-block partials: 3 per block of the per-cell grid (filter pass) and 6 per block of
+    // the monitor grid
     size_t nb = ((size_t)(d.nz + les::BX - 1) / les::BX) * ((d.ny + les::BY - 1) / les::BY) * d.nx;
-    d.part_len = 6 * nb + 64;
+    d.part_len = 6 * (nb > (size_t)les::MON_BLOCKS ? nb : (size_t)les::MON_BLOCKS) + 64;
     size_t planes = (size_t)d.ny * d.nz;
     bool ok = cudaMalloc(&d.attr, d.n) == cudaSuccess &&
               cudaMalloc(&d.dC, sizeof(les::Consts)) == cudaSuccess &&
@@ -339,6 +401,7 @@ void lesgpu_destroy(lesgpu_ctx* ctx) {
     for (cudaEvent_t e : d.ev_pool) cudaEventDestroy(e);
     for (int q = 0; q < 16; q++)
         if (d.marks[q]) cudaEventDestroy(d.marks[q]);
+    free_loop(d);
     if (d.stream) cudaStreamDestroy(d.stream);
     delete ctx;
 }
@@ -546,9 +609,143 @@ int lesgpu_step(lesgpu_ctx* ctx, double dt, int t_loop) {
     if (!d.have_state || !d.have_attr) return fail(ctx, LESGPU_ESTATE, "state and attribute map must be uploaded");
     if (d.n_inlet > 0 && !d.have_inflow) return fail(ctx, LESGPU_ESTATE, "lesgpu_set_inflow must precede each step");
     if (!(dt > 0.0) || !isfinite(dt)) return fail(ctx, LESGPU_EINVAL, "dt must be positive and finite");
-    cudaError_t e = (d.precision == LESGPU_FP64) ? les::step_f64(d, dt, t_loop) : les::step_f32(d, dt, t_loop);
+    cudaError_t e = (d.precision == LESGPU_FP64) ? les::step_f64(d, dt, t_loop, false)
+                                                 : les::step_f32(d, dt, t_loop, false);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "step");
     d.have_inflow = false;
+    return LESGPU_OK;
+}
+
+
+int lesgpu_loop_begin(lesgpu_ctx* ctx, const unsigned int rng_window[31], const double* vortices, int nv, int t_loop) {
+    if (!ctx || !rng_window || nv < 0 || (nv > 0 && !vortices)) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    if (!d.have_state || !d.have_attr) return fail(ctx, LESGPU_ESTATE, "state and attribute map must be uploaded");
+    CK(cudaStreamSynchronize(d.stream));
+    free_loop(d);
+    if (nv > d.nv_cap) {
+        cudaFree(d.vort);
+        d.vort = nullptr;
+        CK(cudaMalloc(&d.vort, (size_t)nv * 7 * sizeof(double)));
+        d.nv_cap = nv;
+    }
+    d.nv = nv;
+    if (nv > 0) CK(cudaMemcpy(d.vort, vortices, (size_t)nv * 7 * sizeof(double), cudaMemcpyHostToDevice));
+    // at most 6 draws per vortex and 3 per inlet cell in one step
+    d.jrows = 6 * nv + 3 * d.n_inlet;
+    if (d.jrows < 31) d.jrows = 31;
+    std::vector<unsigned int> J = jump_table(d.jrows);
+    CK(cudaMalloc(&d.J, J.size() * sizeof(unsigned int)));
+    CK(cudaMemcpy(d.J, J.data(), J.size() * sizeof(unsigned int), cudaMemcpyHostToDevice));
+    les::LoopState ls{};
+    for (int j = 0; j < 31; j++) ls.win[j] = rng_window[j];
+    CK(cudaMalloc(&d.dL, sizeof(les::LoopState)));
+    CK(cudaMemcpy(d.dL, &ls, sizeof(ls), cudaMemcpyHostToDevice));
+    const lesgpu_config& g = ctx->cfg;
+    d.lp_lbox = g.length_scale; d.lp_ly = g.ly; d.lp_lz = g.lz; d.lp_uin = g.inlet_velocity;
+    d.lp_ti = g.turbulence_intensity; d.lp_ell = g.length_scale; d.lp_cfl = g.courant;
+    d.lp_cfld = g.courant_diffusion; d.lp_dx = g.lx / (double)g.nx;
+    // default history: the reference's 7 probe stations on the line k = NZ/2 (:274, :3406)
+    const double xs[7] = {0.010, 0.015, 0.020, 0.025, 0.030, 0.035, 0.040};
+    std::vector<int> st;
+    for (double x : xs) {
+        int ip = (int)(x / d.lp_dx);
+        if (ip > 0 && ip < d.nx - 1) st.push_back(ip);
+    }
+    int r = alloc_history(ctx, st.data(), (int)st.size(), d.nz / 2, 64);
+    if (r) return r;
+    // step counters in the scalar block
+    les::Scalars h;
+    CK(cudaMemcpy(&h, d.dS, sizeof(h), cudaMemcpyDeviceToHost));
+    h.t_loop = t_loop;
+    h.run_step = 0;
+    h.nonfinite = 0;
+    CK(cudaMemcpy(d.dS, &h, sizeof(h), cudaMemcpyHostToDevice));
+    d.loop_ready = true;
+    d.total_bytes += J.size() * sizeof(unsigned int);
+    return LESGPU_OK;
+}
+
+int lesgpu_loop_config(lesgpu_ctx* ctx, const int* i_stations, int n, int k_line, int capacity_steps) {
+    if (!ctx || n < 0 || (n > 0 && !i_stations) || capacity_steps < 1) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    if (!d.loop_ready) return fail(ctx, LESGPU_ESTATE, "lesgpu_loop_begin first");
+    if (k_line < 0 || k_line >= d.nz) return fail(ctx, LESGPU_EINVAL, "k_line out of range");
+    for (int q = 0; q < n; q++)
+        if (i_stations[q] < 0 || i_stations[q] >= d.nx) return fail(ctx, LESGPU_EINVAL, "station out of range");
+    CK(cudaStreamSynchronize(d.stream));
+    return alloc_history(ctx, i_stations, n, k_line, capacity_steps);
+}
+
+int lesgpu_run(lesgpu_ctx* ctx, int nsteps) {
+    if (!ctx || nsteps < 0) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    if (!d.loop_ready) return fail(ctx, LESGPU_ESTATE, "lesgpu_loop_begin first");
+    if (nsteps > d.loop_cap) return fail(ctx, LESGPU_EINVAL, "nsteps exceeds the history capacity (lesgpu_loop_config)");
+    if (nsteps == 0) return LESGPU_OK;
+    // run_step restarts at 0 for every run (history slots)
+    CK(cudaMemsetAsync((char*)d.dS + offsetof(les::Scalars, run_step), 0, sizeof(int), d.stream));
+    const bool fp64 = d.precision == LESGPU_FP64;
+    if (d.timing) {
+        for (int q = 0; q < nsteps; q++) {
+            cudaError_t e = fp64 ? les::step_f64(d, 0.0, 0, true) : les::step_f32(d, 0.0, 0, true);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "run");
+        }
+        return LESGPU_OK;
+    }
+    if (!d.graph_ok) {
+        // capture one device-loop step; every launch reads its varying inputs (dt, t_loop,
+        // history slot) from device memory, so the graph is replayed unchanged
+        cudaGraph_t gr = nullptr;
+        CK(cudaStreamBeginCapture(d.stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = fp64 ? les::step_f64(d, 0.0, 0, true) : les::step_f32(d, 0.0, 0, true);
+        cudaError_t e2 = cudaStreamEndCapture(d.stream, &gr);
+        if (e != cudaSuccess) { if (gr) cudaGraphDestroy(gr); return cuda_fail(ctx, e, "capture"); }
+        if (e2 != cudaSuccess) return cuda_fail(ctx, e2, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&d.graph, gr, 0);
+        cudaGraphDestroy(gr);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGraphInstantiate");
+        d.graph_ok = true;
+    }
+    for (int q = 0; q < nsteps; q++) CK(cudaGraphLaunch(d.graph, d.stream));
+    return LESGPU_OK;
+}
+
+int lesgpu_loop_history(lesgpu_ctx* ctx, int nsteps, double* dt, double* umax, double* probes, double* monitor) {
+    if (!ctx || nsteps < 0) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    if (!d.loop_ready) return fail(ctx, LESGPU_ESTATE, "lesgpu_loop_begin first");
+    if (nsteps > d.loop_cap) return fail(ctx, LESGPU_EINVAL, "nsteps exceeds the history capacity");
+    CK(cudaStreamSynchronize(d.stream));
+    les::Scalars h;
+    CK(cudaMemcpy(&h, d.dS, sizeof(h), cudaMemcpyDeviceToHost));
+    if (h.nonfinite & 2) return fail(ctx, LESGPU_ESTATE, "rand() jump table too short");
+    if (nsteps == 0) return LESGPU_OK;
+    if (dt) CK(cudaMemcpy(dt, d.hist_dt, nsteps * sizeof(double), cudaMemcpyDeviceToHost));
+    if (umax) CK(cudaMemcpy(umax, d.hist_umax, nsteps * sizeof(double), cudaMemcpyDeviceToHost));
+    if (probes && d.loop_nst > 0)
+        CK(cudaMemcpy(probes, d.hist_probe, (size_t)nsteps * d.loop_nst * d.ny * 6 * sizeof(double),
+                      cudaMemcpyDeviceToHost));
+    if (monitor) CK(cudaMemcpy(monitor, d.hist_mon, (size_t)nsteps * 6 * sizeof(double), cudaMemcpyDeviceToHost));
+    return LESGPU_OK;
+}
+
+int lesgpu_loop_end(lesgpu_ctx* ctx, unsigned int rng_window[31], double* vortices, int* t_loop) {
+    if (!ctx) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    if (!d.loop_ready) return fail(ctx, LESGPU_ESTATE, "lesgpu_loop_begin first");
+    CK(cudaStreamSynchronize(d.stream));
+    les::LoopState ls;
+    CK(cudaMemcpy(&ls, d.dL, sizeof(ls), cudaMemcpyDeviceToHost));
+    les::Scalars h;
+    CK(cudaMemcpy(&h, d.dS, sizeof(h), cudaMemcpyDeviceToHost));
+    if (rng_window)
+        for (int j = 0; j < 31; j++) rng_window[j] = ls.win[j];
+    if (vortices && d.nv > 0) CK(cudaMemcpy(vortices, d.vort, (size_t)d.nv * 7 * sizeof(double), cudaMemcpyDeviceToHost));
+    if (t_loop) *t_loop = h.t_loop;
+    d.total_bytes -= (size_t)d.jrows * 31 * sizeof(unsigned int);
+    free_loop(d);
+    if (h.nonfinite & 2) return fail(ctx, LESGPU_ESTATE, "rand() jump table too short");
     return LESGPU_OK;
 }
 

@@ -16,6 +16,8 @@ constexpr int NSTATE = 11;                                  // u v w T G rho Y0.
 constexpr int NACC = 10;                                    // rhou rhov rhow T G Y0..Y4
 // thread-block shape of the per-cell passes: 32 consecutive k-cells x 8 j-rows
 constexpr int BX = 32, BY = 8, NT = BX * BY;
+// grid of the grid-stride monitor reductions (4 blocks per SM on 148 SMs)
+constexpr int MON_BLOCKS = 592;
 
 // Fixed constants of the reference (les_combustion_solver.c:136-188, 2164-2166, 234-245).
 constexpr double R_UNIV = 8.314462;
@@ -83,8 +85,20 @@ struct Scalars {
     double umax, numax, alphamax;       // dt inputs (:1472-1485, :4401-4408)
     double mon[6];                      // monitor reductions
     double sem[6];                      // SEM sums (debug)
-    unsigned int counter[4];            // last-block counters (0: filter, 1: bc, 2: aux)
-    int nonfinite;
+    unsigned int counter[4];            // last-block counters (0: filter, 1: bc, 2: aux, 3: monitor)
+    int nonfinite;                      // bit 1: rand() jump table too short (device loop)
+    double dt;                          // dt of the step being computed
+    double umax_used;                   // |u|max that produced dt (after the inlet fallback)
+    int t_loop;                         // reference time-step index of the step being computed
+    int run_step;                       // index of the step within the current device-loop run
+};
+
+// rand() stream state of the device-resident loop (les_devloop.cuh).
+struct LoopState {
+    unsigned int win[31];     // x[n-31 .. n-1] of the rand() stream, oldest first
+    int n_rec;                // vortices recycled in the last step (diagnostic)
+    int draws;                // rand() draws of the last step
+    unsigned long long total_draws;
 };
 
 __device__ __forceinline__ size_t cid(int i, int j, int k, int ny, int nz) {

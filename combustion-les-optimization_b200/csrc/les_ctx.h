@@ -59,6 +59,20 @@ struct DevCtx {
     double* h_pinned = nullptr;         // pinned staging for small transfers
     size_t h_pinned_len = 0;
     bool have_attr = false, have_state = false, have_inflow = false;
+    // device-resident time loop (les_devloop.cuh)
+    bool loop_ready = false;
+    unsigned int* J = nullptr;          // rand() jump-ahead rows, jrows x 31
+    int jrows = 0;
+    void* dL = nullptr;                 // LoopState
+    int* loop_st = nullptr;             // probe stations
+    int loop_nst = 0, loop_kline = 0, loop_cap = 0;
+    double* hist_probe = nullptr;       // cap x nst x NY x 6
+    double* hist_dt = nullptr;          // cap
+    double* hist_umax = nullptr;        // cap
+    double* hist_mon = nullptr;         // cap x 6
+    double lp_lbox = 0, lp_ly = 0, lp_lz = 0, lp_uin = 0, lp_ti = 0, lp_ell = 0, lp_cfl = 0, lp_cfld = 0, lp_dx = 0;
+    cudaGraphExec_t graph = nullptr;    // one captured device-loop step
+    bool graph_ok = false;
     // kernel timing: event pairs recorded around each kernel class during a step
     bool timing = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -78,13 +92,14 @@ void tmark_flush(DevCtx& c);
 // Per-precision entry points (les_f64.cu / les_f32.cu).
 cudaError_t sem_inflow(DevCtx& c);
 int selfcheck_division(const double* divisors, int nd, size_t n, unsigned long long seed, unsigned long long* bad);
-cudaError_t step_f64(DevCtx& c, double dt, int t_loop);
+cudaError_t loop_pre(DevCtx& c);
+cudaError_t step_f64(DevCtx& c, double dt, int t_loop, bool device_mode);
 cudaError_t umax_f64(DevCtx& c);
 cudaError_t monitor_f64(DevCtx& c);
 cudaError_t probe_f64(DevCtx& c, int n, int kline);
 cudaError_t check_f64(DevCtx& c, int field);
 cudaError_t rhs_only_f64(DevCtx& c, int t_loop);
-cudaError_t step_f32(DevCtx& c, double dt, int t_loop);
+cudaError_t step_f32(DevCtx& c, double dt, int t_loop, bool device_mode);
 cudaError_t rhs_only_f32(DevCtx& c, int t_loop);
 cudaError_t umax_f32(DevCtx& c);
 cudaError_t monitor_f32(DevCtx& c);

@@ -5,7 +5,9 @@
 
 namespace les {
 
-cudaError_t step_f32(DevCtx& c, double dt, int t_loop) { return step_impl<float>(c, dt, t_loop); }
+cudaError_t step_f32(DevCtx& c, double dt, int t_loop, bool device_mode) {
+    return step_impl<float>(c, dt, t_loop, device_mode);
+}
 cudaError_t rhs_only_f32(DevCtx& c, int t_loop) { return rhs_only_impl<float>(c, t_loop); }
 cudaError_t umax_f32(DevCtx& c) { return umax_impl<float>(c); }
 cudaError_t monitor_f32(DevCtx& c) { return monitor_impl<float>(c); }

@@ -6,6 +6,7 @@
 // floating-point operations one for one.
 #include "les_launch.cuh"
 #include "les_sem.cuh"
+#include "les_devloop.cuh"
 
 namespace les {
 
@@ -57,7 +58,16 @@ int selfcheck_division(const double* divisors, int nd, size_t n, unsigned long l
     return e == cudaSuccess ? 0 : -2;
 }
 
-cudaError_t step_f64(DevCtx& c, double dt, int t_loop) { return step_impl<double>(c, dt, t_loop); }
+cudaError_t loop_pre(DevCtx& c) {
+    k_loop_pre<<<1, LOOP_THREADS, 0, c.stream>>>(c.dC, c.dS, (LoopState*)c.dL, c.J, c.jrows, c.vort, c.nv, c.noise,
+                                                 c.n_inlet, c.lp_lbox, c.lp_ly, c.lp_lz, c.lp_uin, c.lp_ti, c.lp_ell,
+                                                 c.lp_cfl, c.lp_cfld, c.lp_dx);
+    return cudaGetLastError();
+}
+
+cudaError_t step_f64(DevCtx& c, double dt, int t_loop, bool device_mode) {
+    return step_impl<double>(c, dt, t_loop, device_mode);
+}
 cudaError_t rhs_only_f64(DevCtx& c, int t_loop) { return rhs_only_impl<double>(c, t_loop); }
 cudaError_t umax_f64(DevCtx& c) { return umax_impl<double>(c); }
 cudaError_t monitor_f64(DevCtx& c) { return monitor_impl<double>(c); }

@@ -565,7 +565,7 @@ __device__ __forceinline__ R lap3(const Consts& C, const R* __restrict__ q, ptrd
 template <typename R>
 __global__ void __launch_bounds__(NT, LES_MINB_FLOW)
     k_rhs_flow(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> F, PropBuf<R> P, KFlow<R> kf,
-               KDbg<R> kd, const Scalars* __restrict__ Sc, int t_loop) {
+               KDbg<R> kd, const Scalars* __restrict__ Sc) {
     const int nx = C.nx, ny = C.ny, nz = C.nz;
     const int k = blockIdx.x * BX + threadIdx.x;
     const int j = blockIdx.y * BY + threadIdx.y;
@@ -687,7 +687,7 @@ __global__ void __launch_bounds__(NT, LES_MINB_FLOW)
         SgsFaces<R> gf = sgs_faces<R>(P.nu_t + id, sI, sJ, C.d_sct2);
         R sgs = sgs_div<R>(C, Gf, gf, sI, sJ);
         R gx, gy, gz;
-        if (t_loop >= C.weno_step && !band3) {
+        if (Sc->t_loop >= C.weno_step && !band3) {
             gx = weno5_grad<R>(C, Gf, sI, C.d_dx);
             gy = weno5_grad<R>(C, Gf, sJ, C.d_dy);
             gz = weno5_grad<R>(C, Gf, 1, C.d_dz);
@@ -729,7 +729,7 @@ __global__ void __launch_bounds__(NT, LES_MINB_FLOW)
 template <typename R>
 __global__ void __launch_bounds__(NT, LES_MINB_SCALAR)
     k_rhs_scalar(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> F, PropBuf<R> P, F11<R> S0, F11<R> St,
-                 AccBuf<R> acc, KFlow<R> kf, KDbg<R> kd, double dt, int stage) {
+                 AccBuf<R> acc, KFlow<R> kf, KDbg<R> kd, const Scalars* __restrict__ Sc, int stage) {
     const int nx = C.nx, ny = C.ny, nz = C.nz;
     const int k = blockIdx.x * BX + threadIdx.x;
     const int j = blockIdx.y * BY + threadIdx.y;
@@ -810,6 +810,7 @@ __global__ void __launch_bounds__(NT, LES_MINB_SCALAR)
     // ---- RK4 bookkeeping.  acc holds k1, k1 + 2k2, (k1 + 2k2) + 2k3: exactly the
     // left-to-right partial sums of k1 + 2.0*k2 + 2.0*k3 + k4 (:4520).
     const bool fin = (stage == 3);
+    const double dt = Sc->dt;
     R incr[NACC];
     if (stage == 0) {
 #pragma unroll
@@ -1129,6 +1130,103 @@ __global__ void k_probe(LES_KERNEL_CONSTS, F11<R> S, PropBuf<R> P, const int* __
     o[3] = (double)S.p[4][id];
     o[4] = (double)P.nu_t[id];
     o[5] = (double)P.S_mag[id];
+}
+
+// Host-driven steps: dt and t_loop come from the caller.
+static __global__ void k_set_step(Scalars* __restrict__ Sc, double dt, int t_loop) {
+    Sc->dt = dt;
+    Sc->t_loop = t_loop;
+}
+
+// Device loop, after the boundary conditions: the probe lines of record_flame_region_data
+// (:3403-3471) and dt/|u|max of this step go to history slot run_step.
+template <typename R>
+__global__ void k_loop_post(LES_KERNEL_CONSTS, F11<R> S, PropBuf<R> P, const Scalars* __restrict__ Sc,
+                            const int* __restrict__ st, int n, int kline, int cap, double* __restrict__ hprobe,
+                            double* __restrict__ hdt, double* __restrict__ humax) {
+    const int ny = C.ny, nz = C.nz;
+    const int slot = Sc->run_step;
+    if (slot < 0 || slot >= cap) return;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int q = blockIdx.y;
+    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+        hdt[slot] = Sc->dt;
+        humax[slot] = Sc->umax_used;
+    }
+    if (j >= ny || q >= n) return;
+    const size_t id = cid(st[q], j, kline, ny, nz);
+    double* o = hprobe + (((size_t)slot * n + q) * ny + j) * 6;
+    o[0] = (double)S.p[0][id];
+    o[1] = (double)S.p[1][id];
+    o[2] = (double)S.p[2][id];
+    o[3] = (double)S.p[4][id];
+    o[4] = (double)P.nu_t[id];
+    o[5] = (double)P.S_mag[id];
+}
+
+// Device loop: the monitor reductions (:3874-3918) on steps with t_loop % 10 == 0, written
+// to history slot run_step (other slots are left untouched).
+template <typename R>
+__global__ void __launch_bounds__(NT) k_loop_monitor(LES_KERNEL_CONSTS, F11<R> S, double* __restrict__ part,
+                                                     Scalars* __restrict__ Sc, size_t n, int cap,
+                                                     double* __restrict__ hmon) {
+    __shared__ double sh[NT / 32];
+    __shared__ bool last;
+    if (Sc->t_loop % 10 != 0) return;          // uniform across the grid
+    const int slot = Sc->run_step;
+    if (slot < 0 || slot >= cap) return;
+    const int tid = threadIdx.x;
+    double mass = 0.0, tmin = 1.0e9, tmax = -1.0e9, gmin = 1.0e9, gmax = -1.0e9, ymin = 1.0e9;
+    for (size_t id = (size_t)blockIdx.x * NT + tid; id < n; id += (size_t)gridDim.x * NT) {
+        double r = (double)S.p[5][id], T = (double)S.p[3][id], G = (double)S.p[4][id], Y = (double)S.p[6][id];
+        mass += ((r * C.dx) * C.dy) * C.dz;
+        tmin = fmin(tmin, T); tmax = fmax(tmax, T);
+        gmin = fmin(gmin, G); gmax = fmax(gmax, G);
+        ymin = fmin(ymin, Y);
+    }
+    const unsigned nblk = gridDim.x;
+    double v[6];
+    v[0] = block_sum<NT>(mass, sh, tid);
+    v[1] = block_min<NT>(tmin, sh, tid);
+    v[2] = block_max<NT>(tmax, sh, tid);
+    v[3] = block_min<NT>(gmin, sh, tid);
+    v[4] = block_max<NT>(gmax, sh, tid);
+    v[5] = block_min<NT>(ymin, sh, tid);
+    if (tid == 0) {
+        for (int q = 0; q < 6; q++) part[q * nblk + blockIdx.x] = v[q];
+        __threadfence();
+        unsigned t = atomicAdd(&Sc->counter[3], 1u);
+        last = (t == nblk - 1);
+    }
+    __syncthreads();
+    if (last) {
+        __threadfence();
+        double acc[6] = {0.0, 1.0e9, -1.0e9, 1.0e9, -1.0e9, 1.0e9};
+        for (unsigned q = tid; q < nblk; q += NT) {
+            acc[0] += __ldcg(&part[q]);
+            acc[1] = fmin(acc[1], __ldcg(&part[nblk + q]));
+            acc[2] = fmax(acc[2], __ldcg(&part[2 * nblk + q]));
+            acc[3] = fmin(acc[3], __ldcg(&part[3 * nblk + q]));
+            acc[4] = fmax(acc[4], __ldcg(&part[4 * nblk + q]));
+            acc[5] = fmin(acc[5], __ldcg(&part[5 * nblk + q]));
+        }
+        acc[0] = block_sum<NT>(acc[0], sh, tid);
+        acc[1] = block_min<NT>(acc[1], sh, tid);
+        acc[2] = block_max<NT>(acc[2], sh, tid);
+        acc[3] = block_min<NT>(acc[3], sh, tid);
+        acc[4] = block_max<NT>(acc[4], sh, tid);
+        acc[5] = block_min<NT>(acc[5], sh, tid);
+        if (tid == 0) {
+            for (int q = 0; q < 6; q++) hmon[(size_t)slot * 6 + q] = acc[q];
+            Sc->counter[3] = 0u;
+        }
+    }
+}
+
+// Device loop, last launch of a step: advance the step counters.
+static __global__ void k_loop_tick(Scalars* __restrict__ Sc) {
+    Sc->t_loop += 1;
+    Sc->run_step += 1;
 }
 
 template <typename R>

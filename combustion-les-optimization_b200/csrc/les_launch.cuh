@@ -35,9 +35,24 @@ static inline dim3 cell_grid(const DevCtx& c) {
     return dim3((unsigned)((c.nz + BX - 1) / BX), (unsigned)((c.ny + BY - 1) / BY), (unsigned)c.nx);
 }
 
+// Every launch that writes per-block partials checks the buffer first: `per_block` values
+// per block for `blocks` blocks must fit in c.part.
+static inline bool part_fits(const DevCtx& c, size_t blocks, size_t per_block) {
+    return blocks * per_block <= c.part_len;
+}
+static inline size_t cell_blocks(const DevCtx& c) {
+    dim3 g = cell_grid(c);
+    return (size_t)g.x * g.y * g.z;
+}
+
+// One time step.  Host-driven (device_mode false): dt and t_loop come from the caller and
+// the inflow from lesgpu_set_inflow.  Device loop (true): dt, the vortex update and the
+// inflow noise are computed on the GPU first, and the step's history is recorded at the
+// end; every launch then reads only device memory, so the sequence can be graph-captured.
 template <typename R>
-cudaError_t step_impl(DevCtx& c, double dt, int t_loop) {
+cudaError_t step_impl(DevCtx& c, double dt, int t_loop, bool device_mode) {
     cudaStream_t st = c.stream;
+    if (!part_fits(c, cell_blocks(c), 3) || !part_fits(c, MON_BLOCKS, 6)) return cudaErrorInvalidValue;
     const dim3 g = cell_grid(c), b(BX, BY);
     F11<R> S = f11<R>(c.S), St = f11<R>(c.St), F = f11<R>(c.F);
     PropBuf<R> P = props<R>(c);
@@ -50,8 +65,10 @@ cudaError_t step_impl(DevCtx& c, double dt, int t_loop) {
     KFlow<R> kf;
     for (int q = 0; q < 4; q++) kf.p[q] = (R*)c.kflow[q];
 
-    // SEM inflow plane (:943-1075)
     int tm = tmark_begin(c, 0);
+    if (device_mode) loop_pre(c);
+    else k_set_step<<<1, 1, 0, st>>>(c.dS, dt, t_loop);
+    // SEM inflow plane (:943-1075)
     sem_inflow(c);
     tmark_end(c, tm);
     // four RK4 stages (:4428-4544)
@@ -66,10 +83,10 @@ cudaError_t step_impl(DevCtx& c, double dt, int t_loop) {
         // the k-arrays of the first stage are kept for inspection when requested
         const KDbg<R>& kds = (s == 0) ? kd : knone;
         tm = tmark_begin(c, 3);
-        k_rhs_flow<R><<<g, b, 0, st>>>(c.hC, c.attr, F, P, kf, kds, c.dS, t_loop);
+        k_rhs_flow<R><<<g, b, 0, st>>>(c.hC, c.attr, F, P, kf, kds, c.dS);
         tmark_end(c, tm);
         tm = tmark_begin(c, 5);
-        k_rhs_scalar<R><<<g, b, 0, st>>>(c.hC, c.attr, F, P, S, St, acc, kf, kds, dt, s);
+        k_rhs_scalar<R><<<g, b, 0, st>>>(c.hC, c.attr, F, P, S, St, acc, kf, kds, c.dS, s);
         tmark_end(c, tm);
     }
     // apply_boundary_conditions (:2967-3161)
@@ -84,6 +101,13 @@ cudaError_t step_impl(DevCtx& c, double dt, int t_loop) {
         }
         k_bc_eos<R><<<g, b, 0, st>>>(c.hC, c.attr, S, c.part, c.dS);
     }
+    if (device_mode) {
+        const int tpb = 64;
+        k_loop_post<R><<<dim3((c.ny + tpb - 1) / tpb, c.loop_nst > 0 ? c.loop_nst : 1), tpb, 0, st>>>(
+            c.hC, S, P, c.dS, c.loop_st, c.loop_nst, c.loop_kline, c.loop_cap, c.hist_probe, c.hist_dt, c.hist_umax);
+        k_loop_monitor<R><<<MON_BLOCKS, NT, 0, st>>>(c.hC, S, c.part, c.dS, c.n, c.loop_cap, c.hist_mon);
+        k_loop_tick<<<1, 1, 0, st>>>(c.dS);
+    }
     tmark_end(c, tm);
     tmark_flush(c);
     return cudaGetLastError();
@@ -94,6 +118,7 @@ cudaError_t step_impl(DevCtx& c, double dt, int t_loop) {
 template <typename R>
 cudaError_t rhs_only_impl(DevCtx& c, int t_loop) {
     cudaStream_t st = c.stream;
+    if (!part_fits(c, cell_blocks(c), 3)) return cudaErrorInvalidValue;
     const dim3 g = cell_grid(c), b(BX, BY);
     F11<R> S = f11<R>(c.S), St = f11<R>(c.St), F = f11<R>(c.F);
     PropBuf<R> P = props<R>(c);
@@ -103,22 +128,25 @@ cudaError_t rhs_only_impl(DevCtx& c, int t_loop) {
     for (int q = 0; q < NACC; q++) kd.p[q] = (R*)c.kd[q];
     KFlow<R> kf;
     for (int q = 0; q < 4; q++) kf.p[q] = (R*)c.kflow[q];
+    k_set_step<<<1, 1, 0, st>>>(c.dS, 0.0, t_loop);
     k_filter_props<R><<<g, b, 0, st>>>(c.hC, c.attr, S, F, P, c.part, c.dS, 1);
     k_strain<R><<<g, b, 0, st>>>(c.hC, c.attr, F, P);
-    k_rhs_flow<R><<<g, b, 0, st>>>(c.hC, c.attr, F, P, kf, kd, c.dS, t_loop);
-    k_rhs_scalar<R><<<g, b, 0, st>>>(c.hC, c.attr, F, P, S, St, acc, kf, kd, 0.0, 0);
+    k_rhs_flow<R><<<g, b, 0, st>>>(c.hC, c.attr, F, P, kf, kd, c.dS);
+    k_rhs_scalar<R><<<g, b, 0, st>>>(c.hC, c.attr, F, P, S, St, acc, kf, kd, c.dS, 0);
     return cudaGetLastError();
 }
 
 template <typename R>
 cudaError_t umax_impl(DevCtx& c) {
+    if (!part_fits(c, cell_blocks(c), 1)) return cudaErrorInvalidValue;
     k_umax<R><<<cell_grid(c), dim3(BX, BY), 0, c.stream>>>(c.hC, c.attr, f11<R>(c.S), c.part, c.dS);
     return cudaGetLastError();
 }
 
 template <typename R>
 cudaError_t monitor_impl(DevCtx& c) {
-    const int nb = 592;   // 4 x 148 SMs
+    const int nb = MON_BLOCKS;
+    if (!part_fits(c, nb, 6)) return cudaErrorInvalidValue;
     k_monitor<R><<<nb, NT, 0, c.stream>>>(c.hC, f11<R>(c.S), c.part, c.dS, c.n);
     return cudaGetLastError();
 }

@@ -357,10 +357,9 @@ int les_solver_set_outputs(les_solver* s, const char* dir, int flags) {
     return LESGPU_OK;
 }
 
-/* record_flame_region_data (:3403-3471): the lower G = 0.5 crossing on the line k = NZ/2
- * at each x-station, then every row within SAMPLING_RANGE (1.0 m, i.e. all rows). */
-static int write_probes(les_solver* s, int t_loop) {
-    int st[7], slot[7], m = 0;
+/* The x-stations that record_flame_region_data keeps (0 < i < NX-1), with their slot n. */
+static int probe_stations(const les_solver* s, int* st, int* slot) {
+    int m = 0;
     for (int n = 0; n < 7; n++) {
         int ip = s->probe_i[n];
         if (ip <= 0 || ip >= s->nx - 1) continue;
@@ -368,12 +367,15 @@ static int write_probes(les_solver* s, int t_loop) {
         slot[m] = n;
         m++;
     }
-    if (m == 0) return LESGPU_OK;
-    const int kline = s->nz / 2;
-    int rc = lesgpu_probe_lines(s->ctx, st, m, kline, s->probe_buf);
-    if (rc) return rc;
+    return m;
+}
+
+/* record_flame_region_data (:3403-3471): the lower G = 0.5 crossing on the line k = NZ/2
+ * at each x-station, then every row within SAMPLING_RANGE (1.0 m, i.e. all rows).
+ * lines holds m stations x NY x {u, v, w, G, nu_t, S_mag}. */
+static void append_probe_rows(les_solver* s, int t_loop, const double* lines, int m, const int* slot) {
     for (int q = 0; q < m; q++) {
-        const double* row = s->probe_buf + (size_t)q * s->ny * 6;
+        const double* row = lines + (size_t)q * s->ny * 6;
         double y_flame = -1.0;
         for (int j = 0; j < s->ny - 1; j++) {
             double G1 = row[6 * j + 3], G2 = row[6 * (j + 1) + 3];
@@ -400,7 +402,27 @@ static int write_probes(les_solver* s, int t_loop) {
         }
         fclose(fp);
     }
+}
+
+static int write_probes(les_solver* s, int t_loop) {
+    int st[7], slot[7];
+    int m = probe_stations(s, st, slot);
+    if (m == 0) return LESGPU_OK;
+    int rc = lesgpu_probe_lines(s->ctx, st, m, s->nz / 2, s->probe_buf);
+    if (rc) return rc;
+    append_probe_rows(s, t_loop, s->probe_buf, m, slot);
     return LESGPU_OK;
+}
+
+static void append_monitor_row(les_solver* s, int step, double dt, const double* m) {
+    char path[1200];
+    join_path(path, sizeof(path), s->out_dir, "simulation_monitor.csv");
+    FILE* fp = fopen(path, "a");
+    if (!fp) return;
+    fseek(fp, 0, SEEK_END);
+    if (ftell(fp) == 0) fprintf(fp, "step,dt,total_mass,min_T,max_T,min_G,max_G,min_Y_C3H8\n");
+    fprintf(fp, "%d,%.6e,%.6e,%.2f,%.2f,%.4f,%.4f,%.2e\n", step, dt, m[0], m[1], m[2], m[3], m[4], m[5]);
+    fclose(fp);
 }
 
 /* write_monitor_log (:3874-3924), every 10 steps */
@@ -409,14 +431,7 @@ static int write_monitor(les_solver* s, int step, double dt) {
     double m[6];
     int rc = lesgpu_monitor(s->ctx, m);
     if (rc) return rc;
-    char path[1200];
-    join_path(path, sizeof(path), s->out_dir, "simulation_monitor.csv");
-    FILE* fp = fopen(path, "a");
-    if (!fp) return LESGPU_OK;
-    fseek(fp, 0, SEEK_END);
-    if (ftell(fp) == 0) fprintf(fp, "step,dt,total_mass,min_T,max_T,min_G,max_G,min_Y_C3H8\n");
-    fprintf(fp, "%d,%.6e,%.6e,%.2f,%.2f,%.4f,%.4f,%.2e\n", step, dt, m[0], m[1], m[2], m[3], m[4], m[5]);
-    fclose(fp);
+    append_monitor_row(s, step, dt, m);
     return LESGPU_OK;
 }
 
@@ -451,6 +466,71 @@ int les_solver_step(les_solver* s) {
         if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
     }
     s->t_loop++;
+    return LESGPU_OK;
+}
+
+/* The same time loop with the host side on the GPU (lesgpu_loop_*): steps are queued in
+ * chunks without a host round trip; between chunks the probe and monitor rows are written
+ * from the step history, and checkpoints fall on chunk boundaries. */
+int les_solver_run_device(les_solver* s, int nsteps, int chunk) {
+    if (!s || nsteps < 0) return LESGPU_EINVAL;
+    if (chunk <= 0) chunk = 64;
+    if (nsteps == 0) return LESGPU_OK;
+    unsigned int win[31];
+    for (int j = 0; j < 31; j++) win[j] = (unsigned int)s->rng.r[(s->rng.f + j) % 31];
+    int rc = lesgpu_loop_begin(s->ctx, win, s->vort, s->cfg.num_vortices, s->t_loop);
+    if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
+    int st[7], slot[7];
+    int m = probe_stations(s, st, slot);
+    rc = lesgpu_loop_config(s->ctx, st, m, s->nz / 2, chunk);
+    double* hdt = (double*)malloc((size_t)chunk * sizeof(double));
+    double* hum = (double*)malloc((size_t)chunk * sizeof(double));
+    double* hmon = (double*)malloc((size_t)chunk * 6 * sizeof(double));
+    double* hpr = (double*)malloc((size_t)chunk * (m > 0 ? m : 1) * s->ny * 6 * sizeof(double));
+    if (!hdt || !hum || !hmon || !hpr) rc = LESGPU_ENOMEM;
+    const int want_probes = (s->out_flags & LES_OUT_PROBES) && s->out_dir[0];
+    const int want_mon = (s->out_flags & LES_OUT_MONITOR) && s->out_dir[0];
+    const int want_ckpt = (s->out_flags & LES_OUT_CHECKPOINT) && s->out_dir[0];
+    int left = nsteps;
+    while (rc == LESGPU_OK && left > 0) {
+        int n = left < chunk ? left : chunk;
+        if (want_ckpt) {
+            /* end the chunk on the next checkpoint step (t > 0, t % 50 == 0) */
+            for (int q = 0; q < n; q++) {
+                int t = s->t_loop + q;
+                if (t > 0 && t % 50 == 0) { n = q + 1; break; }
+            }
+        }
+        rc = lesgpu_run(s->ctx, n);
+        if (rc == LESGPU_OK)
+            rc = lesgpu_loop_history(s->ctx, n, hdt, hum, want_probes ? hpr : NULL, want_mon ? hmon : NULL);
+        if (rc) break;
+        for (int q = 0; q < n; q++) {
+            const int t = s->t_loop + q;
+            if (want_probes && m > 0) append_probe_rows(s, t, hpr + (size_t)q * m * s->ny * 6, m, slot);
+            if (want_mon && t % 10 == 0) append_monitor_row(s, t, hdt[q], hmon + 6 * (size_t)q);
+        }
+        s->dt = hdt[n - 1];
+        s->umax = hum[n - 1];
+        s->t_loop += n;
+        left -= n;
+        const int tl = s->t_loop - 1;
+        if (want_ckpt && tl > 0 && tl % 50 == 0) {
+            char path[1200];
+            join_path(path, sizeof(path), s->out_dir, "checkpoint.bin");
+            rc = les_solver_save_checkpoint(s, path, tl);
+        }
+    }
+    int t_back = 0;
+    int rc2 = lesgpu_loop_end(s->ctx, win, s->vort, &t_back);
+    if (rc2 == LESGPU_OK) {
+        for (int j = 0; j < 31; j++) s->rng.r[j] = (int)win[j];
+        s->rng.f = 0;
+        s->rng.b = 28;
+    }
+    free(hdt); free(hum); free(hmon); free(hpr);
+    if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
+    if (rc2) return serr(s, rc2, lesgpu_last_error(s->ctx));
     return LESGPU_OK;
 }
 

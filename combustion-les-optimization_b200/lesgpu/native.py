@@ -139,6 +139,12 @@ def lib():
         _sig(L, "les_solver_set_outputs", C.c_int, [vp, C.c_char_p, C.c_int])
         _sig(L, "les_solver_step", C.c_int, [vp])
         _sig(L, "les_solver_run", C.c_int, [vp, C.c_int])
+        _sig(L, "les_solver_run_device", C.c_int, [vp, C.c_int, C.c_int])
+        _sig(L, "lesgpu_loop_begin", C.c_int, [vp, vp, dp, C.c_int, C.c_int])
+        _sig(L, "lesgpu_loop_config", C.c_int, [vp, vp, C.c_int, C.c_int, C.c_int])
+        _sig(L, "lesgpu_run", C.c_int, [vp, C.c_int])
+        _sig(L, "lesgpu_loop_history", C.c_int, [vp, C.c_int, dp, dp, dp, dp])
+        _sig(L, "lesgpu_loop_end", C.c_int, [vp, vp, dp, C.POINTER(C.c_int)])
         _sig(L, "les_solver_t_loop", C.c_int, [vp])
         _sig(L, "les_solver_last_dt", C.c_double, [vp])
         _sig(L, "les_solver_last_umax", C.c_double, [vp])
@@ -362,6 +368,10 @@ class Solver:
 
     def run(self, n: int):
         self._check(lib().les_solver_run(self._h, n), "run")
+
+    def run_device(self, n: int, chunk: int = 64):
+        """n steps with the host side on the GPU (graph-replayed, no per-step round trip)."""
+        self._check(lib().les_solver_run_device(self._h, n, chunk), "run_device")
 
     @property
     def t_loop(self) -> int:

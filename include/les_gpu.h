@@ -127,6 +127,29 @@ int lesgpu_set_inflow(lesgpu_ctx* ctx, const double* vortices, int nv, const dou
  * central/WENO5 G-gradient switch (:2740-2780).  Asynchronous on the context's stream. */
 int lesgpu_step(lesgpu_ctx* ctx, double dt, int t_loop);
 
+/* Device-resident time loop.  The host-driven cycle above (lesgpu_dt_inputs -> host rand()
+ * -> lesgpu_set_inflow -> lesgpu_step) needs one host round trip per step.  These calls move
+ * that host side onto the GPU: dt is computed from the device maxima, update_vortices
+ * (:900-939) and the inflow noise (:2990-2992) draw from the same glibc rand() stream
+ * through a jump-ahead table (bit-identical draws), and each step records its dt, |u|max,
+ * probe lines and (every 10th step) the monitor values in a history buffer.  One step is
+ * captured once as a CUDA graph and replayed.
+ *
+ * lesgpu_loop_begin: hand over the host's rand() window (the last 31 words of the
+ *   generator, oldest first: x[n-31..n-1]), the vortex table and t_loop.
+ * lesgpu_loop_config: probe stations / line and the history capacity in steps (default:
+ *   the reference's seven stations on k = NZ/2 and 64 steps).
+ * lesgpu_run: queue nsteps (<= capacity) steps; asynchronous.
+ * lesgpu_loop_history: after a run, per-step dt and |u|max (nsteps each), probe lines
+ *   (nsteps x n x NY x 6) and monitor rows (nsteps x 6, written on steps with
+ *   t_loop % 10 == 0 only); any pointer may be NULL.
+ * lesgpu_loop_end: hand the rand() window, vortices and t_loop back to the host. */
+int lesgpu_loop_begin(lesgpu_ctx* ctx, const unsigned int rng_window[31], const double* vortices, int nv, int t_loop);
+int lesgpu_loop_config(lesgpu_ctx* ctx, const int* i_stations, int n, int k_line, int capacity_steps);
+int lesgpu_run(lesgpu_ctx* ctx, int nsteps);
+int lesgpu_loop_history(lesgpu_ctx* ctx, int nsteps, double* dt, double* umax, double* probes, double* monitor);
+int lesgpu_loop_end(lesgpu_ctx* ctx, unsigned int rng_window[31], double* vortices, int* t_loop);
+
 /* Probe lines for record_flame_region_data (:3403-3471) and the point buffer (:4558-4569):
  * for each of n x-stations, NY rows of {u, v, w, G, nu_t, S_mag} on the line k = k_line.
  * out holds n * NY * 6 doubles. */

@@ -64,6 +64,10 @@ int les_solver_set_outputs(les_solver* s, const char* dir, int flags);
  * noise draws with rand(), the GPU step, then the enabled outputs. */
 int les_solver_step(les_solver* s);
 int les_solver_run(les_solver* s, int nsteps);
+/* The same loop with the host side on the GPU (lesgpu_loop_* in les_gpu.h): nsteps steps
+ * queued in chunks of `chunk` steps (<= 0: 64) without a per-step host round trip; results,
+ * rand() stream and output files are identical to les_solver_run. */
+int les_solver_run_device(les_solver* s, int nsteps, int chunk);
 
 int les_solver_t_loop(const les_solver* s);
 double les_solver_last_dt(const les_solver* s);

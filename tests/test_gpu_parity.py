@@ -278,3 +278,58 @@ def test_constant_division_matches_ieee(N):
         divs.append(2.0 * c.accel_width * c.accel_width)
     divs += [m / 1000.0 for m in props.synthetic_species().mw]
     assert N.selfcheck_division(divs, 1 << 21) == 0
+
+
+def test_device_loop_matches_host_loop(N, tmp_path):
+    """The device-resident loop (dt, vortex recycling and inflow noise on the GPU through the
+    rand() jump-ahead, graph-replayed steps) is bit-identical to the host-driven loop,
+    including the rand() stream handed back afterwards and the probe/monitor files."""
+    from lesgpu.config import preset
+    cfg = preset("c1", seed=4242)
+    a, b = N.Solver(cfg), N.Solver(cfg)
+    da, db = tmp_path / "host", tmp_path / "dev"
+    da.mkdir()
+    db.mkdir()
+    a.set_outputs(str(da), N.LES_OUT_PROBES | N.LES_OUT_MONITOR)
+    b.set_outputs(str(db), N.LES_OUT_PROBES | N.LES_OUT_MONITOR)
+    a.step(23)
+    b.run_device(23, chunk=7)
+    assert a.t_loop == b.t_loop == 23
+    assert a.last_dt == b.last_dt
+    np.testing.assert_array_equal(a.vortices(), b.vortices())
+    sa, sb = a.state(), b.state()
+    for f in STATE:
+        np.testing.assert_array_equal(sa[f], sb[f], err_msg=f)
+    # host-driven steps continue from the handed-back rand() window
+    a.step(2)
+    b.step(2)
+    np.testing.assert_array_equal(a.vortices(), b.vortices())
+    np.testing.assert_array_equal(a.state()["u"], b.state()["u"])
+    for fn in ["simulation_monitor.csv"] + [f"probe_data_flame_region_loc{n}.csv" for n in range(7)]:
+        assert (da / fn).read_text() == (db / fn).read_text(), fn
+    a.close()
+    b.close()
+
+
+def test_device_loop_chunking_invariant(N, tmp_path):
+    """Splitting a device-loop run into chunks (history slots, graph replays across chunk
+    boundaries, checkpoint stops at t % 50 == 0) does not change the result or the files."""
+    from lesgpu.config import preset
+    cfg = preset("small")
+    outs = []
+    for chunk in (3, 64):
+        d = tmp_path / f"c{chunk}"
+        d.mkdir()
+        s = N.Solver(cfg)
+        s.set_outputs(str(d), N.LES_OUT_PROBES | N.LES_OUT_MONITOR | N.LES_OUT_CHECKPOINT)
+        s.run_device(53, chunk=chunk)
+        outs.append((s.state(), s.vortices(), s.last_dt, d))
+        s.close()
+    (sa, va, ta, da), (sb, vb, tb, db) = outs
+    assert ta == tb
+    np.testing.assert_array_equal(va, vb)
+    for f in STATE:
+        np.testing.assert_array_equal(sa[f], sb[f], err_msg=f)
+    for fn in ["simulation_monitor.csv", "checkpoint.bin", "restart_info.txt"]:
+        assert (da / fn).read_bytes() == (db / fn).read_bytes(), fn
+    assert (da / "restart_info.txt").read_text() == "BINARY\n50\n"
