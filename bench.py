@@ -252,14 +252,17 @@ def run_ours(args):
     esz = 4 if prec == N.FP32 else 8
     sol = N.Solver(cfg, precision=prec, device=local)
     ctx = sol.ctx
-    per_step_launches = (2 if True else 0) + 12 + 4
+    # per step: loop_pre, 2 SEM, 4 x 4 stage kernels, 4 BC, loop_post, loop_monitor, loop_tick
+    per_step_launches = 1 + 2 + 16 + 4 + 3
 
-    # ---- warm-up
-    sol.step(args.warmup)
+    # ---- warm-up (device-resident loop session; graph capture happens here)
+    sol.loop_begin(chunk=max(args.warmup, args.steps))
+    sol.loop_run(args.warmup)
     ctx.sync()
     torch.cuda.synchronize()
 
-    # ---- value: K device-resident steps
+    # ---- value: K device-resident steps (dt, rand() draws, SEM and the RK4 step on the GPU,
+    # one CUDA graph replay per step), state resident in HBM
     clocks = Clocks(local) if rank == 0 else None
     _barrier(world)
     torch.cuda.synchronize()
@@ -267,11 +270,12 @@ def run_ours(args):
     if clocks:
         clocks.start()
     ctx.mark(0)
-    sol.step(args.steps)
+    sol.loop_run(args.steps)
     ctx.mark(1)
     ms = ctx.elapsed_ms(0, 1)
     torch.cuda.synchronize()
     clk = clocks.stop() if clocks else None
+    sol.loop_end()
     _barrier(world)
     ms_max = _max_over_ranks(ms, world)
     value = world * cfg.cells * args.steps / (ms_max / 1e3)
@@ -293,33 +297,51 @@ def run_ours(args):
                 "frac": achieved / peak, "peak_kind": peak_kind,
                 "traffic": (traffic * cfg.cells if traffic is not None else None),
                 "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": avg_ms,
+                "kernel_ms_per_step": {k: v[0] / nprof for k, v in kt.items()},
                 "kernel_share": {k: (v[0] / max(sum(x[0] for x in kt.values()), 1e-30)) for k, v in kt.items()},
-                "step_achieved_gbs": STEP_BYTES_PER_CELL * esz / 8 * cfg.cells / (step_ms / 1e3) / 1e9}
+                "step_achieved_gbs": STEP_BYTES_PER_CELL * esz / 8 * cfg.cells / (step_ms / 1e3) / 1e9,
+                "step_frac": STEP_BYTES_PER_CELL * esz / 8 * cfg.cells / (step_ms / 1e3) / 1e9 / peak}
 
-    # ---- e2e: public API with host buffers (pinned), copies inside the timed region
+    # ---- e2e through the public solver API with host buffers (pinned): the state is
+    # uploaded, K steps run on the device loop with every step's history (dt, |u|max, the
+    # probe lines, monitor rows) read back, and the final state downloaded -- all timed
     st = sol.state()
     pinned = {k: torch.empty(v.shape, dtype=torch.float64, pin_memory=True) for k, v in st.items()}
     for k, v in st.items():
         pinned[k].numpy()[...] = v
     host_state = {k: t.numpy() for k, t in pinned.items()}
-    stations = [int(x / (cfg.lx / cfg.nx)) for x in (0.010, 0.015, 0.020, 0.025, 0.030, 0.035, 0.040)]
-    stations = [i for i in stations if 0 < i < cfg.nx - 1]
+    tmpd = tempfile.mkdtemp(prefix="lesbench_")
+    sol.set_outputs(tmpd, N.LES_OUT_PROBES | N.LES_OUT_MONITOR)
+    sol.loop_begin(chunk=args.steps)
     _barrier(world)
     ctx.sync()
     ctx.mark(2)
     ctx.upload_state(host_state)
-    for _ in range(args.steps):
-        sol.step(1)
-        ctx.probe_lines(stations, cfg.nz // 2)
+    sol.loop_run(args.steps)
     out = ctx.download_state()
     ctx.mark(3)
+    sol.loop_end()
     e2e_ms = _max_over_ranks(ctx.elapsed_ms(2, 3), world)
     e2e_value = world * cfg.cells * args.steps / (e2e_ms / 1e3)
+    sol.set_outputs(None, 0)
+    shutil.rmtree(tmpd, ignore_errors=True)
+    stations = [int(x / (cfg.lx / cfg.nx)) for x in (0.010, 0.015, 0.020, 0.025, 0.030, 0.035, 0.040)]
+    stations = [i for i in stations if 0 < i < cfg.nx - 1]
     state_bytes = 11 * cfg.cells * 8
-    n_inlet = int((sol.attribute()[0] == 1).sum())
-    h2d = state_bytes / args.steps + cfg.num_vortices * 7 * 8 + n_inlet * 3 * 8
-    d2h = state_bytes / args.steps + 64 + len(stations) * cfg.ny * 6 * 8
+    h2d = state_bytes / args.steps
+    d2h = state_bytes / args.steps + 8 * (2 + 6) + len(stations) * cfg.ny * 6 * 8
     del out
+
+    # ---- the literal host-driven ABI cycle per step (dt inputs -> host rand() ->
+    # lesgpu_set_inflow -> lesgpu_step -> probe lines), for comparison
+    nh = max(2, min(args.steps, 10))
+    ctx.mark(4)
+    for _ in range(nh):
+        sol.step(1)
+        ctx.probe_lines(stations, cfg.nz // 2)
+    ctx.mark(5)
+    host_ms = ctx.elapsed_ms(4, 5) / nh
+    n_inlet = int((sol.attribute()[0] == 1).sum())
 
     result = None
     if rank == 0:
@@ -339,7 +361,11 @@ def run_ours(args):
                        "l2": f"inputs larger than L2 ({ctx.device_bytes / 2**30:.2f} GiB resident per replica)"},
             "roofline": roofline,
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "path": "les_solver: upload state, device loop with per-step history read-back, download"},
+            "host_driven_step": {"ms_per_step": host_ms, "value": world * cfg.cells / (host_ms / 1e3),
+                                 "h2d_bytes_per_step": cfg.num_vortices * 7 * 8 + n_inlet * 3 * 8 + 16,
+                                 "d2h_bytes_per_step": 24 + len(stations) * cfg.ny * 6 * 8},
             "gpu_launches": per_step_launches * args.steps,
             "clocks": clk,
         }

@@ -485,9 +485,10 @@ int lesgpu_upload_state(lesgpu_ctx* ctx, const double* const* fields, int nfield
     }
     DevCtx& d = ctx->d;
     // dt inputs as after start-up or a restart: nu and alpha are not part of the state
-    // (never restored by the reference), so their maxima start at zero (:4401-4408).
-    les::Scalars z{};
-    CK(cudaMemcpyAsync(d.dS, &z, sizeof(z), cudaMemcpyHostToDevice, d.stream));
+    // (never restored by the reference), so their maxima start at zero (:4401-4408).  The
+    // step counters of a running device loop are kept.
+    CK(cudaMemsetAsync((char*)d.dS + offsetof(les::Scalars, numax), 0, sizeof(double), d.stream));
+    CK(cudaMemsetAsync((char*)d.dS + offsetof(les::Scalars, alphamax), 0, sizeof(double), d.stream));
     cudaError_t e = (d.precision == LESGPU_FP64) ? les::umax_f64(d) : les::umax_f32(d);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "umax");
     CK(cudaStreamSynchronize(d.stream));

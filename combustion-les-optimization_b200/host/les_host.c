@@ -72,6 +72,10 @@ struct les_solver {
     int out_flags;
     int probe_i[7];
     double* probe_buf;
+    /* device-loop session (les_solver_loop_*) */
+    int loop_on, l_chunk, l_m;
+    int l_st[7], l_slot[7];
+    double *l_dt, *l_umax, *l_mon, *l_probe;
     char err[256];
 };
 
@@ -309,6 +313,7 @@ int les_solver_create(const lesgpu_config* cfg, const char* chem_path, const cha
 
 void les_solver_destroy(les_solver* s) {
     if (!s) return;
+    if (s->loop_on) les_solver_loop_end(s);
     if (s->ctx) lesgpu_destroy(s->ctx);
     free(s->attr); free(s->vort); free(s->noise); free(s->probe_buf);
     free(s);
@@ -437,6 +442,7 @@ static int write_monitor(les_solver* s, int step, double dt) {
 
 int les_solver_step(les_solver* s) {
     if (!s) return LESGPU_EINVAL;
+    if (s->loop_on) return serr(s, LESGPU_ESTATE, "end the device loop before host-driven steps");
     const lesgpu_config* c = &s->cfg;
     /* dt (:4399-4411) */
     double umax, numax, alphamax;
@@ -472,28 +478,45 @@ int les_solver_step(les_solver* s) {
 /* The same time loop with the host side on the GPU (lesgpu_loop_*): steps are queued in
  * chunks without a host round trip; between chunks the probe and monitor rows are written
  * from the step history, and checkpoints fall on chunk boundaries. */
-int les_solver_run_device(les_solver* s, int nsteps, int chunk) {
-    if (!s || nsteps < 0) return LESGPU_EINVAL;
+static void loop_free(les_solver* s) {
+    free(s->l_dt); free(s->l_umax); free(s->l_mon); free(s->l_probe);
+    s->l_dt = s->l_umax = s->l_mon = s->l_probe = NULL;
+}
+
+int les_solver_loop_begin(les_solver* s, int chunk) {
+    if (!s) return LESGPU_EINVAL;
+    if (s->loop_on) return serr(s, LESGPU_ESTATE, "device loop already running");
     if (chunk <= 0) chunk = 64;
-    if (nsteps == 0) return LESGPU_OK;
     unsigned int win[31];
     for (int j = 0; j < 31; j++) win[j] = (unsigned int)s->rng.r[(s->rng.f + j) % 31];
     int rc = lesgpu_loop_begin(s->ctx, win, s->vort, s->cfg.num_vortices, s->t_loop);
     if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
-    int st[7], slot[7];
-    int m = probe_stations(s, st, slot);
-    rc = lesgpu_loop_config(s->ctx, st, m, s->nz / 2, chunk);
-    double* hdt = (double*)malloc((size_t)chunk * sizeof(double));
-    double* hum = (double*)malloc((size_t)chunk * sizeof(double));
-    double* hmon = (double*)malloc((size_t)chunk * 6 * sizeof(double));
-    double* hpr = (double*)malloc((size_t)chunk * (m > 0 ? m : 1) * s->ny * 6 * sizeof(double));
-    if (!hdt || !hum || !hmon || !hpr) rc = LESGPU_ENOMEM;
+    s->l_m = probe_stations(s, s->l_st, s->l_slot);
+    rc = lesgpu_loop_config(s->ctx, s->l_st, s->l_m, s->nz / 2, chunk);
+    if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
+    s->l_chunk = chunk;
+    s->l_dt = (double*)malloc((size_t)chunk * sizeof(double));
+    s->l_umax = (double*)malloc((size_t)chunk * sizeof(double));
+    s->l_mon = (double*)malloc((size_t)chunk * 6 * sizeof(double));
+    s->l_probe = (double*)malloc((size_t)chunk * (s->l_m > 0 ? s->l_m : 1) * s->ny * 6 * sizeof(double));
+    if (!s->l_dt || !s->l_umax || !s->l_mon || !s->l_probe) {
+        loop_free(s);
+        return serr(s, LESGPU_ENOMEM, "host history buffers");
+    }
+    s->loop_on = 1;
+    return LESGPU_OK;
+}
+
+int les_solver_loop_run(les_solver* s, int nsteps) {
+    if (!s || nsteps < 0) return LESGPU_EINVAL;
+    if (!s->loop_on) return serr(s, LESGPU_ESTATE, "les_solver_loop_begin first");
     const int want_probes = (s->out_flags & LES_OUT_PROBES) && s->out_dir[0];
     const int want_mon = (s->out_flags & LES_OUT_MONITOR) && s->out_dir[0];
     const int want_ckpt = (s->out_flags & LES_OUT_CHECKPOINT) && s->out_dir[0];
-    int left = nsteps;
-    while (rc == LESGPU_OK && left > 0) {
-        int n = left < chunk ? left : chunk;
+    const int m = s->l_m;
+    int left = nsteps, rc = LESGPU_OK;
+    while (left > 0) {
+        int n = left < s->l_chunk ? left : s->l_chunk;
         if (want_ckpt) {
             /* end the chunk on the next checkpoint step (t > 0, t % 50 == 0) */
             for (int q = 0; q < n; q++) {
@@ -503,15 +526,16 @@ int les_solver_run_device(les_solver* s, int nsteps, int chunk) {
         }
         rc = lesgpu_run(s->ctx, n);
         if (rc == LESGPU_OK)
-            rc = lesgpu_loop_history(s->ctx, n, hdt, hum, want_probes ? hpr : NULL, want_mon ? hmon : NULL);
-        if (rc) break;
+            rc = lesgpu_loop_history(s->ctx, n, s->l_dt, s->l_umax, want_probes ? s->l_probe : NULL,
+                                     want_mon ? s->l_mon : NULL);
+        if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
         for (int q = 0; q < n; q++) {
             const int t = s->t_loop + q;
-            if (want_probes && m > 0) append_probe_rows(s, t, hpr + (size_t)q * m * s->ny * 6, m, slot);
-            if (want_mon && t % 10 == 0) append_monitor_row(s, t, hdt[q], hmon + 6 * (size_t)q);
+            if (want_probes && m > 0) append_probe_rows(s, t, s->l_probe + (size_t)q * m * s->ny * 6, m, s->l_slot);
+            if (want_mon && t % 10 == 0) append_monitor_row(s, t, s->l_dt[q], s->l_mon + 6 * (size_t)q);
         }
-        s->dt = hdt[n - 1];
-        s->umax = hum[n - 1];
+        s->dt = s->l_dt[n - 1];
+        s->umax = s->l_umax[n - 1];
         s->t_loop += n;
         left -= n;
         const int tl = s->t_loop - 1;
@@ -519,19 +543,35 @@ int les_solver_run_device(les_solver* s, int nsteps, int chunk) {
             char path[1200];
             join_path(path, sizeof(path), s->out_dir, "checkpoint.bin");
             rc = les_solver_save_checkpoint(s, path, tl);
+            if (rc) return rc;
         }
     }
-    int t_back = 0;
-    int rc2 = lesgpu_loop_end(s->ctx, win, s->vort, &t_back);
-    if (rc2 == LESGPU_OK) {
-        for (int j = 0; j < 31; j++) s->rng.r[j] = (int)win[j];
-        s->rng.f = 0;
-        s->rng.b = 28;
-    }
-    free(hdt); free(hum); free(hmon); free(hpr);
-    if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
-    if (rc2) return serr(s, rc2, lesgpu_last_error(s->ctx));
     return LESGPU_OK;
+}
+
+int les_solver_loop_end(les_solver* s) {
+    if (!s) return LESGPU_EINVAL;
+    if (!s->loop_on) return LESGPU_OK;
+    unsigned int win[31];
+    int t_back = 0;
+    int rc = lesgpu_loop_end(s->ctx, win, s->vort, &t_back);
+    s->loop_on = 0;
+    loop_free(s);
+    if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
+    for (int j = 0; j < 31; j++) s->rng.r[j] = (int)win[j];
+    s->rng.f = 0;
+    s->rng.b = 28;
+    return LESGPU_OK;
+}
+
+int les_solver_run_device(les_solver* s, int nsteps, int chunk) {
+    if (!s || nsteps < 0) return LESGPU_EINVAL;
+    if (nsteps == 0) return LESGPU_OK;
+    int rc = les_solver_loop_begin(s, chunk);
+    if (rc) return rc;
+    rc = les_solver_loop_run(s, nsteps);
+    int rc2 = les_solver_loop_end(s);
+    return rc ? rc : rc2;
 }
 
 int les_solver_run(les_solver* s, int nsteps) {

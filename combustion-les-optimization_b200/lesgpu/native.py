@@ -140,6 +140,9 @@ def lib():
         _sig(L, "les_solver_step", C.c_int, [vp])
         _sig(L, "les_solver_run", C.c_int, [vp, C.c_int])
         _sig(L, "les_solver_run_device", C.c_int, [vp, C.c_int, C.c_int])
+        _sig(L, "les_solver_loop_begin", C.c_int, [vp, C.c_int])
+        _sig(L, "les_solver_loop_run", C.c_int, [vp, C.c_int])
+        _sig(L, "les_solver_loop_end", C.c_int, [vp])
         _sig(L, "lesgpu_loop_begin", C.c_int, [vp, vp, dp, C.c_int, C.c_int])
         _sig(L, "lesgpu_loop_config", C.c_int, [vp, vp, C.c_int, C.c_int, C.c_int])
         _sig(L, "lesgpu_run", C.c_int, [vp, C.c_int])
@@ -372,6 +375,15 @@ class Solver:
     def run_device(self, n: int, chunk: int = 64):
         """n steps with the host side on the GPU (graph-replayed, no per-step round trip)."""
         self._check(lib().les_solver_run_device(self._h, n, chunk), "run_device")
+
+    def loop_begin(self, chunk: int = 64):
+        self._check(lib().les_solver_loop_begin(self._h, chunk), "loop_begin")
+
+    def loop_run(self, n: int):
+        self._check(lib().les_solver_loop_run(self._h, n), "loop_run")
+
+    def loop_end(self):
+        self._check(lib().les_solver_loop_end(self._h), "loop_end")
 
     @property
     def t_loop(self) -> int:

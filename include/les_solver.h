@@ -68,6 +68,12 @@ int les_solver_run(les_solver* s, int nsteps);
  * queued in chunks of `chunk` steps (<= 0: 64) without a per-step host round trip; results,
  * rand() stream and output files are identical to les_solver_run. */
 int les_solver_run_device(les_solver* s, int nsteps, int chunk);
+/* The device loop as a session: begin (hands the rand() window and vortices to the GPU,
+ * sizes the history for `chunk` steps), any number of runs, end (hands them back).
+ * Host-driven steps are refused while a session is open. */
+int les_solver_loop_begin(les_solver* s, int chunk);
+int les_solver_loop_run(les_solver* s, int nsteps);
+int les_solver_loop_end(les_solver* s);
 
 int les_solver_t_loop(const les_solver* s);
 double les_solver_last_dt(const les_solver* s);
