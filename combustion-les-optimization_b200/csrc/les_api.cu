@@ -43,6 +43,12 @@ int cuda_fail(lesgpu_ctx* c, cudaError_t e, const char* where) {
         if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call);   \
     } while (0)
 
+#define CKC(c, call)                                               \
+    do {                                                           \
+        cudaError_t e_ = (call);                                   \
+        if (e_ != cudaSuccess) return cuda_fail((c), e_, #call);   \
+    } while (0)
+
 bool all_zero4(const double* c) { return c[0] == 0.0 && c[1] == 0.0 && c[2] == 0.0 && c[3] == 0.0; }
 
 // Constant table: grid spacings and the species/model constants in the form the kernels use.
@@ -301,7 +307,7 @@ int lesgpu_load_species(const char* chem_path, const char* tran_path, lesgpu_spe
 size_t lesgpu_bytes_for_grid(int nx, int ny, int nz, int precision) {
     size_t n = (size_t)nx * ny * nz;
     size_t esz = (precision == LESGPU_FP32) ? 4 : 8;
-    size_t nb = ((size_t)(nz + les::BX - 1) / les::BX) * ((ny + les::BY - 1) / les::BY) * nx;
+    size_t nb = les::max_cell_blocks(nx, ny, nz);
     if (nb < (size_t)les::MON_BLOCKS) nb = les::MON_BLOCKS;
     size_t planes = (size_t)ny * nz;
     return fields_for_precision() * n * esz + n +              // fields + attribute bytes
@@ -347,9 +353,9 @@ int lesgpu_create(const lesgpu_config* cfg, const lesgpu_species* sp, lesgpu_ctx
     d.aT = take(); d.nu_t = take(); d.S_mag = take(); d.ST = take(); d.mu_eff = take();
     for (int q = 0; q < les::NACC; q++) d.acc[q] = take();
     for (int q = 0; q < 4; q++) d.kflow[q] = take();
-    // per-block partials: 3 per block of the per-cell grid (filter pass) and 6 per block of
-    // the monitor grid
-    size_t nb = ((size_t)(d.nz + les::BX - 1) / les::BX) * ((d.ny + les::BY - 1) / les::BY) * d.nx;
+    // per-block partials: 3 per block of the per-cell grid (filter pass, any tile shape) and
+    // 6 per block of the monitor grid
+    size_t nb = les::max_cell_blocks(d.nx, d.ny, d.nz);
     d.part_len = 6 * (nb > (size_t)les::MON_BLOCKS ? nb : (size_t)les::MON_BLOCKS) + 64;
     size_t planes = (size_t)d.ny * d.nz;
     bool ok = cudaMalloc(&d.attr, d.n) == cudaSuccess &&
@@ -858,6 +864,194 @@ int lesgpu_selfcheck_division(const double* divisors, int nd, size_t n, unsigned
 int lesgpu_sync(lesgpu_ctx* ctx) {
     if (!ctx) return LESGPU_EINVAL;
     CK(cudaStreamSynchronize(ctx->d.stream));
+    return LESGPU_OK;
+}
+
+// ---------------------------------------------------------------- tiles and autotuning
+
+static void drop_graph(DevCtx& d) {
+    if (d.graph) cudaGraphExecDestroy(d.graph);
+    d.graph = nullptr;
+    d.graph_ok = false;
+}
+
+int lesgpu_set_tiles(lesgpu_ctx* ctx, const int tiles[5]) {
+    if (!ctx || !tiles) return LESGPU_EINVAL;
+    for (int q = 0; q < les::NSH_CLASSES; q++)
+        if (tiles[q] < 0 || tiles[q] >= les::NSHAPES) return fail(ctx, LESGPU_EINVAL, "tile index out of range");
+    DevCtx& d = ctx->d;
+    CK(cudaStreamSynchronize(d.stream));
+    for (int q = 0; q < les::NSH_CLASSES; q++) d.shape[q] = tiles[q];
+    drop_graph(d);
+    return LESGPU_OK;
+}
+
+int lesgpu_get_tiles(const lesgpu_ctx* ctx, int tiles[5]) {
+    if (!ctx || !tiles) return LESGPU_EINVAL;
+    for (int q = 0; q < les::NSH_CLASSES; q++) tiles[q] = ctx->d.shape[q];
+    return LESGPU_OK;
+}
+
+int lesgpu_autotune(lesgpu_ctx* ctx, int reps, int tiles_out[5], double* ms_out) {
+    if (!ctx || reps < 1) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    if (!d.have_state || !d.have_attr) return fail(ctx, LESGPU_ESTATE, "state and attribute map must be uploaded");
+    CK(cudaStreamSynchronize(d.stream));
+    // the stage kernels overwrite the dt inputs, <rho_f> and the step counters: keep a copy
+    les::Scalars saved;
+    CK(cudaMemcpy(&saved, d.dS, sizeof(saved), cudaMemcpyDeviceToHost));
+    const bool was_timing = d.timing;
+    int old[les::NSH_CLASSES];
+    for (int q = 0; q < les::NSH_CLASSES; q++) old[q] = d.shape[q];
+    const int cls_of[4] = {LESGPU_K_FILTER, LESGPU_K_STRAIN, LESGPU_K_RHS_FLOW, LESGPU_K_RHS_SCALAR};
+    double ms[4][les::NSHAPES];
+    cudaError_t e = cudaSuccess;
+    for (int t = 0; t < les::NSHAPES && e == cudaSuccess; t++) {
+        for (int q = 0; q < les::NSH_CLASSES; q++) d.shape[q] = t;
+        d.timing = false;
+        e = (d.precision == LESGPU_FP64) ? les::rhs_only_f64(d, 0) : les::rhs_only_f32(d, 0);   // warm-up
+        d.timing = true;
+        for (int q = 0; q < 8; q++) { d.kms[q] = 0.0; d.kcount[q] = 0; }
+        for (int r = 0; r < reps && e == cudaSuccess; r++)
+            e = (d.precision == LESGPU_FP64) ? les::rhs_only_f64(d, 0) : les::rhs_only_f32(d, 0);
+        for (int c = 0; c < 4; c++)
+            ms[c][t] = d.kcount[cls_of[c]] > 0 ? d.kms[cls_of[c]] / (double)d.kcount[cls_of[c]] : 1e30;
+    }
+    d.timing = was_timing;
+    for (int q = 0; q < 8; q++) { d.kms[q] = 0.0; d.kcount[q] = 0; }
+    cudaError_t e2 = cudaStreamSynchronize(d.stream);
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaMemcpy(d.dS, &saved, sizeof(saved), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        for (int q = 0; q < les::NSH_CLASSES; q++) d.shape[q] = old[q];
+        return cuda_fail(ctx, e, "autotune");
+    }
+    int best[les::NSH_CLASSES];
+    for (int c = 0; c < 4; c++) {
+        best[c] = 0;
+        for (int t = 1; t < les::NSHAPES; t++)
+            if (ms[c][t] < ms[c][best[c]]) best[c] = t;
+    }
+    best[les::SH_EOS] = best[les::SH_FILTER];
+    for (int q = 0; q < les::NSH_CLASSES; q++) d.shape[q] = best[q];
+    drop_graph(d);
+    if (tiles_out)
+        for (int q = 0; q < les::NSH_CLASSES; q++) tiles_out[q] = best[q];
+    if (ms_out)
+        for (int c = 0; c < 4; c++)
+            for (int t = 0; t < les::NSHAPES; t++) ms_out[c * les::NSHAPES + t] = ms[c][t];
+    return LESGPU_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- groups
+
+struct lesgpu_group {
+    std::vector<lesgpu_ctx*> m;
+    int device = 0;
+    cudaStream_t root = nullptr;
+    cudaEvent_t fork = nullptr, done = nullptr;
+    std::vector<cudaEvent_t> joins, ready;
+    cudaGraphExec_t exec = nullptr;
+};
+
+extern "C" {
+
+void lesgpu_group_destroy(lesgpu_group* g) {
+    if (!g) return;
+    if (g->root) cudaStreamSynchronize(g->root);
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    for (cudaEvent_t e : g->joins) if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : g->ready) if (e) cudaEventDestroy(e);
+    if (g->fork) cudaEventDestroy(g->fork);
+    if (g->done) cudaEventDestroy(g->done);
+    if (g->root) cudaStreamDestroy(g->root);
+    delete g;
+}
+
+int lesgpu_group_create(lesgpu_ctx* const* ctxs, int n, lesgpu_group** out) {
+    if (!ctxs || n < 1 || !out) return LESGPU_EINVAL;
+    *out = nullptr;
+    for (int q = 0; q < n; q++) {
+        if (!ctxs[q]) return LESGPU_EINVAL;
+        const DevCtx& d = ctxs[q]->d;
+        if (!d.loop_ready) return fail(ctxs[q], LESGPU_ESTATE, "group members need lesgpu_loop_begin first");
+        if (d.timing) return fail(ctxs[q], LESGPU_ESTATE, "group members must have kernel timing off");
+        if (ctxs[q]->cfg.device != ctxs[0]->cfg.device)
+            return fail(ctxs[q], LESGPU_EINVAL, "group members must share one device");
+        for (int r = 0; r < q; r++)
+            if (ctxs[r] == ctxs[q]) return fail(ctxs[q], LESGPU_EINVAL, "context listed twice in a group");
+    }
+    lesgpu_group* g = new (std::nothrow) lesgpu_group();
+    if (!g) return LESGPU_ENOMEM;
+    g->m.assign(ctxs, ctxs + n);
+    g->device = ctxs[0]->cfg.device;
+    lesgpu_ctx* c0 = ctxs[0];
+    cudaError_t e = cudaSetDevice(g->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&g->root, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->done, cudaEventDisableTiming);
+    g->joins.assign(n, nullptr);
+    g->ready.assign(n, nullptr);
+    for (int q = 0; q < n && e == cudaSuccess; q++) {
+        e = cudaEventCreateWithFlags(&g->joins[q], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->ready[q], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctxs[q]->d.stream);
+    }
+    if (e != cudaSuccess) { int r = cuda_fail(c0, e, "group_create"); lesgpu_group_destroy(g); return r; }
+    // capture: fork from the root stream into every member stream, one device-loop step per
+    // member, join back into the root
+    cudaGraph_t gr = nullptr;
+    e = cudaStreamBeginCapture(g->root, cudaStreamCaptureModeThreadLocal);
+    cudaError_t el = cudaSuccess;
+    if (e == cudaSuccess) {
+        el = cudaEventRecord(g->fork, g->root);
+        for (int q = 0; q < n && el == cudaSuccess; q++) {
+            DevCtx& d = ctxs[q]->d;
+            el = cudaStreamWaitEvent(d.stream, g->fork, 0);
+            if (el == cudaSuccess)
+                el = (d.precision == LESGPU_FP64) ? les::step_f64(d, 0.0, 0, true) : les::step_f32(d, 0.0, 0, true);
+            if (el == cudaSuccess) el = cudaEventRecord(g->joins[q], d.stream);
+            if (el == cudaSuccess) el = cudaStreamWaitEvent(g->root, g->joins[q], 0);
+        }
+        cudaError_t ee = cudaStreamEndCapture(g->root, &gr);
+        if (el == cudaSuccess) el = ee;
+    } else {
+        el = e;
+    }
+    if (el == cudaSuccess) el = cudaGraphInstantiate(&g->exec, gr, 0);
+    if (gr) cudaGraphDestroy(gr);
+    if (el != cudaSuccess) {
+        cudaGetLastError();
+        int r = cuda_fail(c0, el, "group capture");
+        lesgpu_group_destroy(g);
+        return r;
+    }
+    *out = g;
+    return LESGPU_OK;
+}
+
+int lesgpu_group_run(lesgpu_group* g, int nsteps) {
+    if (!g || nsteps < 0) return LESGPU_EINVAL;
+    if (nsteps == 0) return LESGPU_OK;
+    for (lesgpu_ctx* c : g->m) {
+        if (!c->d.loop_ready) return fail(c, LESGPU_ESTATE, "member's device-loop session has ended");
+        if (nsteps > c->d.loop_cap) return fail(c, LESGPU_EINVAL, "nsteps exceeds a member's history capacity");
+    }
+    lesgpu_ctx* c0 = g->m[0];
+    const int n = (int)g->m.size();
+    // order after each member's earlier work, then restart every member's history slot
+    for (int q = 0; q < n; q++) {
+        DevCtx& d = g->m[q]->d;
+        CKC(c0, cudaEventRecord(g->ready[q], d.stream));
+        CKC(c0, cudaStreamWaitEvent(g->root, g->ready[q], 0));
+        CKC(c0, cudaMemsetAsync((char*)d.dS + offsetof(les::Scalars, run_step), 0, sizeof(int), g->root));
+    }
+    for (int s = 0; s < nsteps; s++) CKC(c0, cudaGraphLaunch(g->exec, g->root));
+    // later work on a member's stream (history read-back, sync) waits for the replays
+    CKC(c0, cudaEventRecord(g->done, g->root));
+    for (int q = 0; q < n; q++) CKC(c0, cudaStreamWaitEvent(g->m[q]->d.stream, g->done, 0));
     return LESGPU_OK;
 }
 

@@ -11,6 +11,30 @@
 
 namespace les {
 
+// Thread-block tiles of the per-cell kernels, (k extent, j extent), 256 threads each.  Every
+// kernel indexes through blockDim, so the tile is a launch parameter chosen per kernel class
+// (lesgpu_set_tiles / lesgpu_autotune); the results do not depend on it except through the
+// order of the block partial sums of <rho_f>.
+struct Shape {
+    int bx, by;
+};
+constexpr int NSHAPES = 4;
+constexpr Shape kShapes[NSHAPES] = {{32, 8}, {64, 4}, {16, 16}, {128, 2}};
+enum { SH_FILTER = 0, SH_STRAIN = 1, SH_FLOW = 2, SH_SCALAR = 3, SH_EOS = 4, NSH_CLASSES = 5 };
+
+inline size_t blocks_for_shape(int nx, int ny, int nz, int s) {
+    const Shape t = kShapes[s];
+    return (size_t)((nz + t.bx - 1) / t.bx) * (size_t)((ny + t.by - 1) / t.by) * (size_t)nx;
+}
+inline size_t max_cell_blocks(int nx, int ny, int nz) {
+    size_t m = 0;
+    for (int s = 0; s < NSHAPES; s++) {
+        size_t b = blocks_for_shape(nx, ny, nz, s);
+        if (b > m) m = b;
+    }
+    return m;
+}
+
 struct DevCtx {
     int nx = 0, ny = 0, nz = 0, precision = 0;
     size_t n = 0;                       // cells
@@ -73,6 +97,7 @@ struct DevCtx {
     double lp_lbox = 0, lp_ly = 0, lp_lz = 0, lp_uin = 0, lp_ti = 0, lp_ell = 0, lp_cfl = 0, lp_cfld = 0, lp_dx = 0;
     cudaGraphExec_t graph = nullptr;    // one captured device-loop step
     bool graph_ok = false;
+    int shape[NSH_CLASSES] = {0, 0, 0, 0, 0};   // tile (index into kShapes) per kernel class
     // kernel timing: event pairs recorded around each kernel class during a step
     bool timing = false;
     std::vector<cudaEvent_t> ev_pool;

@@ -241,10 +241,10 @@ __global__ void __launch_bounds__(NT, LES_MINB_FILTER)
     __shared__ double sh[NT / 32];
     __shared__ bool last;
     const int nx = C.nx, ny = C.ny, nz = C.nz;
-    const int k = blockIdx.x * BX + threadIdx.x;
-    const int j = blockIdx.y * BY + threadIdx.y;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i = blockIdx.z;
-    const int tid = threadIdx.y * BX + threadIdx.x;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
     const ptrdiff_t sI = (ptrdiff_t)ny * nz, sJ = (ptrdiff_t)nz;
     double mass = 0.0, mnu = 0.0, mal = 0.0;
     if (k < nz && j < ny) {
@@ -326,8 +326,8 @@ template <typename R>
 __global__ void __launch_bounds__(NT, 3)
     k_strain(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> F, PropBuf<R> P) {
     const int nx = C.nx, ny = C.ny, nz = C.nz;
-    const int k = blockIdx.x * BX + threadIdx.x;
-    const int j = blockIdx.y * BY + threadIdx.y;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i = blockIdx.z;
     if (k >= nz || j >= ny) return;
     const ptrdiff_t sI = (ptrdiff_t)ny * nz, sJ = (ptrdiff_t)nz;
@@ -567,8 +567,8 @@ __global__ void __launch_bounds__(NT, LES_MINB_FLOW)
     k_rhs_flow(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> F, PropBuf<R> P, KFlow<R> kf,
                KDbg<R> kd, const Scalars* __restrict__ Sc) {
     const int nx = C.nx, ny = C.ny, nz = C.nz;
-    const int k = blockIdx.x * BX + threadIdx.x;
-    const int j = blockIdx.y * BY + threadIdx.y;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i = blockIdx.z;
     if (k >= nz || j >= ny) return;
     const ptrdiff_t sI = (ptrdiff_t)ny * nz, sJ = (ptrdiff_t)nz;
@@ -731,8 +731,8 @@ __global__ void __launch_bounds__(NT, LES_MINB_SCALAR)
     k_rhs_scalar(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> F, PropBuf<R> P, F11<R> S0, F11<R> St,
                  AccBuf<R> acc, KFlow<R> kf, KDbg<R> kd, const Scalars* __restrict__ Sc, int stage) {
     const int nx = C.nx, ny = C.ny, nz = C.nz;
-    const int k = blockIdx.x * BX + threadIdx.x;
-    const int j = blockIdx.y * BY + threadIdx.y;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i = blockIdx.z;
     if (k >= nz || j >= ny) return;
     const ptrdiff_t sI = (ptrdiff_t)ny * nz, sJ = (ptrdiff_t)nz;
@@ -964,10 +964,10 @@ __global__ void __launch_bounds__(NT) k_bc_eos(LES_KERNEL_CONSTS, const uint8_t*
     __shared__ double sh[NT / 32];
     __shared__ bool last;
     const int ny = C.ny, nz = C.nz;
-    const int k = blockIdx.x * BX + threadIdx.x;
-    const int j = blockIdx.y * BY + threadIdx.y;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i = blockIdx.z;
-    const int tid = threadIdx.y * BX + threadIdx.x;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
     double vmax = 0.0;
     if (k < nz && j < ny) {
         const size_t id = cid(i, j, k, ny, nz);
@@ -1024,10 +1024,10 @@ __global__ void __launch_bounds__(NT) k_umax(LES_KERNEL_CONSTS, const uint8_t* _
     __shared__ double sh[NT / 32];
     __shared__ bool last;
     const int ny = C.ny, nz = C.nz;
-    const int k = blockIdx.x * BX + threadIdx.x;
-    const int j = blockIdx.y * BY + threadIdx.y;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i = blockIdx.z;
-    const int tid = threadIdx.y * BX + threadIdx.x;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
     double vmax = 0.0;
     if (k < nz && j < ny) {
         const size_t id = cid(i, j, k, ny, nz);

@@ -31,8 +31,13 @@ static PropBuf<R> props(const DevCtx& c) {
     return P;
 }
 
-static inline dim3 cell_grid(const DevCtx& c) {
-    return dim3((unsigned)((c.nz + BX - 1) / BX), (unsigned)((c.ny + BY - 1) / BY), (unsigned)c.nx);
+static inline dim3 cell_block(const DevCtx& c, int cls) {
+    const Shape t = kShapes[c.shape[cls]];
+    return dim3((unsigned)t.bx, (unsigned)t.by);
+}
+static inline dim3 cell_grid(const DevCtx& c, int cls) {
+    const Shape t = kShapes[c.shape[cls]];
+    return dim3((unsigned)((c.nz + t.bx - 1) / t.bx), (unsigned)((c.ny + t.by - 1) / t.by), (unsigned)c.nx);
 }
 
 // Every launch that writes per-block partials checks the buffer first: `per_block` values
@@ -40,8 +45,8 @@ static inline dim3 cell_grid(const DevCtx& c) {
 static inline bool part_fits(const DevCtx& c, size_t blocks, size_t per_block) {
     return blocks * per_block <= c.part_len;
 }
-static inline size_t cell_blocks(const DevCtx& c) {
-    dim3 g = cell_grid(c);
+static inline size_t cell_blocks(const DevCtx& c, int cls) {
+    dim3 g = cell_grid(c, cls);
     return (size_t)g.x * g.y * g.z;
 }
 
@@ -52,8 +57,14 @@ static inline size_t cell_blocks(const DevCtx& c) {
 template <typename R>
 cudaError_t step_impl(DevCtx& c, double dt, int t_loop, bool device_mode) {
     cudaStream_t st = c.stream;
-    if (!part_fits(c, cell_blocks(c), 3) || !part_fits(c, MON_BLOCKS, 6)) return cudaErrorInvalidValue;
-    const dim3 g = cell_grid(c), b(BX, BY);
+    if (!part_fits(c, cell_blocks(c, SH_FILTER), 3) || !part_fits(c, cell_blocks(c, SH_EOS), 1) ||
+        !part_fits(c, MON_BLOCKS, 6))
+        return cudaErrorInvalidValue;
+    const dim3 gA = cell_grid(c, SH_FILTER), bA = cell_block(c, SH_FILTER);
+    const dim3 gB = cell_grid(c, SH_STRAIN), bB = cell_block(c, SH_STRAIN);
+    const dim3 gC = cell_grid(c, SH_FLOW), bC = cell_block(c, SH_FLOW);
+    const dim3 gD = cell_grid(c, SH_SCALAR), bD = cell_block(c, SH_SCALAR);
+    const dim3 gE = cell_grid(c, SH_EOS), bE = cell_block(c, SH_EOS);
     F11<R> S = f11<R>(c.S), St = f11<R>(c.St), F = f11<R>(c.F);
     PropBuf<R> P = props<R>(c);
     AccBuf<R> acc;
@@ -75,18 +86,18 @@ cudaError_t step_impl(DevCtx& c, double dt, int t_loop, bool device_mode) {
     for (int s = 0; s < 4; s++) {
         F11<R> in = (s == 0) ? S : St;
         tm = tmark_begin(c, 1);
-        k_filter_props<R><<<g, b, 0, st>>>(c.hC, c.attr, in, F, P, c.part, c.dS, s == 3 ? 1 : 0);
+        k_filter_props<R><<<gA, bA, 0, st>>>(c.hC, c.attr, in, F, P, c.part, c.dS, s == 3 ? 1 : 0);
         tmark_end(c, tm);
         tm = tmark_begin(c, 2);
-        k_strain<R><<<g, b, 0, st>>>(c.hC, c.attr, F, P);
+        k_strain<R><<<gB, bB, 0, st>>>(c.hC, c.attr, F, P);
         tmark_end(c, tm);
         // the k-arrays of the first stage are kept for inspection when requested
         const KDbg<R>& kds = (s == 0) ? kd : knone;
         tm = tmark_begin(c, 3);
-        k_rhs_flow<R><<<g, b, 0, st>>>(c.hC, c.attr, F, P, kf, kds, c.dS);
+        k_rhs_flow<R><<<gC, bC, 0, st>>>(c.hC, c.attr, F, P, kf, kds, c.dS);
         tmark_end(c, tm);
         tm = tmark_begin(c, 5);
-        k_rhs_scalar<R><<<g, b, 0, st>>>(c.hC, c.attr, F, P, S, St, acc, kf, kds, c.dS, s);
+        k_rhs_scalar<R><<<gD, bD, 0, st>>>(c.hC, c.attr, F, P, S, St, acc, kf, kds, c.dS, s);
         tmark_end(c, tm);
     }
     // apply_boundary_conditions (:2967-3161)
@@ -99,7 +110,7 @@ cudaError_t step_impl(DevCtx& c, double dt, int t_loop, bool device_mode) {
             k_bc_jface<R><<<dim3((c.nz + tpb - 1) / tpb, c.nx - 2), tpb, 0, st>>>(c.hC, c.attr, S);
             k_bc_kface<R><<<dim3((c.ny + tpb - 1) / tpb, c.nx - 2), tpb, 0, st>>>(c.hC, c.attr, S);
         }
-        k_bc_eos<R><<<g, b, 0, st>>>(c.hC, c.attr, S, c.part, c.dS);
+        k_bc_eos<R><<<gE, bE, 0, st>>>(c.hC, c.attr, S, c.part, c.dS);
     }
     if (device_mode) {
         const int tpb = 64;
@@ -113,13 +124,14 @@ cudaError_t step_impl(DevCtx& c, double dt, int t_loop, bool device_mode) {
     return cudaGetLastError();
 }
 
-// Stage-1 right-hand side at the current state with the inspection buffers filled; the
-// state itself is not advanced (dt = 0 leaves the stage state equal to Phi_n).
+// Stage-1 right-hand side at the current state with the inspection buffers filled (when
+// debug buffers exist); the state itself is not advanced (dt = 0 leaves the stage state
+// equal to Phi_n).  The four kernels are bracketed by the kernel-timing marks, which the
+// tile autotuner reads.
 template <typename R>
 cudaError_t rhs_only_impl(DevCtx& c, int t_loop) {
     cudaStream_t st = c.stream;
-    if (!part_fits(c, cell_blocks(c), 3)) return cudaErrorInvalidValue;
-    const dim3 g = cell_grid(c), b(BX, BY);
+    if (!part_fits(c, cell_blocks(c, SH_FILTER), 3)) return cudaErrorInvalidValue;
     F11<R> S = f11<R>(c.S), St = f11<R>(c.St), F = f11<R>(c.F);
     PropBuf<R> P = props<R>(c);
     AccBuf<R> acc;
@@ -129,17 +141,28 @@ cudaError_t rhs_only_impl(DevCtx& c, int t_loop) {
     KFlow<R> kf;
     for (int q = 0; q < 4; q++) kf.p[q] = (R*)c.kflow[q];
     k_set_step<<<1, 1, 0, st>>>(c.dS, 0.0, t_loop);
-    k_filter_props<R><<<g, b, 0, st>>>(c.hC, c.attr, S, F, P, c.part, c.dS, 1);
-    k_strain<R><<<g, b, 0, st>>>(c.hC, c.attr, F, P);
-    k_rhs_flow<R><<<g, b, 0, st>>>(c.hC, c.attr, F, P, kf, kd, c.dS);
-    k_rhs_scalar<R><<<g, b, 0, st>>>(c.hC, c.attr, F, P, S, St, acc, kf, kd, c.dS, 0);
+    int tm = tmark_begin(c, 1);
+    k_filter_props<R><<<cell_grid(c, SH_FILTER), cell_block(c, SH_FILTER), 0, st>>>(c.hC, c.attr, S, F, P, c.part,
+                                                                                   c.dS, 1);
+    tmark_end(c, tm);
+    tm = tmark_begin(c, 2);
+    k_strain<R><<<cell_grid(c, SH_STRAIN), cell_block(c, SH_STRAIN), 0, st>>>(c.hC, c.attr, F, P);
+    tmark_end(c, tm);
+    tm = tmark_begin(c, 3);
+    k_rhs_flow<R><<<cell_grid(c, SH_FLOW), cell_block(c, SH_FLOW), 0, st>>>(c.hC, c.attr, F, P, kf, kd, c.dS);
+    tmark_end(c, tm);
+    tm = tmark_begin(c, 5);
+    k_rhs_scalar<R><<<cell_grid(c, SH_SCALAR), cell_block(c, SH_SCALAR), 0, st>>>(c.hC, c.attr, F, P, S, St, acc,
+                                                                                   kf, kd, c.dS, 0);
+    tmark_end(c, tm);
+    tmark_flush(c);
     return cudaGetLastError();
 }
 
 template <typename R>
 cudaError_t umax_impl(DevCtx& c) {
-    if (!part_fits(c, cell_blocks(c), 1)) return cudaErrorInvalidValue;
-    k_umax<R><<<cell_grid(c), dim3(BX, BY), 0, c.stream>>>(c.hC, c.attr, f11<R>(c.S), c.part, c.dS);
+    if (!part_fits(c, cell_blocks(c, SH_EOS), 1)) return cudaErrorInvalidValue;
+    k_umax<R><<<cell_grid(c, SH_EOS), cell_block(c, SH_EOS), 0, c.stream>>>(c.hC, c.attr, f11<R>(c.S), c.part, c.dS);
     return cudaGetLastError();
 }
 

@@ -507,44 +507,64 @@ int les_solver_loop_begin(les_solver* s, int chunk) {
     return LESGPU_OK;
 }
 
-int les_solver_loop_run(les_solver* s, int nsteps) {
-    if (!s || nsteps < 0) return LESGPU_EINVAL;
+/* Length of the next chunk of a session with `left` steps to go: at most the history
+ * capacity, and ending on the next checkpoint step (t > 0, t % 50 == 0) when checkpoints
+ * are written. */
+int les_solver_next_chunk(const les_solver* s, int left) {
+    if (!s || left <= 0 || !s->loop_on) return 0;
+    int n = left < s->l_chunk ? left : s->l_chunk;
+    if ((s->out_flags & LES_OUT_CHECKPOINT) && s->out_dir[0]) {
+        for (int q = 0; q < n; q++) {
+            int t = s->t_loop + q;
+            if (t > 0 && t % 50 == 0) { n = q + 1; break; }
+        }
+    }
+    return n;
+}
+
+/* After n queued device-loop steps: read the step history back, write the probe and
+ * monitor rows, advance t_loop and write the checkpoint that ends the chunk. */
+int les_solver_loop_collect(les_solver* s, int n) {
+    if (!s || n < 0) return LESGPU_EINVAL;
     if (!s->loop_on) return serr(s, LESGPU_ESTATE, "les_solver_loop_begin first");
+    if (n > s->l_chunk) return serr(s, LESGPU_EINVAL, "more steps than the history holds");
+    if (n == 0) return LESGPU_OK;
     const int want_probes = (s->out_flags & LES_OUT_PROBES) && s->out_dir[0];
     const int want_mon = (s->out_flags & LES_OUT_MONITOR) && s->out_dir[0];
     const int want_ckpt = (s->out_flags & LES_OUT_CHECKPOINT) && s->out_dir[0];
     const int m = s->l_m;
-    int left = nsteps, rc = LESGPU_OK;
+    int rc = lesgpu_loop_history(s->ctx, n, s->l_dt, s->l_umax, want_probes ? s->l_probe : NULL,
+                                 want_mon ? s->l_mon : NULL);
+    if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
+    for (int q = 0; q < n; q++) {
+        const int t = s->t_loop + q;
+        if (want_probes && m > 0) append_probe_rows(s, t, s->l_probe + (size_t)q * m * s->ny * 6, m, s->l_slot);
+        if (want_mon && t % 10 == 0) append_monitor_row(s, t, s->l_dt[q], s->l_mon + 6 * (size_t)q);
+    }
+    s->dt = s->l_dt[n - 1];
+    s->umax = s->l_umax[n - 1];
+    s->t_loop += n;
+    const int tl = s->t_loop - 1;
+    if (want_ckpt && tl > 0 && tl % 50 == 0) {
+        char path[1200];
+        join_path(path, sizeof(path), s->out_dir, "checkpoint.bin");
+        rc = les_solver_save_checkpoint(s, path, tl);
+        if (rc) return rc;
+    }
+    return LESGPU_OK;
+}
+
+int les_solver_loop_run(les_solver* s, int nsteps) {
+    if (!s || nsteps < 0) return LESGPU_EINVAL;
+    if (!s->loop_on) return serr(s, LESGPU_ESTATE, "les_solver_loop_begin first");
+    int left = nsteps;
     while (left > 0) {
-        int n = left < s->l_chunk ? left : s->l_chunk;
-        if (want_ckpt) {
-            /* end the chunk on the next checkpoint step (t > 0, t % 50 == 0) */
-            for (int q = 0; q < n; q++) {
-                int t = s->t_loop + q;
-                if (t > 0 && t % 50 == 0) { n = q + 1; break; }
-            }
-        }
-        rc = lesgpu_run(s->ctx, n);
-        if (rc == LESGPU_OK)
-            rc = lesgpu_loop_history(s->ctx, n, s->l_dt, s->l_umax, want_probes ? s->l_probe : NULL,
-                                     want_mon ? s->l_mon : NULL);
+        const int n = les_solver_next_chunk(s, left);
+        int rc = lesgpu_run(s->ctx, n);
         if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
-        for (int q = 0; q < n; q++) {
-            const int t = s->t_loop + q;
-            if (want_probes && m > 0) append_probe_rows(s, t, s->l_probe + (size_t)q * m * s->ny * 6, m, s->l_slot);
-            if (want_mon && t % 10 == 0) append_monitor_row(s, t, s->l_dt[q], s->l_mon + 6 * (size_t)q);
-        }
-        s->dt = s->l_dt[n - 1];
-        s->umax = s->l_umax[n - 1];
-        s->t_loop += n;
+        rc = les_solver_loop_collect(s, n);
+        if (rc) return rc;
         left -= n;
-        const int tl = s->t_loop - 1;
-        if (want_ckpt && tl > 0 && tl % 50 == 0) {
-            char path[1200];
-            join_path(path, sizeof(path), s->out_dir, "checkpoint.bin");
-            rc = les_solver_save_checkpoint(s, path, tl);
-            if (rc) return rc;
-        }
     }
     return LESGPU_OK;
 }

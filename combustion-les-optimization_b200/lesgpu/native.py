@@ -30,6 +30,7 @@ _INSPECT = (["u_f", "v_f", "w_f", "T_f", "G_f", "rho_f"] + [f"Y{k}_f" for k in r
 FIELD_IDS.update({name: 100 + q for q, name in enumerate(_INSPECT)})
 
 ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "EIO", -5: "ESTATE", -6: "ENONFINITE"}
+LESGPU_EINVAL, LESGPU_ECUDA, LESGPU_ENOMEM, LESGPU_EIO, LESGPU_ESTATE, LESGPU_ENONFINITE = -1, -2, -3, -4, -5, -6
 
 LES_OUT_PROBES, LES_OUT_MONITOR, LES_OUT_CHECKPOINT = 1, 2, 4
 
@@ -143,6 +144,20 @@ def lib():
         _sig(L, "les_solver_loop_begin", C.c_int, [vp, C.c_int])
         _sig(L, "les_solver_loop_run", C.c_int, [vp, C.c_int])
         _sig(L, "les_solver_loop_end", C.c_int, [vp])
+        _sig(L, "les_solver_next_chunk", C.c_int, [vp, C.c_int])
+        _sig(L, "les_solver_loop_collect", C.c_int, [vp, C.c_int])
+        _sig(L, "lesgpu_autotune", C.c_int, [vp, C.c_int, vp, dp])
+        _sig(L, "lesgpu_set_tiles", C.c_int, [vp, vp])
+        _sig(L, "lesgpu_get_tiles", C.c_int, [vp, vp])
+        _sig(L, "lesgpu_group_create", C.c_int, [vp, C.c_int, C.POINTER(vp)])
+        _sig(L, "lesgpu_group_run", C.c_int, [vp, C.c_int])
+        _sig(L, "lesgpu_group_destroy", None, [vp])
+        _sig(L, "les_ensemble_create", C.c_int, [vp, C.c_int, C.c_char_p, C.c_char_p, C.c_int, C.POINTER(vp)])
+        _sig(L, "les_ensemble_run", C.c_int, [vp, C.c_int, C.c_int])
+        _sig(L, "les_ensemble_size", C.c_int, [vp])
+        _sig(L, "les_ensemble_member", vp, [vp, C.c_int])
+        _sig(L, "les_ensemble_last_error", C.c_char_p, [vp])
+        _sig(L, "les_ensemble_destroy", None, [vp])
         _sig(L, "lesgpu_loop_begin", C.c_int, [vp, vp, dp, C.c_int, C.c_int])
         _sig(L, "lesgpu_loop_config", C.c_int, [vp, vp, C.c_int, C.c_int, C.c_int])
         _sig(L, "lesgpu_run", C.c_int, [vp, C.c_int])
@@ -310,6 +325,26 @@ class Context:
         self._check(lib().lesgpu_elapsed_ms(self._h, a, b, C.byref(v)), "elapsed_ms")
         return v.value
 
+    # thread-block tiles (k extent, j extent) indexed by lesgpu_set_tiles, per class
+    # {filter, strain, rhs_flow, rhs_scalar, eos}
+    TILES = [(32, 8), (64, 4), (16, 16), (128, 2)]
+
+    def autotune(self, reps: int = 3):
+        """Install the fastest tile per kernel class; returns (tiles[5], ms[4 classes, 4 tiles])."""
+        tiles = np.zeros(5, dtype=np.int32)
+        ms = np.zeros(16)
+        self._check(lib().lesgpu_autotune(self._h, reps, tiles.ctypes.data, ms.ctypes.data), "autotune")
+        return tiles.tolist(), ms.reshape(4, 4)
+
+    def set_tiles(self, tiles):
+        t = np.ascontiguousarray(tiles, dtype=np.int32)
+        self._check(lib().lesgpu_set_tiles(self._h, t.ctypes.data), "set_tiles")
+
+    def get_tiles(self):
+        t = np.zeros(5, dtype=np.int32)
+        self._check(lib().lesgpu_get_tiles(self._h, t.ctypes.data), "get_tiles")
+        return t.tolist()
+
     KERNEL_CLASSES = ["sem", "filter_props", "strain", "rhs_flow", "bc", "rhs_scalar"]
 
     def kernel_timing(self, on: bool = True):
@@ -345,6 +380,20 @@ class Solver:
         self.ctx.shape = self.shape
         self.ctx._h = C.c_void_p(lib().les_solver_ctx(h))
 
+    @classmethod
+    def wrap(cls, handle, cfg: SolverConfig) -> "Solver":
+        """A view of a les_solver owned elsewhere (an ensemble member); close() only detaches."""
+        s = cls.__new__(cls)
+        s.cfg = cfg
+        s.shape = (cfg.nx, cfg.ny, cfg.nz)
+        s._h = C.c_void_p(handle)
+        s._owned = False
+        s.ctx = Context.__new__(Context)
+        s.ctx.cfg = cfg
+        s.ctx.shape = s.shape
+        s.ctx._h = C.c_void_p(lib().les_solver_ctx(s._h))
+        return s
+
     def _check(self, rc: int, what: str):
         if rc != 0:
             raise LesgpuError(rc, f"{what}: {lib().les_solver_last_error(self._h).decode()}")
@@ -352,7 +401,8 @@ class Solver:
     def close(self):
         if getattr(self, "_h", None):
             self.ctx._h = None
-            lib().les_solver_destroy(self._h)
+            if getattr(self, "_owned", True):
+                lib().les_solver_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -75,6 +75,7 @@ typedef struct lesgpu_species {
 } lesgpu_species;
 
 typedef struct lesgpu_ctx lesgpu_ctx;
+typedef struct lesgpu_group lesgpu_group;
 
 /* Field ids for lesgpu_get_field: the 11 state fields, then per-step diagnostics. */
 enum {
@@ -150,6 +151,20 @@ int lesgpu_run(lesgpu_ctx* ctx, int nsteps);
 int lesgpu_loop_history(lesgpu_ctx* ctx, int nsteps, double* dt, double* umax, double* probes, double* monitor);
 int lesgpu_loop_end(lesgpu_ctx* ctx, unsigned int rng_window[31], double* vortices, int* t_loop);
 
+/* Groups (no reference counterpart; the reference runs one LES per process, and its
+ * Bayesian optimiser runs trials one after another, bayesian_optimizer.py:568-673).  A group
+ * advances several contexts of one device together: one step of every member is captured
+ * once as a single multi-stream CUDA graph (each member on its own stream, branches
+ * independent), so members whose grids are too small to fill the GPU share it.  Every
+ * member must be in a device-loop session (lesgpu_loop_begin) with kernel timing off;
+ * lesgpu_group_run queues nsteps (<= each member's history capacity) replays and is
+ * asynchronous: each member's lesgpu_loop_history / lesgpu_sync waits for it.  A member's
+ * results are bit-identical to running it alone with the same tiles.  Changing a member's
+ * tiles or history layout after lesgpu_group_create requires a new group. */
+int lesgpu_group_create(lesgpu_ctx* const* ctxs, int n, lesgpu_group** out);
+int lesgpu_group_run(lesgpu_group* g, int nsteps);
+void lesgpu_group_destroy(lesgpu_group* g);
+
 /* Probe lines for record_flame_region_data (:3403-3471) and the point buffer (:4558-4569):
  * for each of n x-stations, NY rows of {u, v, w, G, nu_t, S_mag} on the line k = k_line.
  * out holds n * NY * 6 doubles. */
@@ -211,6 +226,19 @@ int lesgpu_kernel_times(lesgpu_ctx* ctx, double* ms, long long* launches, int n)
  * IEEE division.  Runs on the current device; allocates a few bytes of device memory. */
 int lesgpu_selfcheck_division(const double* divisors, int nd, size_t n, unsigned long long seed,
                               unsigned long long* mismatches);
+
+/* Thread-block tiles of the per-cell kernels (no reference counterpart; the reference is
+ * serial C).  tiles[c] for the classes {filter, strain, rhs_flow, rhs_scalar, eos} indexes
+ * the shapes 0 = 32x8, 1 = 64x4, 2 = 16x16, 3 = 128x2 (k extent x j extent, 256 threads).
+ * lesgpu_autotune times `reps` evaluations of the four stage kernels per shape at the
+ * current state, picks the fastest shape per class (eos follows filter), installs it and
+ * optionally returns it and the times (ms_out: 4 classes x 4 shapes, ms per launch).  It
+ * leaves the state, the dt inputs and the step counters as they were.  The tile changes
+ * only the launch geometry; results change only through the summation order of the block
+ * partials of <rho_f> (rounding level). */
+int lesgpu_set_tiles(lesgpu_ctx* ctx, const int tiles[5]);
+int lesgpu_get_tiles(const lesgpu_ctx* ctx, int tiles[5]);
+int lesgpu_autotune(lesgpu_ctx* ctx, int reps, int tiles_out[5], double* ms_out);
 
 /* Block until all work queued on the context's stream has finished. */
 int lesgpu_sync(lesgpu_ctx* ctx);

@@ -74,6 +74,13 @@ int les_solver_run_device(les_solver* s, int nsteps, int chunk);
 int les_solver_loop_begin(les_solver* s, int chunk);
 int les_solver_loop_run(les_solver* s, int nsteps);
 int les_solver_loop_end(les_solver* s);
+/* The two halves of les_solver_loop_run, for callers that queue the steps themselves (a
+ * group graph, les_ensemble_run): next_chunk gives the length of the next chunk of a
+ * session with `left` steps to go (history capacity, checkpoint steps); after those steps
+ * are queued, loop_collect reads their history back, writes the outputs and advances
+ * t_loop. */
+int les_solver_next_chunk(const les_solver* s, int left);
+int les_solver_loop_collect(les_solver* s, int nsteps);
 
 int les_solver_t_loop(const les_solver* s);
 double les_solver_last_dt(const les_solver* s);
@@ -90,6 +97,22 @@ int les_solver_load_checkpoint(les_solver* s, const char* path, int* t_out);
 /* Vortex table (nv x 7) and rand() draw count, for inspection. */
 int les_solver_vortices(const les_solver* s, double* out);
 unsigned long long les_solver_rng_draws(const les_solver* s);
+
+/* Ensembles (no reference counterpart as an API: the reference's Bayesian optimiser runs
+ * one LES per parameter proposal, bayesian_optimizer.py:568-673).  n solvers with their own
+ * configs (grids, model constants, seeds) on one device, all advanced by one multi-stream
+ * graph per step (lesgpu_group_*).  autotune != 0 picks each member's tiles at creation
+ * (lesgpu_autotune).  les_ensemble_run advances every member by nsteps in chunks of
+ * `chunk` steps (<= 0: 64), writing each member's enabled outputs as les_solver_run_device
+ * does; each member's results equal running it alone with the same tiles. */
+typedef struct les_ensemble les_ensemble;
+int les_ensemble_create(const lesgpu_config* cfgs, int n, const char* chem_path, const char* tran_path, int autotune,
+                        les_ensemble** out);
+int les_ensemble_run(les_ensemble* e, int nsteps, int chunk);
+int les_ensemble_size(const les_ensemble* e);
+les_solver* les_ensemble_member(les_ensemble* e, int i);
+const char* les_ensemble_last_error(const les_ensemble* e);
+void les_ensemble_destroy(les_ensemble* e);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,150 @@
+"""Ensembles, group graphs and tile selection on the GPU.
+
+* members advanced together by one multi-stream graph per step give bit-identical states
+  and output files to the same members run alone with the same tiles;
+* the thread-block tile changes results only through the summation order of <rho_f>
+  (relative L2 difference at rounding level, 1e-13 after three steps);
+* lesgpu_autotune leaves the state, the dt inputs and the counters as they were.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+STATE = ["u", "v", "w", "T", "G", "rho", "Y0", "Y1", "Y2", "Y3", "Y4"]
+TOL_TILE = 1e-13
+
+
+@pytest.fixture(scope="module")
+def N(lesgpu_native, cuda_device):
+    return lesgpu_native
+
+
+def rel(a, b):
+    nb = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
+
+
+def _files(d):
+    return {f: open(os.path.join(d, f), "rb").read() for f in sorted(os.listdir(d))}
+
+
+def test_ensemble_members_match_solo_runs(N, tmp_path):
+    from lesgpu.config import preset
+    from lesgpu.ensemble import Ensemble
+    cfgs = [preset("tiny", seed=11, cs_unburned=0.09, relax=2500.0),
+            preset("small", seed=12, accel_strength=3.5),
+            preset("c1", seed=13, cs_unburned=0.2, relax=100.0)]
+    ens = Ensemble(cfgs, precision=N.FP64, autotune=True)
+    dirs = []
+    for q, m in enumerate(ens.members):
+        d = tmp_path / f"ens{q}"
+        d.mkdir()
+        m.set_outputs(str(d), N.LES_OUT_PROBES | N.LES_OUT_MONITOR)
+        dirs.append(str(d))
+    ens.run(12, chunk=5)
+    got = [m.state() for m in ens.members]
+    tiles = [m.ctx.get_tiles() for m in ens.members]
+    t_loops = [m.t_loop for m in ens.members]
+    ens.close()
+    for q, (cfg, st, tl) in enumerate(zip(cfgs, got, tiles)):
+        assert all(0 <= t < 4 for t in tl)
+        solo = N.Solver(cfg)
+        solo.ctx.set_tiles(tl)
+        d = tmp_path / f"solo{q}"
+        d.mkdir()
+        solo.set_outputs(str(d), N.LES_OUT_PROBES | N.LES_OUT_MONITOR)
+        solo.run_device(12, chunk=12)
+        ref = solo.state()
+        assert t_loops[q] == solo.t_loop == 12
+        for f in STATE:
+            np.testing.assert_array_equal(st[f], ref[f], err_msg=f"member {q}: {f}")
+        assert _files(dirs[q]) == _files(str(d)), f"member {q}: output files differ"
+        solo.close()
+
+
+def test_ensemble_continues_across_runs(N):
+    """Two ensemble runs in a row equal one run of the summed length."""
+    from lesgpu.config import preset
+    from lesgpu.ensemble import Ensemble
+    cfgs = [preset("tiny", seed=3), preset("small", seed=4)]
+    a = Ensemble(cfgs, precision=N.FP64, autotune=False)
+    a.run(4, chunk=4)
+    a.run(5, chunk=3)
+    sa = [m.state() for m in a.members]
+    a.close()
+    b = Ensemble(cfgs, precision=N.FP64, autotune=False)
+    b.run(9, chunk=9)
+    sb = [m.state() for m in b.members]
+    b.close()
+    for x, y in zip(sa, sb):
+        for f in STATE:
+            np.testing.assert_array_equal(x[f], y[f])
+
+
+def test_tiles_change_only_rounding(N):
+    from lesgpu.config import preset
+    cfg = preset("small")
+    ref = None
+    for t in range(4):
+        s = N.Solver(cfg)
+        s.ctx.set_tiles([t] * 5)
+        assert s.ctx.get_tiles() == [t] * 5
+        s.step(3)
+        st = s.state()
+        s.close()
+        if ref is None:
+            ref = st
+            continue
+        for f in STATE:
+            assert rel(st[f], ref[f]) < TOL_TILE, (t, f, rel(st[f], ref[f]))
+
+
+def test_autotune_leaves_state_and_dt_inputs(N):
+    from lesgpu.config import preset
+    cfg = preset("small", seed=5)
+    a = N.Solver(cfg)
+    a.step(2)
+    before = a.ctx.dt_inputs()
+    tiles, ms = a.ctx.autotune(reps=2)
+    assert len(tiles) == 5 and all(0 <= t < 4 for t in tiles)
+    assert ms.shape == (4, 4) and np.all(ms > 0) and np.all(np.isfinite(ms))
+    assert tiles[4] == tiles[0]
+    for c in range(4):
+        assert ms[c, tiles[c]] == ms[c].min()
+    assert a.ctx.dt_inputs() == before
+    a.step(3)
+    b = N.Solver(cfg)
+    b.step(2)
+    b.ctx.set_tiles(tiles)
+    b.step(3)
+    sa, sb = a.state(), b.state()
+    for f in STATE:
+        np.testing.assert_array_equal(sa[f], sb[f], err_msg=f)
+    assert a.t_loop == b.t_loop == 5
+    a.close()
+    b.close()
+
+
+def test_group_requires_loop_sessions(N):
+    from lesgpu.config import preset
+    L = N.lib()
+    s = N.Solver(preset("tiny"))
+    arr = (C.c_void_p * 1)(s.ctx._h.value)
+    g = C.c_void_p()
+    assert L.lesgpu_group_create(arr, 1, C.byref(g)) == N.LESGPU_ESTATE
+    s.loop_begin(chunk=4)
+    assert L.lesgpu_group_create(arr, 1, C.byref(g)) == 0
+    assert L.lesgpu_group_run(g, 5) == N.LESGPU_EINVAL      # beyond the history capacity
+    assert L.lesgpu_group_run(g, 2) == 0
+    L.lesgpu_group_destroy(g)
+    s.loop_end()
+    assert s.t_loop == 0        # steps queued through the raw group are not collected
+    dup = (C.c_void_p * 2)(s.ctx._h.value, s.ctx._h.value)
+    s.loop_begin(chunk=4)
+    assert L.lesgpu_group_create(dup, 2, C.byref(g)) == N.LESGPU_EINVAL
+    s.loop_end()
+    s.close()

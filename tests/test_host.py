@@ -123,3 +123,18 @@ def test_presets_match_reference_build_configs():
         assert c.num_vortices == m["nv"] and c.initial_flame_front_i == m["i_f"]
         assert c.inlet_velocity == m["u_in"] and c.turbulence_intensity == m["ti"]
         assert c.length_scale == m["ell"] and c.courant == m["courant"]
+
+
+def test_ensemble_parameter_sets():
+    """The batched-ensemble workload: 64 sets, CS_UNBURNED in [0.08, 0.22], strength in
+    [0, 2] x default, nudging in [0, 1] x default, grids alternating, reproducible."""
+    from lesgpu.ensemble import ensemble_configs
+    a, b = ensemble_configs(64, seed=5), ensemble_configs(64, seed=5)
+    assert [c.as_dict() for c in a] == [c.as_dict() for c in b]
+    assert sum(1 for c in a if (c.nx, c.ny, c.nz) == (128, 64, 64)) == 32
+    assert sum(1 for c in a if (c.nx, c.ny, c.nz) == (96, 48, 48)) == 32
+    assert all(0.08 <= c.cs_unburned <= 0.22 for c in a)
+    assert all(0.0 <= c.accel_strength <= 2 * 2.0361 for c in a)
+    assert all(0.0 <= c.relax <= 5000.0 for c in a)
+    assert len({c.seed for c in a}) == 64
+    assert ensemble_configs(64, seed=6)[0].cs_unburned != a[0].cs_unburned
