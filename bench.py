@@ -57,7 +57,10 @@ KERNEL_BYTES_PER_CELL = {
     "bc": (9 + 6) * 8,                        # EOS pass over all cells dominates the BC class
     "sem": 0,
 }
-STEP_BYTES_PER_CELL = 1664                    # SURVEY 8(d) convention, FP64, per cell-step
+# Whole step, FP64: per RK stage read the stage state (11 fields), Phi_n (10) and the RK
+# accumulator (10), write the accumulator (10) and the next stage state (11): 52 field
+# accesses x 4 stages x 8 B = 1664 B per cell-step (832 B with 4-byte fields).
+STEP_BYTES_PER_CELL = 1664
 
 
 def _peaks():
@@ -252,6 +255,11 @@ def run_ours(args):
     esz = 4 if prec == N.FP32 else 8
     sol = N.Solver(cfg, precision=prec, device=local)
     ctx = sol.ctx
+    # thread-block tile per kernel class: timed on this GPU at the initial state
+    if args.tiles == "auto":
+        ctx.autotune(3)
+    tiles = {k: "x".join(map(str, ctx.TILES[t])) for k, t in
+             zip(["filter_props", "strain", "rhs_flow", "rhs_scalar", "eos"], ctx.get_tiles())}
     # per step: loop_pre, 2 SEM, 4 x 4 stage kernels, 4 BC, loop_post, loop_monitor, loop_tick
     per_step_launches = 1 + 2 + 16 + 4 + 3
 
@@ -358,7 +366,8 @@ def run_ours(args):
             "data": "synthetic: the reference's initial flame state, seeded SEM inflow, placeholder species properties",
             "config": {"workload": WORKLOADS.get(args.workload, args.workload), "grid": [cfg.nx, cfg.ny, cfg.nz],
                        "cells": cfg.cells, "precision": args.precision, "parallelism": f"replicas x{world}",
-                       "l2": f"inputs larger than L2 ({ctx.device_bytes / 2**30:.2f} GiB resident per replica)"},
+                       "l2": f"inputs larger than L2 ({ctx.device_bytes / 2**30:.2f} GiB resident per replica)",
+                       "tiles": tiles},
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
@@ -387,6 +396,8 @@ def main(argv=None) -> int:
     ap.add_argument("--workload", default="c2")
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tiles", choices=["auto", "default"], default="auto",
+                    help="auto: per-class thread-block tiles picked by lesgpu_autotune; default: 32x8 everywhere")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3
