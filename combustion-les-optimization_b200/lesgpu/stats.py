@@ -23,6 +23,7 @@ history.  All statistics are computed in float64 with numpy.
 """
 from __future__ import annotations
 
+import io
 import os
 from typing import Dict, Optional
 
@@ -37,7 +38,12 @@ def read_probe_csv(path: str) -> Dict[str, np.ndarray]:
         header = fp.readline().strip().split(",")
     if header != COLUMNS:
         raise ValueError(f"{path}: unexpected header {header}")
-    data = np.loadtxt(path, delimiter=",", skiprows=1, ndmin=2)
+    with open(path) as fp:
+        fp.readline()
+        body = fp.read()
+    if not body.strip():
+        return {c: np.zeros(0) for c in COLUMNS}
+    data = np.loadtxt(io.StringIO(body), delimiter=",", ndmin=2)
     if data.size == 0:
         return {c: np.zeros(0) for c in COLUMNS}
     return {c: data[:, q].astype(np.float64) for q, c in enumerate(COLUMNS)}

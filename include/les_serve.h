@@ -1,0 +1,85 @@
+/*
+ * les_serve.h -- serving loop: many LES solve requests on one GPU, admitted by an HBM
+ * budget and advanced together (continuous batching).
+ *
+ * No counterpart in the reference, which runs one solve per process (main(),
+ * les_combustion_solver.c:4016-4632).  Each request is one les_solver (les_solver.h) with
+ * its own grid, model constants, seed, rand() stream and output files; its results are the
+ * same as running it alone with les_solver_run_device.  One host thread drives a server.
+ *
+ *   les_serve_submit   queue a request (refused at once if it can never fit the budget);
+ *   les_serve_step     one scheduling round: admit queued requests in arrival order while a
+ *                      slot is free and their memory fits, queue up to quantum_steps steps
+ *                      of every active request (one stream and graph each, overlapping on
+ *                      the device), collect their step histories, retire finished ones
+ *                      (final state copied to the host when results are kept, device
+ *                      memory returned at once).  Returns the number of requests still
+ *                      queued or active (>= 0) or a negative LESGPU_E* code;
+ *   les_serve_cancel   drop a queued or active request between rounds;
+ *   les_serve_info / les_serve_result / les_serve_release / les_serve_stats.
+ * Latency is completion time minus submission time (CLOCK_MONOTONIC); p50/p99 use linear
+ * interpolation between order statistics.
+ */
+#ifndef LES_SERVE_H
+#define LES_SERVE_H
+
+#include <stddef.h>
+
+#include "les_solver.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { LES_REQ_QUEUED = 0, LES_REQ_ACTIVE = 1, LES_REQ_DONE = 2, LES_REQ_CANCELLED = 3, LES_REQ_FAILED = 4 };
+
+typedef struct les_serve_options {
+    size_t budget_bytes;      /* HBM the server may hand to requests */
+    int max_slots;            /* at most this many active requests */
+    int quantum_steps;        /* steps per request per round */
+    int keep_results;         /* copy each final state to the host (les_serve_result) */
+    int autotune;             /* tiles per grid size, timed on its first request and reused */
+    int backfill;             /* admit later requests that fit while the head of the queue waits */
+    int device;
+    char chem_path[1024];
+    char tran_path[1024];
+} les_serve_options;
+
+typedef struct les_serve_request_info {
+    int state, error, steps_done, nsteps;
+    size_t bytes;             /* budgeted bytes */
+    size_t device_bytes;      /* bytes the solver holds (active requests) */
+    double t_submit, t_admit, t_done, latency_s;
+} les_serve_request_info;
+
+typedef struct les_serve_summary {
+    long long submitted, queued, active, done, failed, cancelled;
+    size_t bytes_in_use;
+    double cell_steps;        /* cell-steps completed */
+    double busy_s;            /* first admission to last completion */
+    double cell_steps_per_s;
+    double latency_p50_s, latency_p99_s, latency_max_s;
+} les_serve_summary;
+
+typedef struct les_serve les_serve;
+
+void les_serve_default_options(les_serve_options* opt);
+/* Device bytes the server budgets for one request (grid fields, device-loop tables). */
+size_t les_serve_request_bytes(const lesgpu_config* cfg, int quantum_steps);
+int les_serve_create(const les_serve_options* opt, les_serve** out);
+int les_serve_submit(les_serve* s, const lesgpu_config* cfg, int nsteps, const char* out_dir, int out_flags,
+                     long long* id);
+int les_serve_step(les_serve* s);
+int les_serve_cancel(les_serve* s, long long id);
+int les_serve_info(les_serve* s, long long id, les_serve_request_info* info);
+int les_serve_result(les_serve* s, long long id, double* const* fields, int nfields);
+int les_serve_release(les_serve* s, long long id);
+int les_serve_stats(les_serve* s, les_serve_summary* st);
+const char* les_serve_last_error(const les_serve* s);
+void les_serve_destroy(les_serve* s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LES_SERVE_H */
