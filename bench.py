@@ -145,12 +145,13 @@ class Clocks:
         return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def _dist():
+def _dist(backend: str = "nccl"):
+    """Rank, local rank and world size from the torchrun environment; joins the process group
+    (NCCL on the GPU box, gloo for the CPU tests) when there is more than one rank."""
     import torch.distributed as dist
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if world > 1 and not dist.is_initialized():
         import datetime
-        backend = "nccl"
         dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -162,9 +163,17 @@ def _max_over_ranks(x: float, world: int) -> float:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_throughput(cells: int, steps: int, ms_local: float, world: int):
+    """Replicas only: every rank advances its own copy of the workload, so the job processed
+    world x cells x steps cell-steps in the slowest rank's device time."""
+    ms_max = _max_over_ranks(ms_local, world)
+    return ms_max, world * cells * steps / (ms_max / 1e3)
 
 
 def _barrier(world: int):
@@ -285,8 +294,7 @@ def run_ours(args):
     clk = clocks.stop() if clocks else None
     sol.loop_end()
     _barrier(world)
-    ms_max = _max_over_ranks(ms, world)
-    value = world * cfg.cells * args.steps / (ms_max / 1e3)
+    ms_max, value = replica_throughput(cfg.cells, args.steps, ms, world)
 
     # ---- roofline: per-kernel-class device time over a few further steps
     ctx.kernel_timing(True)

@@ -228,11 +228,7 @@ static int finish(les_serve* s, serve_req* q) {
     return rc;
 }
 
-int les_serve_step(les_serve* s) {
-    if (!s) return LESGPU_EINVAL;
-    /* 1. admission, in arrival order */
-    while (s->head < s->n && s->reqs[s->head]->state != LES_REQ_QUEUED && s->reqs[s->head]->state != LES_REQ_ACTIVE)
-        s->head++;
+static void admit_queued(les_serve* s) {
     for (long long i = s->head; i < s->n && s->n_active < s->opt.max_slots; i++) {
         serve_req* q = s->reqs[i];
         if (q->state != LES_REQ_QUEUED) continue;
@@ -244,7 +240,16 @@ int les_serve_step(les_serve* s) {
         if (rc == LESGPU_ENOMEM && s->n_active > 0) break;   /* the device is fuller than budgeted: wait */
         if (rc) retire(s, q, LES_REQ_FAILED, rc);
     }
-    /* 2. queue one quantum of every active request (asynchronous, one stream each) */
+}
+
+int les_serve_step(les_serve* s) {
+    if (!s) return LESGPU_EINVAL;
+    while (s->head < s->n && s->reqs[s->head]->state != LES_REQ_QUEUED && s->reqs[s->head]->state != LES_REQ_ACTIVE)
+        s->head++;
+    /* with nothing running there is nothing to overlap: admit first */
+    const int admit_early = (s->n_active == 0);
+    if (admit_early) admit_queued(s);
+    /* 1. queue one quantum of every active request (asynchronous, one stream each) */
     int* qn = NULL;
     serve_req** act = NULL;
     int na = 0;
@@ -272,6 +277,9 @@ int les_serve_step(les_serve* s) {
             na++;
         }
     }
+    /* 2. admission, in arrival order, while the quanta just queued run on the device (the
+     *    host-side set-up of a new request overlaps them); new requests join next round */
+    if (!admit_early) admit_queued(s);
     /* 3. collect histories and retire finished requests */
     for (int a = 0; a < na; a++) {
         serve_req* q = act[a];

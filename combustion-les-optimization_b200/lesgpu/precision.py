@@ -8,10 +8,10 @@ and the final state fields.
 
 The flow is chaotic: any perturbation, even at rounding level, grows until the two
 trajectories decorrelate, after which their statistics differ by sampling noise alone.  A
-third run separates that floor from the precision error: the FP64 form again with other
-thread-block tiles, which changes only the summation order of the <rho_f> block partials
-(differences of 1e-16 relative at the first step).  Its profile differences against the
-first FP64 run are reported beside the FP32 ones as ``floor_fp64_reordered``.
+third run separates that floor from the precision error: the FP64 form again from an initial
+temperature field scaled by (1 + 1e-15), a rounding-level perturbation.  Its profile
+differences against the first FP64 run are reported beside the FP32 ones as
+``profiles_floor_fp64_perturbed``.
 """
 from __future__ import annotations
 
@@ -43,10 +43,12 @@ def _pool(directory: str) -> Dict[str, np.ndarray]:
 
 
 def run_form(cfg: SolverConfig, precision: int, steps: int, directory: str, chunk: int = 64, device: int = 0,
-             tiles=None):
+             perturb: float = 0.0):
     s = N.Solver(cfg, precision=precision, device=device)
-    if tiles is not None:
-        s.ctx.set_tiles(tiles)
+    if perturb:
+        st = s.state()
+        st["T"] = st["T"] * (1.0 + perturb)
+        s.ctx.upload_state(st)
     s.set_outputs(directory, N.LES_OUT_PROBES | N.LES_OUT_MONITOR)
     t = time.perf_counter()
     s.run_device(steps, chunk=chunk)
@@ -70,17 +72,17 @@ def compare(cfg: SolverConfig, steps: int, workdir: Optional[str] = None, chunk:
     dirs = {k: os.path.join(workdir, k) for k in ("fp64", "fp32", "fp64_alt")}
     for d in dirs.values():
         os.makedirs(d, exist_ok=True)
-    s64, w64 = run_form(cfg, N.FP64, steps, dirs["fp64"], chunk, tiles=[0] * 5)
-    s32, w32 = run_form(cfg, N.FP32, steps, dirs["fp32"], chunk, tiles=[0] * 5)
+    s64, w64 = run_form(cfg, N.FP64, steps, dirs["fp64"], chunk)
+    s32, w32 = run_form(cfg, N.FP32, steps, dirs["fp32"], chunk)
     r64, r32 = _pool(dirs["fp64"]), _pool(dirs["fp32"])
     out = {"grid": [cfg.nx, cfg.ny, cfg.nz], "steps": steps, "rows_fp64": int(len(r64["u"])),
            "rows_fp32": int(len(r32["u"])), "wall_s": {"fp64": w64, "fp32": w32},
            "profiles_fp32": stats.compare_profiles(r32, r64), "state_rel_l2_fp32": _state_err(s32, s64)}
     if floor:
-        salt, walt = run_form(cfg, N.FP64, steps, dirs["fp64_alt"], chunk, tiles=[2] * 5)
+        salt, walt = run_form(cfg, N.FP64, steps, dirs["fp64_alt"], chunk, perturb=1e-15)
         ralt = _pool(dirs["fp64_alt"])
         out["wall_s"]["fp64_alt"] = walt
-        out["profiles_floor_fp64_reordered"] = stats.compare_profiles(ralt, r64)
+        out["profiles_floor_fp64_perturbed"] = stats.compare_profiles(ralt, r64)
         out["state_rel_l2_floor"] = _state_err(salt, s64)
     return out
 
