@@ -112,8 +112,12 @@ class Clocks:
         fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
         os.close(fd)
         self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                      "--format=csv,noheader,nounits", "-lms", "100"],
                                      stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        # wait for the first sample so that the timed region is covered from its start
+        t0 = time.time()
+        while time.time() - t0 < 3.0 and os.path.getsize(self.path) == 0:
+            time.sleep(0.05)
 
     def stop(self):
         if self.proc is None:
@@ -398,7 +402,7 @@ def run_ours(args):
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="c2")

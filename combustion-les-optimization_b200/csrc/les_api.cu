@@ -130,6 +130,8 @@ void build_consts(const lesgpu_config& g, const lesgpu_species& sp, les::Consts&
         C.d_mwk[a] = dc(C.mwk[a]);
         for (int b = 0; b < les::NSP; b++) C.d_wden[a][b] = dc(C.wden[a][b]);
     }
+    C.ssr_exp = 2.0 - C.d3;                                             // :1946
+    les::fill_float_consts(C);
 }
 
 unsigned char* read_record(FILE* fp, int* len) {

@@ -35,8 +35,33 @@ constexpr double SSR_A = 0.2340, SSR_B = 0.2187;
 // by one fma correction q + (x - q*c)*r (Markstein's iteration), which returns the
 // correctly rounded quotient for normal operands -- the same bits as IEEE division -- in
 // 3 FP64 operations instead of a division sequence.
-struct DC {
-    double c, r;
+template <typename T>
+struct DCT {
+    T c, r;
+};
+using DC = DCT<double>;
+
+// Constants that enter the per-cell arithmetic.  The FP32 form reads float copies of them
+// (ConstsF, filled on the host), so no double-to-float conversion runs per cell; the FP64
+// form reads the double originals.  X(name, dims) for values, XD(name, dims) for divisors.
+#define LES_FCONSTS(X, XD)                                                                      \
+    X(dx, ) X(dy, ) X(dz, ) X(dx4, ) X(inlet_center_z, )                                          \
+    X(mwk, [NSP]) X(t_mid, [NSP]) X(nasa_high, [NSP][7]) X(nasa_low, [NSP][7])                  \
+    X(eta, [NSP][4]) X(lam, [NSP][4]) X(dco, [NSP][NSP][4]) X(wpow, [NSP][NSP])                  \
+    X(cs_u, ) X(cs_b, ) X(cs_boost, ) X(accel_strength, ) X(accel_center, ) X(relax, )           \
+    X(s_l, ) X(ssr_cdF, ) X(ssr_exp, ) X(tau_sl, ) X(t_in, ) X(t_amb, ) X(t_burnt_span, )        \
+    X(inletYk, [NSP]) X(ambientYk, [NSP]) X(cons_o2, ) X(prod_co2, ) X(prod_h2o, )               \
+    X(u_in, ) X(noise_amp, )                                                                     \
+    XD(d_dx, ) XD(d_dy, ) XD(d_dz, ) XD(d_2dx, ) XD(d_2dy, ) XD(d_2dz, ) XD(d_dxx, ) XD(d_dyy, ) \
+    XD(d_dzz, ) XD(d_six, ) XD(d_filter, ) XD(d_sct2, ) XD(d_prt2, ) XD(d_ramp, ) XD(d_w2, )      \
+    XD(d_tau_sl, ) XD(d_mwk, [NSP]) XD(d_wden, [NSP][NSP])
+
+struct ConstsF {
+#define LES_DECL_F(name, dims) float name dims;
+#define LES_DECL_FD(name, dims) DCT<float> name dims;
+    LES_FCONSTS(LES_DECL_F, LES_DECL_FD)
+#undef LES_DECL_F
+#undef LES_DECL_FD
 };
 
 // Per-context constants, passed to every kernel by value (__grid_constant__), so reads go
@@ -77,7 +102,41 @@ struct Consts {
     double cons_o2, prod_co2, prod_h2o; // inletYk[C3H8] * stoich
     double u_in, noise_amp;             // INLET_VELOCITY, 0.10*INLET_VELOCITY
     double ti_rms;                      // INLET_VELOCITY * INLET_TURBULENCE_INTENSITY
+    double ssr_exp;                     // 2.0 - D3, the SSR-SGS wrinkling exponent
+    ConstsF f;                          // float copies for the FP32 form
 };
+
+// The constant set a kernel of field type R computes with: Consts itself for double, its
+// float copies for float.
+template <typename R>
+struct KSel;
+template <>
+struct KSel<double> {
+    using type = Consts;
+    __host__ __device__ static const Consts& get(const Consts& C) { return C; }
+};
+template <>
+struct KSel<float> {
+    using type = ConstsF;
+    __host__ __device__ static const ConstsF& get(const Consts& C) { return C.f; }
+};
+template <typename R>
+__host__ __device__ __forceinline__ const typename KSel<R>::type& kc(const Consts& C) {
+    return KSel<R>::get(C);
+}
+
+// Host: fill C.f from the double values.
+inline void to_float(float& d, double s) { d = (float)s; }
+inline void to_float(DCT<float>& d, const DC& s) { d.c = (float)s.c; d.r = (float)s.r; }
+template <typename D, typename S, size_t N>
+inline void to_float(D (&d)[N], const S (&s)[N]) {
+    for (size_t q = 0; q < N; q++) to_float(d[q], s[q]);
+}
+inline void fill_float_consts(Consts& C) {
+#define LES_CONV(name, dims) to_float(C.f.name, C.name);
+    LES_FCONSTS(LES_CONV, LES_CONV)
+#undef LES_CONV
+}
 
 // Reduction results written by the kernels' last-block epilogues.
 struct Scalars {
@@ -110,7 +169,7 @@ __device__ __forceinline__ double cdv(double x, const DC& d) {
     double e = fma(-q, d.c, x);
     return fma(e, d.r, q);
 }
-__device__ __forceinline__ float cdv(float x, const DC& d) { return x * (float)d.r; }
+__device__ __forceinline__ float cdv(float x, const DCT<float>& d) { return x * d.r; }
 
 // x^3 and x^4 rounded once: glibc pow() returns the correctly rounded power for these
 // arguments, while a plain product rounds twice.  The exact square is split with fma,

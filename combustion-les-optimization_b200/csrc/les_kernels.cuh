@@ -70,11 +70,32 @@ struct KFlow {               // momentum and G right-hand sides handed from C1 t
 #ifndef LES_MINB_SCALAR
 #define LES_MINB_SCALAR 3
 #endif
+#ifndef LES_MINB_FILTER_F32
+#define LES_MINB_FILTER_F32 8
+#endif
+#ifndef LES_MINB_STRAIN_F32
+#define LES_MINB_STRAIN_F32 8
+#endif
+#ifndef LES_MINB_FLOW_F32
+#define LES_MINB_FLOW_F32 8
+#endif
+#ifndef LES_MINB_SCALAR_F32
+#define LES_MINB_SCALAR_F32 6
+#endif
+template <typename R>
+struct MinBlocks {
+    static constexpr int filter = LES_MINB_FILTER, strain = 3, flow = LES_MINB_FLOW, scalar = LES_MINB_SCALAR;
+};
+template <>
+struct MinBlocks<float> {
+    static constexpr int filter = LES_MINB_FILTER_F32, strain = LES_MINB_STRAIN_F32, flow = LES_MINB_FLOW_F32,
+                         scalar = LES_MINB_SCALAR_F32;
+};
 
 // ---------------------------------------------------------------------------- helpers
 
 template <typename R>
-__device__ __forceinline__ R fit_prop(const double co[4], int zero, R L, R L2, R L3) {
+__device__ __forceinline__ R fit_prop(const R co[4], int zero, R L, R L2, R L3) {
     // calculate_property_from_fit (:385-391): exp(a0 + a1 L + a2 L^2 + a3 L^3); the T <= 0
     // guard is handled by the callers.
     if (zero) return R(0);
@@ -84,10 +105,11 @@ __device__ __forceinline__ R fit_prop(const double co[4], int zero, R L, R L2, R
 
 template <typename R>
 __device__ __forceinline__ R eos_rho(const Consts& C, R T, const R Y[NSP], R fallback) {
+    const auto& K = kc<R>(C);
     // update_rho_from_EOS (:1894-1905)
     R syw = R(0);
 #pragma unroll
-    for (int s = 0; s < NSP; s++) syw += cdv(Y[s], C.d_mwk[s]);
+    for (int s = 0; s < NSP; s++) syw += cdv(Y[s], K.d_mwk[s]);
     if (syw > R(1e-9) && T > R(1.0)) {
         R W = R(1.0) / syw;
         R Rm = (R)R_UNIV / W;
@@ -100,12 +122,13 @@ __device__ __forceinline__ R eos_rho(const Consts& C, R T, const R Y[NSP], R fal
 template <typename R>
 __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP], R rhof, R& mu_mix, R& nu,
                                            R D[NSP], R& aT, R& cp_out, R& lam_out, R& alpha) {
+    const auto& K = kc<R>(C);
     R X[NSP];
     R syw = R(0);
     bool tpos = Tl > R(0);
     R ym[NSP];
 #pragma unroll
-    for (int s = 0; s < NSP; s++) ym[s] = cdv(Yf[s], C.d_mwk[s]);
+    for (int s = 0; s < NSP; s++) ym[s] = cdv(Yf[s], K.d_mwk[s]);
     if (tpos) {
 #pragma unroll
         for (int s = 0; s < NSP; s++) syw += ym[s];
@@ -120,10 +143,10 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
         R cp = R(0);
 #pragma unroll
         for (int s = 0; s < NSP; s++) {
-            const double* a = (Tl > (R)C.t_mid[s]) ? C.nasa_high[s] : C.nasa_low[s];
+            const auto* a = (Tl > (R)K.t_mid[s]) ? K.nasa_high[s] : K.nasa_low[s];
             R cpr = (R)a[0] + (R)a[1] * Tl + (R)a[2] * T2 + (R)a[3] * T3 + (R)a[4] * T4;
             R cpm = cpr * (R)R_UNIV;
-            R cpk = (C.mwk[s] < 1e-9) ? R(1000.0) : cdv(cpm, C.d_mwk[s]);
+            R cpk = (K.mwk[s] < R(1e-9)) ? R(1000.0) : cdv(cpm, K.d_mwk[s]);
             cp += Yf[s] * cpk;
         }
         Cp = fmax(R(100.0), cp);
@@ -149,8 +172,8 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
     R muk[NSP], lamk[NSP];
 #pragma unroll
     for (int s = 0; s < NSP; s++) {
-        muk[s] = fit_prop<R>(C.eta[s], C.eta_zero[s], L, L2, L3) * R(0.1);
-        lamk[s] = fit_prop<R>(C.lam[s], C.lam_zero[s], L, L2, L3) * R(1e-5);
+        muk[s] = fit_prop<R>(K.eta[s], C.eta_zero[s], L, L2, L3) * R(0.1);
+        lamk[s] = fit_prop<R>(K.lam[s], C.lam_zero[s], L, L2, L3) * R(1e-5);
     }
     // Wilke (:1530-1546) and Wassiljew (:1842-1863) share the same phi_ij, the same skip
     // rule and the same summation order, so one denominator per species serves both.
@@ -163,8 +186,8 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
         for (int b = 0; b < NSP; b++) {
             if (X[b] < R(1e-12)) continue;
             R sr = sqrt(muk[a] / muk[b]);
-            R t = R(1.0) + sr * (R)C.wpow[a][b];
-            R ph = cdv(t * t, C.d_wden[a][b]);
+            R t = R(1.0) + sr * (R)K.wpow[a][b];
+            R ph = cdv(t * t, K.d_wden[a][b]);
             den += X[b] * ph;
         }
         if (den > R(1e-9)) {
@@ -192,7 +215,7 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
             for (int b = a + 1; b < NSP; b++) {
                 R v = R(0);
                 if (X[a] > R(1e-12) || X[b] > R(1e-12))
-                    v = fit_prop<R>(C.dco[a][b], C.dco_zero[a][b], L, L2, L3) * R(1e-4);
+                    v = fit_prop<R>(K.dco[a][b], C.dco_zero[a][b], L, L2, L3) * R(1e-4);
                 Dm[a][b] = v;
                 Dm[b][a] = v;
             }
@@ -202,7 +225,7 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
 #pragma unroll
             for (int b = 0; b < NSP; b++) {
                 R v = R(0);
-                if (a != b && X[b] > R(1e-12)) v = fit_prop<R>(C.dco[a][b], C.dco_zero[a][b], L, L2, L3) * R(1e-4);
+                if (a != b && X[b] > R(1e-12)) v = fit_prop<R>(K.dco[a][b], C.dco_zero[a][b], L, L2, L3) * R(1e-4);
                 Dm[a][b] = v;
             }
     }
@@ -220,7 +243,7 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
         R Dv;
         if (fabs(R(1.0) - X[a]) < R(1e-9)) {
             int o = (a != N2) ? N2 : O2;
-            Dv = fit_prop<R>(C.dco[a][o], C.dco_zero[a][o], L, L2, L3) * R(1e-4);
+            Dv = fit_prop<R>(K.dco[a][o], C.dco_zero[a][o], L, L2, L3) * R(1e-4);
         } else if (sx > R(1e-12)) {
             Dv = (R(1.0) - X[a]) / sx;
         } else {
@@ -235,9 +258,10 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
 // ------------------------------------------------------------------ pass A: filter + props
 
 template <typename R>
-__global__ void __launch_bounds__(NT, LES_MINB_FILTER)
+__global__ void __launch_bounds__(NT, MinBlocks<R>::filter)
     k_filter_props(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> in, F11<R> F, PropBuf<R> P,
                    double* __restrict__ part, Scalars* __restrict__ S, int want_max) {
+    const auto& K = kc<R>(C);
     __shared__ double sh[NT / 32];
     __shared__ bool last;
     const int nx = C.nx, ny = C.ny, nz = C.nz;
@@ -256,7 +280,7 @@ __global__ void __launch_bounds__(NT, LES_MINB_FILTER)
         for (int q = 0; q < NSTATE; q++) {
             const R* __restrict__ x = in.p[q] + id;
             if (filt) {
-                f[q] = cdv(x[-sI] + x[-sJ] + x[-1] + R(FILTER_W) * x[0] + x[1] + x[sJ] + x[sI], C.d_filter);
+                f[q] = cdv(x[-sI] + x[-sJ] + x[-1] + R(FILTER_W) * x[0] + x[1] + x[sJ] + x[sI], K.d_filter);
             } else {
                 f[q] = x[0];
             }
@@ -323,8 +347,9 @@ __global__ void __launch_bounds__(NT, LES_MINB_FILTER)
 // ------------------------------------------------------------------ pass B: strain + nu_t + S_T
 
 template <typename R>
-__global__ void __launch_bounds__(NT, 3)
+__global__ void __launch_bounds__(NT, MinBlocks<R>::strain)
     k_strain(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> F, PropBuf<R> P) {
+    const auto& K = kc<R>(C);
     const int nx = C.nx, ny = C.ny, nz = C.nz;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -338,15 +363,15 @@ __global__ void __launch_bounds__(NT, 3)
         const R* __restrict__ uf = F.p[0] + id;
         const R* __restrict__ vf = F.p[1] + id;
         const R* __restrict__ wf = F.p[2] + id;
-        R du_dx = cdv(uf[sI] - uf[-sI], C.d_2dx);
-        R dv_dy = cdv(vf[sJ] - vf[-sJ], C.d_2dy);
-        R dw_dz = cdv(wf[1] - wf[-1], C.d_2dz);
-        R du_dy = cdv(uf[sJ] - uf[-sJ], C.d_2dy);
-        R du_dz = cdv(uf[1] - uf[-1], C.d_2dz);
-        R dv_dx = cdv(vf[sI] - vf[-sI], C.d_2dx);
-        R dv_dz = cdv(vf[1] - vf[-1], C.d_2dz);
-        R dw_dx = cdv(wf[sI] - wf[-sI], C.d_2dx);
-        R dw_dy = cdv(wf[sJ] - wf[-sJ], C.d_2dy);
+        R du_dx = cdv(uf[sI] - uf[-sI], K.d_2dx);
+        R dv_dy = cdv(vf[sJ] - vf[-sJ], K.d_2dy);
+        R dw_dz = cdv(wf[1] - wf[-1], K.d_2dz);
+        R du_dy = cdv(uf[sJ] - uf[-sJ], K.d_2dy);
+        R du_dz = cdv(uf[1] - uf[-1], K.d_2dz);
+        R dv_dx = cdv(vf[sI] - vf[-sI], K.d_2dx);
+        R dv_dz = cdv(vf[1] - vf[-1], K.d_2dz);
+        R dw_dx = cdv(wf[sI] - wf[-sI], K.d_2dx);
+        R dw_dy = cdv(wf[sJ] - wf[-sJ], K.d_2dy);
         R S11 = du_dx, S22 = dv_dy, S33 = dw_dz;
         R S12 = R(0.5) * (du_dy + dv_dx), S13 = R(0.5) * (du_dz + dw_dx), S23 = R(0.5) * (dv_dz + dw_dy);
         R Sij = R(2.0) * (S12 * S12 + S13 * S13 + S23 * S23) + S11 * S11 + S22 * S22 + S33 * S33;
@@ -355,9 +380,9 @@ __global__ void __launch_bounds__(NT, 3)
         R g = F.p[4][id];
         if (g < R(0.0)) g = R(0.0);
         if (g > R(1.0)) g = R(1.0);
-        R cs = (R)C.cs_u + ((R)C.cs_b - (R)C.cs_u) * g;
-        cs += (R)C.cs_boost * R(4.0) * g * (R(1.0) - g);
-        const R dx = (R)C.dx;
+        R cs = (R)K.cs_u + ((R)K.cs_b - (R)K.cs_u) * g;
+        cs += (R)K.cs_boost * R(4.0) * g * (R(1.0) - g);
+        const R dx = (R)K.dx;
         R nut = (cs * dx) * (cs * dx) * Smag;
         P.nu_t[id] = nut;
         P.S_mag[id] = Smag;
@@ -365,7 +390,7 @@ __global__ void __launch_bounds__(NT, 3)
         // SSR-SGS turbulent flame speed (:1926-1957)
         R nul = P.nu[id];
         R num = Sij - (div * div) * R(1.0 / 3.0);
-        R X = ((R)C.dx4 / (nul * nul)) * num;
+        R X = ((R)K.dx4 / (nul * nul)) * num;
         R d_eta;
         if (X < R(SMALL)) {
             d_eta = R(1.0);
@@ -376,18 +401,18 @@ __global__ void __launch_bounds__(NT, 3)
         }
         R eta = dx / (d_eta + R(SMALL));
         R Dce = R(8.0) * eta;
-        R asf = R(8.0) * exp((R)C.ssr_cdF / (Dce + R(SMALL)));
-        R base = cdv(asf * eta, C.d_dx);
-        R wr = pow(base, (R)(2.0 - C.d3));
+        R asf = R(8.0) * exp((R)K.ssr_cdF / (Dce + R(SMALL)));
+        R base = cdv(asf * eta, K.d_dx);
+        R wr = pow(base, (R)K.ssr_exp);
         R te = R(0.0);
-        if (C.tau_sl > SMALL) te = cdv(dx * fmax(R(0.0), div), C.d_tau_sl);
+        if (K.tau_sl > R(SMALL)) te = cdv(dx * fmax(R(0.0), div), K.d_tau_sl);
         R ratio = wr + te;
-        R st = (R)C.s_l * fmax(R(0.0), ratio);
-        P.ST[id] = fmax((R)C.s_l, st);
+        R st = (R)K.s_l * fmax(R(0.0), ratio);
+        P.ST[id] = fmax((R)K.s_l, st);
     } else {
         P.nu_t[id] = R(0);
         P.S_mag[id] = R(0);
-        P.ST[id] = interior ? (R)C.s_l : R(0);
+        P.ST[id] = interior ? (R)K.s_l : R(0);
         P.mu_eff[id] = R(0);
     }
 }
@@ -397,6 +422,7 @@ __global__ void __launch_bounds__(NT, 3)
 // teno5_reconstruct (:2190-2236)
 template <typename R>
 __device__ __forceinline__ R teno5_rec(const Consts& C, R v0, R v1, R v2, R v3, R v4) {
+    const auto& K = kc<R>(C);
     R a0 = v0 - R(2.0) * v1 + v2, b0 = v0 - R(4.0) * v1 + R(3.0) * v2;
     R a1 = v1 - R(2.0) * v2 + v3, b1 = v1 - v3;
     R a2 = v2 - R(2.0) * v3 + v4, b2 = R(3.0) * v2 - R(4.0) * v3 + v4;
@@ -404,9 +430,9 @@ __device__ __forceinline__ R teno5_rec(const Consts& C, R v0, R v1, R v2, R v3, 
     R is1 = R(13.0 / 12.0) * (a1 * a1) + R(1.0 / 4.0) * (b1 * b1);
     R is2 = R(13.0 / 12.0) * (a2 * a2) + R(1.0 / 4.0) * (b2 * b2);
     int d0 = (is0 < R(TENO_CUT)) ? 1 : 0, d1 = (is1 < R(TENO_CUT)) ? 1 : 0, d2 = (is2 < R(TENO_CUT)) ? 1 : 0;
-    R p0 = cdv(R(2.0) * v0 - R(7.0) * v1 + R(11.0) * v2, C.d_six);
-    R p1 = cdv(-v1 + R(5.0) * v2 + R(2.0) * v3, C.d_six);
-    R p2 = cdv(R(2.0) * v2 + R(5.0) * v3 - v4, C.d_six);
+    R p0 = cdv(R(2.0) * v0 - R(7.0) * v1 + R(11.0) * v2, K.d_six);
+    R p1 = cdv(-v1 + R(5.0) * v2 + R(2.0) * v3, K.d_six);
+    R p2 = cdv(R(2.0) * v2 + R(5.0) * v3 - v4, K.d_six);
     if (d0 + d1 + d2 == 0) {
         if (is0 <= is1 && is0 <= is2) return p0;
         else if (is1 <= is0 && is1 <= is2) return p1;
@@ -420,7 +446,7 @@ __device__ __forceinline__ R teno5_rec(const Consts& C, R v0, R v1, R v2, R v3, 
 
 // One axis of the TENO5 G-advection (:2258-2295).
 template <typename R>
-__device__ __forceinline__ R teno_axis(const Consts& C, R vel, const R* __restrict__ q, ptrdiff_t s, const DC& d) {
+__device__ __forceinline__ R teno_axis(const Consts& C, R vel, const R* __restrict__ q, ptrdiff_t s, const DCT<R>& d) {
     R q0 = q[-3 * s], q1 = q[-2 * s], q2 = q[-s], q3 = q[0], q4 = q[s], q5 = q[2 * s], q6 = q[3 * s];
     if (vel >= R(0.0)) {
         R ph = teno5_rec<R>(C, q1, q2, q3, q4, q5);
@@ -444,7 +470,8 @@ __device__ __forceinline__ void weno_is(R v1, R v2, R v3, R v4, R v5, R& is0, R&
     is2 = R(13.0 / 12.0) * (a2 * a2) + R(1.0 / 4.0) * (b2 * b2);
 }
 template <typename R>
-__device__ __forceinline__ R weno5_grad(const Consts& C, const R* __restrict__ q, ptrdiff_t s, const DC& dx) {
+__device__ __forceinline__ R weno5_grad(const Consts& C, const R* __restrict__ q, ptrdiff_t s, const DCT<R>& dx) {
+    const auto& K = kc<R>(C);
     R p0 = q[-2 * s], p1 = q[-s], p2 = q[0], p3 = q[s], p4 = q[2 * s], p5 = q[3 * s];
     const R eps = R(1.0e-6);
     R i0, i1, i2;
@@ -453,18 +480,18 @@ __device__ __forceinline__ R weno5_grad(const Consts& C, const R* __restrict__ q
     R a0 = R(3.0 / 10.0) / (e0 * e0), a1 = R(6.0 / 10.0) / (e1 * e1), a2 = R(1.0 / 10.0) / (e2 * e2);
     R sa = a0 + a1 + a2;
     R w0 = a0 / sa, w1 = a1 / sa, w2 = a2 / sa;
-    R s0 = cdv(R(2.0) * p1 - R(7.0) * p2 + R(11.0) * p3, C.d_six);
-    R s1 = cdv(-p2 + R(5.0) * p3 + R(2.0) * p4, C.d_six);
-    R s2 = cdv(R(2.0) * p3 + R(5.0) * p4 - p5, C.d_six);
+    R s0 = cdv(R(2.0) * p1 - R(7.0) * p2 + R(11.0) * p3, K.d_six);
+    R s1 = cdv(-p2 + R(5.0) * p3 + R(2.0) * p4, K.d_six);
+    R s2 = cdv(R(2.0) * p3 + R(5.0) * p4 - p5, K.d_six);
     R ph = w0 * s0 + w1 * s1 + w2 * s2;
     weno_is<R>(p0, p1, p2, p3, p4, i0, i1, i2);
     e0 = eps + i0; e1 = eps + i1; e2 = eps + i2;
     a0 = R(1.0 / 10.0) / (e0 * e0); a1 = R(6.0 / 10.0) / (e1 * e1); a2 = R(3.0 / 10.0) / (e2 * e2);
     sa = a0 + a1 + a2;
     w0 = a0 / sa; w1 = a1 / sa; w2 = a2 / sa;
-    R m0 = cdv(-p0 + R(5.0) * p1 + R(2.0) * p2, C.d_six);
-    R m1 = cdv(R(2.0) * p1 + R(5.0) * p2 - p3, C.d_six);
-    R m2 = cdv(R(11.0) * p2 - R(7.0) * p3 + R(2.0) * p4, C.d_six);
+    R m0 = cdv(-p0 + R(5.0) * p1 + R(2.0) * p2, K.d_six);
+    R m1 = cdv(R(2.0) * p1 + R(5.0) * p2 - p3, K.d_six);
+    R m2 = cdv(R(11.0) * p2 - R(7.0) * p3 + R(2.0) * p4, K.d_six);
     R mh = w0 * m0 + w1 * m1 + w2 * m2;
     return cdv(ph - mh, dx);
 }
@@ -480,7 +507,7 @@ __device__ __forceinline__ R superbee(R r) {
 
 // MUSCL-superbee along one axis (:2058-2094); values at offsets -2..+2.
 template <typename R>
-__device__ __forceinline__ R muscl_axis(R vel, R pm2, R pm1, R p0, R pp1, R pp2, const DC& d) {
+__device__ __forceinline__ R muscl_axis(R vel, R pm2, R pm1, R p0, R pp1, R pp2, const DCT<R>& d) {
     if (vel >= R(0.0)) {
         R dup_im = pm1 - pm2, ddn_im = p0 - pm1;
         R r_im = (fabs(ddn_im) < R(SMALL)) ? R(1e9) : dup_im / ddn_im;
@@ -505,13 +532,14 @@ __device__ __forceinline__ R muscl_axis(R vel, R pm2, R pm1, R p0, R pp1, R pp2,
 template <typename R>
 __device__ __forceinline__ R upwind3(const Consts& C, const R* __restrict__ q, ptrdiff_t sI, ptrdiff_t sJ, R u, R v,
                                      R w) {
+    const auto& K = kc<R>(C);
     R f;
-    if (u >= R(0.0)) f = cdv(u * (q[0] - q[-sI]), C.d_dx);
-    else f = cdv(u * (q[sI] - q[0]), C.d_dx);
-    if (v >= R(0.0)) f += cdv(v * (q[0] - q[-sJ]), C.d_dy);
-    else f += cdv(v * (q[sJ] - q[0]), C.d_dy);
-    if (w >= R(0.0)) f += cdv(w * (q[0] - q[-1]), C.d_dz);
-    else f += cdv(w * (q[1] - q[0]), C.d_dz);
+    if (u >= R(0.0)) f = cdv(u * (q[0] - q[-sI]), K.d_dx);
+    else f = cdv(u * (q[sI] - q[0]), K.d_dx);
+    if (v >= R(0.0)) f += cdv(v * (q[0] - q[-sJ]), K.d_dy);
+    else f += cdv(v * (q[sJ] - q[0]), K.d_dy);
+    if (w >= R(0.0)) f += cdv(w * (q[0] - q[-1]), K.d_dz);
+    else f += cdv(w * (q[1] - q[0]), K.d_dz);
     return f;
 }
 
@@ -519,10 +547,11 @@ __device__ __forceinline__ R upwind3(const Consts& C, const R* __restrict__ q, p
 template <typename R>
 __device__ __forceinline__ R conv_muscl(const Consts& C, const R* __restrict__ q, ptrdiff_t sI, ptrdiff_t sJ, bool band2,
                                         R u, R v, R w) {
+    const auto& K = kc<R>(C);
     if (band2) return upwind3<R>(C, q, sI, sJ, u, v, w);
-    R cx = muscl_axis<R>(u, q[-2 * sI], q[-sI], q[0], q[sI], q[2 * sI], C.d_dx);
-    R cy = muscl_axis<R>(v, q[-2 * sJ], q[-sJ], q[0], q[sJ], q[2 * sJ], C.d_dy);
-    R cz = muscl_axis<R>(w, q[-2], q[-1], q[0], q[1], q[2], C.d_dz);
+    R cx = muscl_axis<R>(u, q[-2 * sI], q[-sI], q[0], q[sI], q[2 * sI], K.d_dx);
+    R cy = muscl_axis<R>(v, q[-2 * sJ], q[-sJ], q[0], q[sJ], q[2 * sJ], K.d_dy);
+    R cz = muscl_axis<R>(w, q[-2], q[-1], q[0], q[1], q[2], K.d_dz);
     return cx + cy + cz;
 }
 
@@ -533,7 +562,7 @@ struct SgsFaces {
     R iph, imh, jph, jmh, kph, kmh;
 };
 template <typename R>
-__device__ __forceinline__ SgsFaces<R> sgs_faces(const R* __restrict__ nut, ptrdiff_t sI, ptrdiff_t sJ, const DC& c2) {
+__device__ __forceinline__ SgsFaces<R> sgs_faces(const R* __restrict__ nut, ptrdiff_t sI, ptrdiff_t sJ, const DCT<R>& c2) {
     R n0 = nut[0];
     SgsFaces<R> g;
     g.iph = cdv(nut[sI] + n0, c2); g.imh = cdv(n0 + nut[-sI], c2);
@@ -544,28 +573,31 @@ __device__ __forceinline__ SgsFaces<R> sgs_faces(const R* __restrict__ nut, ptrd
 template <typename R>
 __device__ __forceinline__ R sgs_div(const Consts& C, const R* __restrict__ q, const SgsFaces<R>& g, ptrdiff_t sI,
                                      ptrdiff_t sJ) {
+    const auto& K = kc<R>(C);
     R p0 = q[0];
-    R sx = cdv(cdv(g.iph * (q[sI] - p0), C.d_dx) - cdv(g.imh * (p0 - q[-sI]), C.d_dx), C.d_dx);
-    R sy = cdv(cdv(g.jph * (q[sJ] - p0), C.d_dy) - cdv(g.jmh * (p0 - q[-sJ]), C.d_dy), C.d_dy);
-    R sz = cdv(cdv(g.kph * (q[1] - p0), C.d_dz) - cdv(g.kmh * (p0 - q[-1]), C.d_dz), C.d_dz);
+    R sx = cdv(cdv(g.iph * (q[sI] - p0), K.d_dx) - cdv(g.imh * (p0 - q[-sI]), K.d_dx), K.d_dx);
+    R sy = cdv(cdv(g.jph * (q[sJ] - p0), K.d_dy) - cdv(g.jmh * (p0 - q[-sJ]), K.d_dy), K.d_dy);
+    R sz = cdv(cdv(g.kph * (q[1] - p0), K.d_dz) - cdv(g.kmh * (p0 - q[-1]), K.d_dz), K.d_dz);
     return sx + sy + sz;
 }
 
 template <typename R>
 __device__ __forceinline__ R lap3(const Consts& C, const R* __restrict__ q, ptrdiff_t sI, ptrdiff_t sJ) {
+    const auto& K = kc<R>(C);
     R p0 = q[0];
-    R a = cdv(q[sI] - R(2.0) * p0 + q[-sI], C.d_dxx);
-    R b = cdv(q[sJ] - R(2.0) * p0 + q[-sJ], C.d_dyy);
-    R c = cdv(q[1] - R(2.0) * p0 + q[-1], C.d_dzz);
+    R a = cdv(q[sI] - R(2.0) * p0 + q[-sI], K.d_dxx);
+    R b = cdv(q[sJ] - R(2.0) * p0 + q[-sJ], K.d_dyy);
+    R c = cdv(q[1] - R(2.0) * p0 + q[-1], K.d_dzz);
     return a + b + c;
 }
 
 // C1: momentum (:2552-2697) with calculate_convection_conservative (:683-727) and the G
 // equation (:2706-2825).  Writes k_rhou, k_rhov, k_rhow, k_G of fluid cells.
 template <typename R>
-__global__ void __launch_bounds__(NT, LES_MINB_FLOW)
+__global__ void __launch_bounds__(NT, MinBlocks<R>::flow)
     k_rhs_flow(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> F, PropBuf<R> P, KFlow<R> kf,
                KDbg<R> kd, const Scalars* __restrict__ Sc) {
+    const auto& K = kc<R>(C);
     const int nx = C.nx, ny = C.ny, nz = C.nz;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -617,8 +649,8 @@ __global__ void __launch_bounds__(NT, LES_MINB_FLOW)
                 p_kph = R(0.5) * pc + R(0.5) * ph[1];
                 p_kmh = R(0.5) * ph[-1] + R(0.5) * pc;
             }
-            R conv = cdv(mf_iph * p_iph - mf_imh * p_imh, C.d_dx) + cdv(mf_jph * p_jph - mf_jmh * p_jmh, C.d_dy) +
-                     cdv(mf_kph * p_kph - mf_kmh * p_kmh, C.d_dz);
+            R conv = cdv(mf_iph * p_iph - mf_imh * p_imh, K.d_dx) + cdv(mf_jph * p_jph - mf_jmh * p_jmh, K.d_dy) +
+                     cdv(mf_kph * p_kph - mf_kmh * p_kmh, K.d_dz);
             kmom[q] = -conv + mu_eff * lap3<R>(C, ph, sI, sJ);
         }
         R grav = (r0 - (R)Sc->rho_avg) * R(G_GRAVITY);
@@ -626,26 +658,26 @@ __global__ void __launch_bounds__(NT, LES_MINB_FLOW)
         if (C.flame_accel) {
             R Gl = Gf[0];
             if (Gl > R(0.01) && Gl < R(0.99)) {
-                R dGx = cdv(Gf[sI] - Gf[-sI], C.d_2dx);
-                R dGy = cdv(Gf[sJ] - Gf[-sJ], C.d_2dy);
-                R dGz = cdv(Gf[1] - Gf[-1], C.d_2dz);
+                R dGx = cdv(Gf[sI] - Gf[-sI], K.d_2dx);
+                R dGy = cdv(Gf[sJ] - Gf[-sJ], K.d_2dy);
+                R dGz = cdv(Gf[1] - Gf[-1], K.d_2dz);
                 if (dGx < R(0.0)) dGx = R(0.0);
                 if (dGy < R(0.0)) dGy = R(0.0);
-                R zrel = ((R)k * (R)C.dz) - (R)C.inlet_center_z;
+                R zrel = ((R)k * (R)K.dz) - (R)K.inlet_center_z;
                 if (zrel > R(0.0)) {
                     if (dGz < R(0.0)) dGz = R(0.0);
                 } else {
                     if (dGz > R(0.0)) dGz = R(0.0);
                 }
-                R df = Gl - (R)C.accel_center;
-                R window = exp(cdv(-(df * df), C.d_w2));
+                R df = Gl - (R)K.accel_center;
+                R window = exp(cdv(-(df * df), K.d_w2));
                 // tip_mask is the literal 1.0 in the momentum source (:2638)
-                R cf = (R)C.accel_strength * r0 * window * R(1.0);
+                R cf = (R)K.accel_strength * r0 * window * R(1.0);
                 fx = cf * dGx * R(0.05);
                 fy = cf * dGy * R(1.0);
                 fz = cf * dGz * R(1.0);
-                R zp = (R)k * (R)C.dz, ramp = R(1.0);
-                if (zp < R(RAMP_DIST)) ramp = cdv(zp, C.d_ramp);
+                R zp = (R)k * (R)K.dz, ramp = R(1.0);
+                if (zp < R(RAMP_DIST)) ramp = cdv(zp, K.d_ramp);
                 fx *= ramp; fy *= ramp; fz *= ramp;
             }
         }
@@ -673,28 +705,28 @@ __global__ void __launch_bounds__(NT, LES_MINB_FLOW)
                 R p_iph = R(0.5) * pc + R(0.5) * Gf[sI], p_imh = R(0.5) * Gf[-sI] + R(0.5) * pc;
                 R p_jph = R(0.5) * pc + R(0.5) * Gf[sJ], p_jmh = R(0.5) * Gf[-sJ] + R(0.5) * pc;
                 R p_kph = R(0.5) * pc + R(0.5) * Gf[1], p_kmh = R(0.5) * Gf[-1] + R(0.5) * pc;
-                R cx = cdv(u0 * (p_iph - p_imh), C.d_dx);
-                R cy = cdv(v0 * (p_jph - p_jmh), C.d_dy);
-                R cz = cdv(w0 * (p_kph - p_kmh), C.d_dz);
+                R cx = cdv(u0 * (p_iph - p_imh), K.d_dx);
+                R cy = cdv(v0 * (p_jph - p_jmh), K.d_dy);
+                R cz = cdv(w0 * (p_kph - p_kmh), K.d_dz);
                 conv = cx + cy + cz;
             }
         } else {
-            R fxa = teno_axis<R>(C, u0, Gf, sI, C.d_dx);
-            R fya = teno_axis<R>(C, v0, Gf, sJ, C.d_dy);
-            R fza = teno_axis<R>(C, w0, Gf, 1, C.d_dz);
+            R fxa = teno_axis<R>(C, u0, Gf, sI, K.d_dx);
+            R fya = teno_axis<R>(C, v0, Gf, sJ, K.d_dy);
+            R fza = teno_axis<R>(C, w0, Gf, 1, K.d_dz);
             conv = fxa + fya + fza;
         }
-        SgsFaces<R> gf = sgs_faces<R>(P.nu_t + id, sI, sJ, C.d_sct2);
+        SgsFaces<R> gf = sgs_faces<R>(P.nu_t + id, sI, sJ, K.d_sct2);
         R sgs = sgs_div<R>(C, Gf, gf, sI, sJ);
         R gx, gy, gz;
         if (Sc->t_loop >= C.weno_step && !band3) {
-            gx = weno5_grad<R>(C, Gf, sI, C.d_dx);
-            gy = weno5_grad<R>(C, Gf, sJ, C.d_dy);
-            gz = weno5_grad<R>(C, Gf, 1, C.d_dz);
+            gx = weno5_grad<R>(C, Gf, sI, K.d_dx);
+            gy = weno5_grad<R>(C, Gf, sJ, K.d_dy);
+            gz = weno5_grad<R>(C, Gf, 1, K.d_dz);
         } else {
-            gx = cdv(Gf[sI] - Gf[-sI], C.d_2dx);
-            gy = cdv(Gf[sJ] - Gf[-sJ], C.d_2dy);
-            gz = cdv(Gf[1] - Gf[-1], C.d_2dz);
+            gx = cdv(Gf[sI] - Gf[-sI], K.d_2dx);
+            gy = cdv(Gf[sJ] - Gf[-sJ], K.d_2dy);
+            gz = cdv(Gf[1] - Gf[-1], K.d_2dz);
         }
         R gmag = sqrt(gx * gx + gy * gy + gz * gz);
         R prop = P.ST[id] * gmag;
@@ -702,8 +734,8 @@ __global__ void __launch_bounds__(NT, LES_MINB_FLOW)
         if (C.flame_accel) {
             R Gl = Gf[0];
             if (Gl > R(0.1) && Gl < R(0.99)) {
-                R df = Gl - (R)C.accel_center;
-                R window = exp(cdv(-(df * df), C.d_w2));
+                R df = Gl - (R)K.accel_center;
+                R window = exp(cdv(-(df * df), K.d_w2));
                 // tip_mask = 1 - exp(-r^2 / 0^2) is exactly 1 for every fluid cell (j >= 1)
                 // because TIP_PROTECTION_RADIUS is 0.0 (:234, :2806-2807).
                 R adc = R(5.0) * (P.nu_t[id] + R(1.0e-5)) * window * R(1.0);
@@ -727,9 +759,10 @@ __global__ void __launch_bounds__(NT, LES_MINB_FLOW)
 // C2: species (:2837-2904) and temperature (:2912-2962), then the RK4 bookkeeping.
 // stage: 0,1,2 -> intermediate stage with coefficient 0.5/0.5/1.0, 3 -> final combine.
 template <typename R>
-__global__ void __launch_bounds__(NT, LES_MINB_SCALAR)
+__global__ void __launch_bounds__(NT, MinBlocks<R>::scalar)
     k_rhs_scalar(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> F, PropBuf<R> P, F11<R> S0, F11<R> St,
                  AccBuf<R> acc, KFlow<R> kf, KDbg<R> kd, const Scalars* __restrict__ Sc, int stage) {
+    const auto& K = kc<R>(C);
     const int nx = C.nx, ny = C.ny, nz = C.nz;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -770,8 +803,8 @@ __global__ void __launch_bounds__(NT, LES_MINB_SCALAR)
     R g = F.p[4][id];
     if (g < R(0.0)) g = R(0.0);
     if (g > R(1.0)) g = R(1.0);
-    const SgsFaces<R> gs = sgs_faces<R>(P.nu_t + id, sI, sJ, C.d_sct2);
-    const R relax = (R)C.relax;
+    const SgsFaces<R> gs = sgs_faces<R>(P.nu_t + id, sI, sJ, K.d_sct2);
+    const R relax = (R)K.relax;
 #pragma unroll
     for (int s = 0; s < NSP; s++) {
         const R* __restrict__ Yf = F.p[6 + s] + id;
@@ -779,11 +812,11 @@ __global__ void __launch_bounds__(NT, LES_MINB_SCALAR)
         R mol = P.D[s][id] * lap3<R>(C, Yf, sI, sJ);
         R sgs = sgs_div<R>(C, Yf, gs, sI, sJ);
         R tgt;
-        if (s == C3H8) tgt = (R)C.inletYk[C3H8] * (R(1.0) - g);
-        else if (s == O2) tgt = fmax(R(0.0), (R)C.inletYk[O2] - (R)C.cons_o2 * g);
-        else if (s == CO2) tgt = (R)C.inletYk[CO2] + (R)C.prod_co2 * g;
-        else if (s == H2O) tgt = (R)C.inletYk[H2O] + (R)C.prod_h2o * g;
-        else tgt = (R)C.inletYk[N2];
+        if (s == C3H8) tgt = (R)K.inletYk[C3H8] * (R(1.0) - g);
+        else if (s == O2) tgt = fmax(R(0.0), (R)K.inletYk[O2] - (R)K.cons_o2 * g);
+        else if (s == CO2) tgt = (R)K.inletYk[CO2] + (R)K.prod_co2 * g;
+        else if (s == H2O) tgt = (R)K.inletYk[H2O] + (R)K.prod_h2o * g;
+        else tgt = (R)K.inletYk[N2];
         R nud = relax * (tgt - Yf[0]);
         kv[5 + s] = -conv + mol + sgs + nud;
     }
@@ -791,9 +824,9 @@ __global__ void __launch_bounds__(NT, LES_MINB_SCALAR)
         const R* __restrict__ Tf = F.p[3] + id;
         R conv = conv_muscl<R>(C, Tf, sI, sJ, band2, u0, v0, w0);
         R mol = P.aT[id] * lap3<R>(C, Tf, sI, sJ);
-        const SgsFaces<R> gt = sgs_faces<R>(P.nu_t + id, sI, sJ, C.d_prt2);
+        const SgsFaces<R> gt = sgs_faces<R>(P.nu_t + id, sI, sJ, K.d_prt2);
         R sgs = sgs_div<R>(C, Tf, gt, sI, sJ);
-        R Tt = (R)C.t_in + g * (R)C.t_burnt_span;
+        R Tt = (R)K.t_in + g * (R)K.t_burnt_span;
         R nud = relax * (Tt - Tf[0]);
         kv[3] = -conv + mol + sgs + nud;
     }
@@ -872,16 +905,18 @@ __device__ __forceinline__ void copy_cell(F11<R>& S, size_t dst, size_t src) {
 }
 template <typename R>
 __device__ __forceinline__ void ambient_cell(const Consts& C, F11<R>& S, size_t dst) {
+    const auto& K = kc<R>(C);
     S.p[0][dst] = R(0); S.p[1][dst] = R(0); S.p[2][dst] = R(0);
-    S.p[3][dst] = (R)C.t_amb; S.p[4][dst] = R(0);
+    S.p[3][dst] = (R)K.t_amb; S.p[4][dst] = R(0);
 #pragma unroll
-    for (int s = 0; s < NSP; s++) S.p[6 + s][dst] = (R)C.ambientYk[s];
+    for (int s = 0; s < NSP; s++) S.p[6 + s][dst] = (R)K.ambientYk[s];
 }
 
 template <typename R>
 __global__ void k_bc_iface(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> S,
                            const double* __restrict__ plane, const double* __restrict__ noise,
                            const int* __restrict__ inlet_pos) {
+    const auto& K = kc<R>(C);
     const int nx = C.nx, ny = C.ny, nz = C.nz;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
@@ -892,15 +927,15 @@ __global__ void k_bc_iface(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, 
         const size_t p = (size_t)j * nz + k;
         const size_t npl = (size_t)ny * nz;
         const int q = inlet_pos[p];
-        const R amp = (R)C.noise_amp;
+        const R amp = (R)K.noise_amp;
         R r1 = (R)noise[3 * q + 0], r2 = (R)noise[3 * q + 1], r3 = (R)noise[3 * q + 2];
-        S.p[0][i0] = fmax(R(0.0), (R)C.u_in + (R)plane[p] + amp * r1);
+        S.p[0][i0] = fmax(R(0.0), (R)K.u_in + (R)plane[p] + amp * r1);
         S.p[1][i0] = (R)plane[npl + p] + amp * r2;
         S.p[2][i0] = (R)plane[2 * npl + p] + amp * r3;
-        S.p[3][i0] = (R)C.t_in;
+        S.p[3][i0] = (R)K.t_in;
         S.p[4][i0] = R(0);
 #pragma unroll
-        for (int s = 0; s < NSP; s++) S.p[6 + s][i0] = (R)C.inletYk[s];
+        for (int s = 0; s < NSP; s++) S.p[6 + s][i0] = (R)K.inletYk[s];
     } else if (a0 == 4) {
         if (S.p[0][i1] < R(0)) ambient_cell<R>(C, S, i0);
         else copy_cell<R>(S, i0, i1);
@@ -961,6 +996,7 @@ __global__ void k_bc_kface(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, 
 template <typename R>
 __global__ void __launch_bounds__(NT) k_bc_eos(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> S,
                                                double* __restrict__ part, Scalars* __restrict__ Sc) {
+    const auto& K = kc<R>(C);
     __shared__ double sh[NT / 32];
     __shared__ bool last;
     const int ny = C.ny, nz = C.nz;
@@ -978,7 +1014,7 @@ __global__ void __launch_bounds__(NT) k_bc_eos(LES_KERNEL_CONSTS, const uint8_t*
         R T = S.p[3][id];
         R syw = R(0);
 #pragma unroll
-        for (int s = 0; s < NSP; s++) syw += cdv(Y[s], C.d_mwk[s]);
+        for (int s = 0; s < NSP; s++) syw += cdv(Y[s], K.d_mwk[s]);
         R rho = (syw > R(1e-9) && T > R(1.0)) ? (R)P_CONST / ((R)R_UNIV / (R(1.0) / syw) * T) : R(1.2);
         S.p[5][id] = rho;
         if (a == 3 || a == 2 || a == 5) {

@@ -15,7 +15,7 @@ from .config import SolverConfig
 
 PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 # LESGPU_LIB selects another build of the same library (tuning variants); default in-tree.
-LIB_PATH = os.environ.get("LESGPU_LIB", os.path.join(PKG_DIR, "liblesgpu.so"))
+LIB_PATH = os.environ.get("LESGPU_LIB") or os.path.join(PKG_DIR, "liblesgpu.so")
 DATA_DIR = os.path.join(PKG_DIR, "data")
 CHEM_BIN = os.path.join(DATA_DIR, "chem.bin")
 TRAN_BIN = os.path.join(DATA_DIR, "tran.bin")
