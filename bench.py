@@ -75,7 +75,7 @@ def _peaks():
 
 def _traffic_table():
     """DRAM bytes per cell per launch from the committed ncu summaries (profiles/*.md lines
-    of the form `traffic <kernel> <workload> <bytes_per_cell>`)."""
+    of the form `traffic <kernel> <workload> <precision> <bytes_per_cell>`)."""
     out = {}
     pd = os.path.join(ROOT, "profiles")
     if not os.path.isdir(pd):
@@ -86,9 +86,9 @@ def _traffic_table():
         with open(os.path.join(pd, fn)) as f:
             for line in f:
                 parts = line.strip().strip("`").split()
-                if len(parts) == 4 and parts[0] == "traffic":
+                if len(parts) == 5 and parts[0] == "traffic":
                     try:
-                        out[(parts[1], parts[2])] = float(parts[3])
+                        out[(parts[1], parts[2], parts[3])] = float(parts[4])
                     except ValueError:
                         pass
     return out
@@ -311,7 +311,7 @@ def run_ours(args):
     bytes_launch = KERNEL_BYTES_PER_CELL[cls] * cfg.cells * esz / 8
     peak, peak_kind = _peaks()
     achieved = bytes_launch / (avg_ms / 1e3) / 1e9
-    traffic = _traffic_table().get((cls, args.workload))
+    traffic = _traffic_table().get((cls, args.workload, args.precision))
     step_ms = ms_max / args.steps
     roofline = {"bound": "hbm", "kernel": cls, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind,
