@@ -8,10 +8,10 @@ and the final state fields.
 
 The flow is chaotic: any perturbation, even at rounding level, grows until the two
 trajectories decorrelate, after which their statistics differ by sampling noise alone.  A
-third run separates that floor from the precision error: the FP64 form again from an initial
-temperature field scaled by (1 + 1e-15), a rounding-level perturbation.  Its profile
-differences against the first FP64 run are reported beside the FP32 ones as
-``profiles_floor_fp64_perturbed``.
+further FP64 runs from an initial temperature field scaled by (1 + eps) separate that floor
+from the precision error: eps = 1e-15 (rounding level in FP64) and eps = 1e-7 (rounding
+level in FP32, applied once).  Their profile and state differences against the first FP64
+run are reported beside the FP32 ones (``profiles_floor_<eps>``).
 """
 from __future__ import annotations
 
@@ -67,9 +67,10 @@ def _state_err(a, b):
     return out
 
 
-def compare(cfg: SolverConfig, steps: int, workdir: Optional[str] = None, chunk: int = 64, floor: bool = True) -> dict:
+def compare(cfg: SolverConfig, steps: int, workdir: Optional[str] = None, chunk: int = 64,
+            floor=(1e-15, 1e-7)) -> dict:
     workdir = workdir or tempfile.mkdtemp(prefix="lesprec_")
-    dirs = {k: os.path.join(workdir, k) for k in ("fp64", "fp32", "fp64_alt")}
+    dirs = {k: os.path.join(workdir, k) for k in ("fp64", "fp32")}
     for d in dirs.values():
         os.makedirs(d, exist_ok=True)
     s64, w64 = run_form(cfg, N.FP64, steps, dirs["fp64"], chunk)
@@ -78,12 +79,14 @@ def compare(cfg: SolverConfig, steps: int, workdir: Optional[str] = None, chunk:
     out = {"grid": [cfg.nx, cfg.ny, cfg.nz], "steps": steps, "rows_fp64": int(len(r64["u"])),
            "rows_fp32": int(len(r32["u"])), "wall_s": {"fp64": w64, "fp32": w32},
            "profiles_fp32": stats.compare_profiles(r32, r64), "state_rel_l2_fp32": _state_err(s32, s64)}
-    if floor:
-        salt, walt = run_form(cfg, N.FP64, steps, dirs["fp64_alt"], chunk, perturb=1e-15)
-        ralt = _pool(dirs["fp64_alt"])
-        out["wall_s"]["fp64_alt"] = walt
-        out["profiles_floor_fp64_perturbed"] = stats.compare_profiles(ralt, r64)
-        out["state_rel_l2_floor"] = _state_err(salt, s64)
+    for eps in (floor or ()):
+        d = os.path.join(workdir, f"fp64_eps{eps:g}")
+        os.makedirs(d, exist_ok=True)
+        salt, walt = run_form(cfg, N.FP64, steps, d, chunk, perturb=eps)
+        ralt = _pool(d)
+        out["wall_s"][f"fp64_eps{eps:g}"] = walt
+        out[f"profiles_floor_{eps:g}"] = stats.compare_profiles(ralt, r64)
+        out[f"state_rel_l2_floor_{eps:g}"] = _state_err(salt, s64)
     return out
 
 
@@ -96,7 +99,7 @@ def main(argv=None) -> int:
     ap.add_argument("--workdir", default=None)
     ap.add_argument("--no-floor", action="store_true")
     a = ap.parse_args(argv)
-    print(json.dumps(compare(preset(a.workload), a.steps, a.workdir, a.chunk, floor=not a.no_floor)))
+    print(json.dumps(compare(preset(a.workload), a.steps, a.workdir, a.chunk, floor=() if a.no_floor else (1e-15, 1e-7))))
     return 0
 
 

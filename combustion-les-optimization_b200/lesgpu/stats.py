@@ -72,14 +72,22 @@ def _group_means(b: np.ndarray, nb: int, cols: Dict[str, np.ndarray]):
     return occ, out
 
 
-def flame_profile(rows: Dict[str, np.ndarray]) -> Dict[str, np.ndarray]:
-    """analysis.py:112-130: Reynolds stresses about the global means, binned in y_relative."""
+def flame_edges(rows: Dict[str, np.ndarray]) -> np.ndarray:
+    """The 0.5 mm y_relative bin edges of analysis.py:126-127, from the rows' own range."""
+    y_mm = rows["y_relative"] * 1000
+    return np.arange(y_mm.min(), y_mm.max() + 0.5, 0.5)
+
+
+def flame_profile(rows: Dict[str, np.ndarray], edges: Optional[np.ndarray] = None) -> Dict[str, np.ndarray]:
+    """analysis.py:112-130: Reynolds stresses about the global means, binned in y_relative.
+    ``edges`` (mm) replaces the rows' own bins, to compare two runs on the same bins."""
     u, v, w, G = rows["u"], rows["v"], rows["w"], rows["G"]
     if len(u) == 0:
         return {k: np.zeros(0) for k in ("bin_center", "u", "v", "w", "G", "re_uu", "re_vv", "re_ww", "re_uv")}
     up, vp, wp = u - u.mean(), v - v.mean(), w - w.mean()
     y_mm = rows["y_relative"] * 1000
-    edges = np.arange(y_mm.min(), y_mm.max() + 0.5, 0.5)
+    if edges is None:
+        edges = flame_edges(rows)
     b = _right_closed_bins(y_mm, edges)
     occ, m = _group_means(b, len(edges) - 1, {"u": u, "v": v, "w": w, "G": G, "re_uu": up * up, "re_vv": vp * vp,
                                                "re_ww": wp * wp, "re_uv": up * vp})
@@ -159,12 +167,12 @@ def profile_error(a: np.ndarray, b: np.ndarray, ref_scale: Optional[float] = Non
 def compare_profiles(rows_a: Dict[str, np.ndarray], rows_b: Dict[str, np.ndarray]) -> Dict[str, float]:
     """Per-profile relative L2 errors of run a against run b (b is the reference run)."""
     err = {}
-    fa, fb = flame_profile(rows_a), flame_profile(rows_b)
-    if len(fa["bin_center"]) == len(fb["bin_center"]) and np.allclose(fa["bin_center"], fb["bin_center"]):
+    if len(rows_b["u"]) and len(rows_a["u"]):
+        e = flame_edges(rows_b)
+        fa, fb = flame_profile(rows_a, e), flame_profile(rows_b, e)
+        common, ia, ib = np.intersect1d(fa["bin_center"], fb["bin_center"], return_indices=True)
         for k in ("u", "re_uu", "re_vv", "re_ww", "re_uv"):
-            err[f"flame_profile.{'mean_u' if k == 'u' else k}"] = profile_error(fa[k], fb[k])
-    else:
-        err["flame_profile.bins_differ"] = float("inf")
+            err[f"flame_profile.{'mean_u' if k == 'u' else k}"] = profile_error(fa[k][ia], fb[k][ib])
     sa, sb = stress_vs_g(rows_a), stress_vs_g(rows_b)
     if len(sa["G_center"]) == len(sb["G_center"]) and np.allclose(sa["G_center"], sb["G_center"]):
         for k in ("u_mean", "uu_cond", "vv_cond", "uv_cond"):
