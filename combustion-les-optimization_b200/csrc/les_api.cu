@@ -146,6 +146,8 @@ unsigned char* read_record(FILE* fp, int* len) {
     return b;
 }
 
+// 11 state fields (Phi_n, always 8-byte) and 48 fields of the form's element size.
+constexpr size_t kStateFields = 11;
 size_t fields_for_precision() { return 59; }
 
 void free_loop(DevCtx& d);
@@ -312,7 +314,7 @@ size_t lesgpu_bytes_for_grid(int nx, int ny, int nz, int precision) {
     size_t nb = les::max_cell_blocks(nx, ny, nz);
     if (nb < (size_t)les::MON_BLOCKS) nb = les::MON_BLOCKS;
     size_t planes = (size_t)ny * nz;
-    return fields_for_precision() * n * esz + n +              // fields + attribute bytes
+    return kStateFields * n * 8 + (fields_for_precision() - kStateFields) * n * esz + n +   // fields + attribute
            (6 * nb + 64) * sizeof(double) +                       // reduction partials
            planes * (3 * sizeof(double) + 2 * sizeof(int)) +      // SEM planes + inlet maps
            3 * planes * sizeof(double) + sizeof(les::Consts) + sizeof(les::Scalars) + (1 << 16);
@@ -338,16 +340,23 @@ int lesgpu_create(const lesgpu_config* cfg, const lesgpu_species* sp, lesgpu_ctx
     if (e != cudaSuccess) { int r = cuda_fail(ctx, e, "cudaSetDevice"); delete ctx; return r; }
     e = cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { int r = cuda_fail(ctx, e, "cudaStreamCreate"); delete ctx; return r; }
-    // one arena for all per-cell fields; each field starts on a 256-byte boundary
+    e = cudaStreamCreateWithFlags(&d.side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&d.ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&d.ev_join, cudaEventDisableTiming);
+    if (e != cudaSuccess) { int r = cuda_fail(ctx, e, "side stream"); lesgpu_destroy(ctx); return r; }
+    // one arena for all per-cell fields; each field starts on a 256-byte boundary.  The
+    // state Phi_n is FP64 in both forms (the RK update runs in FP64); the rest is FP32 in
+    // the precision form.
     const size_t fb = ((d.n * d.esz + 255) / 256) * 256;
+    const size_t fb8 = ((d.n * 8 + 255) / 256) * 256;
     const size_t nf = fields_for_precision();
-    d.arena_bytes = nf * fb;
+    d.arena_bytes = kStateFields * fb8 + (nf - kStateFields) * fb;
     e = cudaMalloc(&d.arena, d.arena_bytes);
     if (e != cudaSuccess) { ctx->d.err = "device arena allocation failed"; lesgpu_destroy(ctx); return LESGPU_ENOMEM; }
     cudaMemsetAsync(d.arena, 0, d.arena_bytes, d.stream);
     char* p = (char*)d.arena;
     auto take = [&]() { void* r = p; p += fb; return r; };
-    for (int q = 0; q < les::NSTATE; q++) d.S[q] = take();
+    for (int q = 0; q < les::NSTATE; q++) { d.S[q] = p; p += fb8; }
     for (int q = 0; q < les::NSTATE; q++) d.St[q] = take();
     for (int q = 0; q < les::NSTATE; q++) d.F[q] = take();
     d.mu_mix = take(); d.nu = take();
@@ -410,6 +419,9 @@ void lesgpu_destroy(lesgpu_ctx* ctx) {
     for (int q = 0; q < 16; q++)
         if (d.marks[q]) cudaEventDestroy(d.marks[q]);
     free_loop(d);
+    if (d.side) { cudaStreamSynchronize(d.side); cudaStreamDestroy(d.side); }
+    if (d.ev_fork) cudaEventDestroy(d.ev_fork);
+    if (d.ev_join) cudaEventDestroy(d.ev_join);
     if (d.stream) cudaStreamDestroy(d.stream);
     delete ctx;
 }
@@ -455,9 +467,9 @@ int lesgpu_upload_attribute(lesgpu_ctx* ctx, const int* attr) {
     return LESGPU_OK;
 }
 
-static int copy_field_in(lesgpu_ctx* ctx, void* dst, const double* src) {
+static int copy_field_in(lesgpu_ctx* ctx, void* dst, const double* src, size_t esz) {
     DevCtx& d = ctx->d;
-    if (d.esz == 8) {
+    if (esz == 8) {
         CK(cudaMemcpyAsync(dst, src, d.n * 8, cudaMemcpyHostToDevice, d.stream));
         CK(cudaStreamSynchronize(d.stream));
         return LESGPU_OK;
@@ -469,9 +481,9 @@ static int copy_field_in(lesgpu_ctx* ctx, void* dst, const double* src) {
     return LESGPU_OK;
 }
 
-static int copy_field_out(lesgpu_ctx* ctx, double* dst, const void* src) {
+static int copy_field_out(lesgpu_ctx* ctx, double* dst, const void* src, size_t esz) {
     DevCtx& d = ctx->d;
-    if (d.esz == 8) {
+    if (esz == 8) {
         CK(cudaMemcpyAsync(dst, src, d.n * 8, cudaMemcpyDeviceToHost, d.stream));
         CK(cudaStreamSynchronize(d.stream));
         return LESGPU_OK;
@@ -488,7 +500,7 @@ int lesgpu_upload_state(lesgpu_ctx* ctx, const double* const* fields, int nfield
     if (!ctx->d.have_attr) return fail(ctx, LESGPU_ESTATE, "upload the attribute map before the state");
     for (int q = 0; q < nfields; q++) {
         if (!fields[q]) return LESGPU_EINVAL;
-        int r = copy_field_in(ctx, ctx->d.S[q], fields[q]);
+        int r = copy_field_in(ctx, ctx->d.S[q], fields[q], 8);
         if (r) return r;
     }
     DevCtx& d = ctx->d;
@@ -508,7 +520,7 @@ int lesgpu_download_state(lesgpu_ctx* ctx, double* const* fields, int nfields) {
     if (!ctx || !fields || nfields < 1 || nfields > LESGPU_NSTATE) return LESGPU_EINVAL;
     for (int q = 0; q < nfields; q++) {
         if (!fields[q]) return LESGPU_EINVAL;
-        int r = copy_field_out(ctx, fields[q], ctx->d.S[q]);
+        int r = copy_field_out(ctx, fields[q], ctx->d.S[q], 8);
         if (r) return r;
     }
     return LESGPU_OK;
@@ -562,7 +574,7 @@ int lesgpu_get_field(lesgpu_ctx* ctx, int id, double* out) {
     } else {
         return fail(ctx, LESGPU_EINVAL, "unknown field id");
     }
-    return copy_field_out(ctx, out, src);
+    return copy_field_out(ctx, out, src, (id >= LESGPU_F_U && id <= LESGPU_F_Y4) ? 8 : d.esz);
 }
 
 int lesgpu_dt_inputs(lesgpu_ctx* ctx, double* umax, double* numax, double* alphamax) {

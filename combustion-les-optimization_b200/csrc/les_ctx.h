@@ -80,6 +80,8 @@ struct DevCtx {
     size_t arena_bytes = 0;
     size_t total_bytes = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;        // SEM plane, overlapped with the RK stages
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     double* h_pinned = nullptr;         // pinned staging for small transfers
     size_t h_pinned_len = 0;
     bool have_attr = false, have_state = false, have_inflow = false;
@@ -115,7 +117,7 @@ void tmark_end(DevCtx& c, int slot);
 void tmark_flush(DevCtx& c);
 
 // Per-precision entry points (les_f64.cu / les_f32.cu).
-cudaError_t sem_inflow(DevCtx& c);
+cudaError_t sem_inflow(DevCtx& c, cudaStream_t st);
 int selfcheck_division(const double* divisors, int nd, size_t n, unsigned long long seed, unsigned long long* bad);
 cudaError_t loop_pre(DevCtx& c);
 cudaError_t step_f64(DevCtx& c, double dt, int t_loop, bool device_mode);

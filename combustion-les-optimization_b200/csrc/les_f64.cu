@@ -10,12 +10,12 @@
 
 namespace les {
 
-cudaError_t sem_inflow(DevCtx& c) {
+cudaError_t sem_inflow(DevCtx& c, cudaStream_t st) {
     if (c.n_inlet <= 0) return cudaSuccess;
     const int tpb = 128;
-    k_sem_plane<<<(c.n_inlet + tpb - 1) / tpb, tpb, 7 * 512 * sizeof(double), c.stream>>>(c.dC, c.inlet_list, c.n_inlet,
-                                                                                         c.vort, c.nv, c.plane);
-    k_sem_normalize<<<1, 256, 0, c.stream>>>(c.dC, c.inlet_list, c.n_inlet, c.plane, c.dS);
+    k_sem_plane<<<(c.n_inlet + tpb - 1) / tpb, tpb, 7 * 512 * sizeof(double), st>>>(c.dC, c.inlet_list, c.n_inlet,
+                                                                                   c.vort, c.nv, c.plane);
+    k_sem_normalize<<<1, 256, 0, st>>>(c.dC, c.inlet_list, c.n_inlet, c.plane, c.dS);
     return cudaGetLastError();
 }
 

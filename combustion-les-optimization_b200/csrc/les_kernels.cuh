@@ -100,7 +100,7 @@ __device__ __forceinline__ R fit_prop(const R co[4], int zero, R L, R L2, R L3) 
     // guard is handled by the callers.
     if (zero) return R(0);
     R lp = (R)co[0] + (R)co[1] * L + (R)co[2] * L2 + (R)co[3] * L3;
-    return exp(lp);
+    return qexp(lp);
 }
 
 template <typename R>
@@ -111,9 +111,9 @@ __device__ __forceinline__ R eos_rho(const Consts& C, R T, const R Y[NSP], R fal
 #pragma unroll
     for (int s = 0; s < NSP; s++) syw += cdv(Y[s], K.d_mwk[s]);
     if (syw > R(1e-9) && T > R(1.0)) {
-        R W = R(1.0) / syw;
-        R Rm = (R)R_UNIV / W;
-        return (R)P_CONST / (Rm * T);
+        R W = qdiv(R(1.0), syw);
+        R Rm = qdiv((R)R_UNIV, W);
+        return qdiv((R)P_CONST, Rm * T);
     }
     return fallback;
 }
@@ -160,12 +160,12 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
         R lam = R(0.025);
         lam_out = lam;
         alpha = R(1.8e-5);
-        aT = (rhof > R(1e-6) && Cp > R(1e-6)) ? lam / (rhof * Cp) : R(0);
+        aT = (rhof > R(1e-6) && Cp > R(1e-6)) ? qdiv(lam, rhof * Cp) : R(0);
         return;
     }
 #pragma unroll
-    for (int s = 0; s < NSP; s++) X[s] = ym[s] / syw;
-    const R L = log(Tl);
+    for (int s = 0; s < NSP; s++) X[s] = qdiv(ym[s], syw);
+    const R L = qlog(Tl);
     const R L2 = L * L;
     const R L3 = pow3_rn(L);
     // pure-species viscosity and conductivity (:394-398, :431-437)
@@ -185,24 +185,24 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
 #pragma unroll
         for (int b = 0; b < NSP; b++) {
             if (X[b] < R(1e-12)) continue;
-            R sr = sqrt(muk[a] / muk[b]);
+            R sr = qsqrt(qdiv(muk[a], muk[b]));
             R t = R(1.0) + sr * (R)K.wpow[a][b];
             R ph = cdv(t * t, K.d_wden[a][b]);
             den += X[b] * ph;
         }
         if (den > R(1e-9)) {
-            mu += (X[a] * muk[a]) / den;
-            lam += (X[a] * lamk[a]) / den;
+            mu += qdiv(X[a] * muk[a], den);
+            lam += qdiv(X[a] * lamk[a], den);
         }
     }
     mu_mix = fmax(R(1e-7), mu);
-    R nuv = (rhof > R(1e-3)) ? mu_mix / rhof : R(1.5e-5);
+    R nuv = (rhof > R(1e-3)) ? qdiv(mu_mix, rhof) : R(1.5e-5);
     nu = fmax(R(1e-7), nuv);
     R lmix = fmax(R(1e-3), lam);
     lam_out = lmix;
     R q = R(0);
     bool qok = (rhof > R(1e-6) && Cp > R(1e-6));
-    if (qok) q = lmix / (rhof * Cp);
+    if (qok) q = qdiv(lmix, rhof * Cp);
     alpha = fmax(R(1e-7), qok ? q : R(1.8e-5));
     aT = q;
     // Hirschfelder-Curtiss (:1716-1749).  Binary coefficients D_kj are evaluated once per
@@ -237,7 +237,7 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
             if (a == b) continue;
             if (X[b] > R(1e-12)) {
                 R Dv = Dm[a][b];
-                if (Dv > R(1e-12)) sx += X[b] / Dv;
+                if (Dv > R(1e-12)) sx += qdiv(X[b], Dv);
             }
         }
         R Dv;
@@ -245,7 +245,7 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
             int o = (a != N2) ? N2 : O2;
             Dv = fit_prop<R>(K.dco[a][o], C.dco_zero[a][o], L, L2, L3) * R(1e-4);
         } else if (sx > R(1e-12)) {
-            Dv = (R(1.0) - X[a]) / sx;
+            Dv = qdiv(R(1.0) - X[a], sx);
         } else {
             Dv = R(1e-5);
         }
@@ -257,9 +257,9 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
 
 // ------------------------------------------------------------------ pass A: filter + props
 
-template <typename R>
+template <typename R, typename RI = R>
 __global__ void __launch_bounds__(NT, MinBlocks<R>::filter)
-    k_filter_props(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> in, F11<R> F, PropBuf<R> P,
+    k_filter_props(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<RI> in, F11<R> F, PropBuf<R> P,
                    double* __restrict__ part, Scalars* __restrict__ S, int want_max) {
     const auto& K = kc<R>(C);
     __shared__ double sh[NT / 32];
@@ -278,11 +278,12 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::filter)
         R f[NSTATE];
 #pragma unroll
         for (int q = 0; q < NSTATE; q++) {
-            const R* __restrict__ x = in.p[q] + id;
+            const RI* __restrict__ x = in.p[q] + id;
             if (filt) {
-                f[q] = cdv(x[-sI] + x[-sJ] + x[-1] + R(FILTER_W) * x[0] + x[1] + x[sJ] + x[sI], K.d_filter);
+                f[q] = cdv(R(x[-sI]) + R(x[-sJ]) + R(x[-1]) + R(FILTER_W) * R(x[0]) + R(x[1]) + R(x[sJ]) + R(x[sI]),
+                           K.d_filter);
             } else {
-                f[q] = x[0];
+                f[q] = R(x[0]);
             }
             F.p[q][id] = f[q];
         }
@@ -375,7 +376,7 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::strain)
         R S11 = du_dx, S22 = dv_dy, S33 = dw_dz;
         R S12 = R(0.5) * (du_dy + dv_dx), S13 = R(0.5) * (du_dz + dw_dx), S23 = R(0.5) * (dv_dz + dw_dy);
         R Sij = R(2.0) * (S12 * S12 + S13 * S13 + S23 * S23) + S11 * S11 + S22 * S22 + S33 * S33;
-        R Smag = sqrt(R(2.0) * Sij);
+        R Smag = qsqrt(R(2.0) * Sij);
         R div = du_dx + dv_dy + dw_dz;
         R g = F.p[4][id];
         if (g < R(0.0)) g = R(0.0);
@@ -390,20 +391,20 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::strain)
         // SSR-SGS turbulent flame speed (:1926-1957)
         R nul = P.nu[id];
         R num = Sij - (div * div) * R(1.0 / 3.0);
-        R X = ((R)K.dx4 / (nul * nul)) * num;
+        R X = qdiv((R)K.dx4, nul * nul) * num;
         R d_eta;
         if (X < R(SMALL)) {
             d_eta = R(1.0);
         } else {
-            R pX = pow(X, R(0.75));
+            R pX = qpow(X, R(0.75));
             R arg = R(SSR_B) * pX;
-            d_eta = R(SSR_A) * pX * (arg > R(1.0) ? log(arg) : R(0.0));
+            d_eta = R(SSR_A) * pX * (arg > R(1.0) ? qlog(arg) : R(0.0));
         }
-        R eta = dx / (d_eta + R(SMALL));
+        R eta = qdiv(dx, d_eta + R(SMALL));
         R Dce = R(8.0) * eta;
-        R asf = R(8.0) * exp((R)K.ssr_cdF / (Dce + R(SMALL)));
+        R asf = R(8.0) * qexp(qdiv((R)K.ssr_cdF, Dce + R(SMALL)));
         R base = cdv(asf * eta, K.d_dx);
-        R wr = pow(base, (R)K.ssr_exp);
+        R wr = qpow(base, (R)K.ssr_exp);
         R te = R(0.0);
         if (K.tau_sl > R(SMALL)) te = cdv(dx * fmax(R(0.0), div), K.d_tau_sl);
         R ratio = wr + te;
@@ -441,7 +442,7 @@ __device__ __forceinline__ R teno5_rec(const Consts& C, R v0, R v1, R v2, R v3, 
     R w0 = (R)d0 * R(0.1), w1 = (R)d1 * R(0.6), w2 = (R)d2 * R(0.3);
     R ws = w0 + w1 + w2;
     if (ws < R(1e-40)) return p1;
-    return (w0 * p0 + w1 * p1 + w2 * p2) / ws;
+    return qdiv(w0 * p0 + w1 * p1 + w2 * p2, ws);
 }
 
 // One axis of the TENO5 G-advection (:2258-2295).
@@ -477,18 +478,18 @@ __device__ __forceinline__ R weno5_grad(const Consts& C, const R* __restrict__ q
     R i0, i1, i2;
     weno_is<R>(p1, p2, p3, p4, p5, i0, i1, i2);
     R e0 = eps + i0, e1 = eps + i1, e2 = eps + i2;
-    R a0 = R(3.0 / 10.0) / (e0 * e0), a1 = R(6.0 / 10.0) / (e1 * e1), a2 = R(1.0 / 10.0) / (e2 * e2);
+    R a0 = qdiv(R(3.0 / 10.0), e0 * e0), a1 = qdiv(R(6.0 / 10.0), e1 * e1), a2 = qdiv(R(1.0 / 10.0), e2 * e2);
     R sa = a0 + a1 + a2;
-    R w0 = a0 / sa, w1 = a1 / sa, w2 = a2 / sa;
+    R w0 = qdiv(a0, sa), w1 = qdiv(a1, sa), w2 = qdiv(a2, sa);
     R s0 = cdv(R(2.0) * p1 - R(7.0) * p2 + R(11.0) * p3, K.d_six);
     R s1 = cdv(-p2 + R(5.0) * p3 + R(2.0) * p4, K.d_six);
     R s2 = cdv(R(2.0) * p3 + R(5.0) * p4 - p5, K.d_six);
     R ph = w0 * s0 + w1 * s1 + w2 * s2;
     weno_is<R>(p0, p1, p2, p3, p4, i0, i1, i2);
     e0 = eps + i0; e1 = eps + i1; e2 = eps + i2;
-    a0 = R(1.0 / 10.0) / (e0 * e0); a1 = R(6.0 / 10.0) / (e1 * e1); a2 = R(3.0 / 10.0) / (e2 * e2);
+    a0 = qdiv(R(1.0 / 10.0), e0 * e0); a1 = qdiv(R(6.0 / 10.0), e1 * e1); a2 = qdiv(R(3.0 / 10.0), e2 * e2);
     sa = a0 + a1 + a2;
-    w0 = a0 / sa; w1 = a1 / sa; w2 = a2 / sa;
+    w0 = qdiv(a0, sa); w1 = qdiv(a1, sa); w2 = qdiv(a2, sa);
     R m0 = cdv(-p0 + R(5.0) * p1 + R(2.0) * p2, K.d_six);
     R m1 = cdv(R(2.0) * p1 + R(5.0) * p2 - p3, K.d_six);
     R m2 = cdv(R(11.0) * p2 - R(7.0) * p3 + R(2.0) * p4, K.d_six);
@@ -510,18 +511,18 @@ template <typename R>
 __device__ __forceinline__ R muscl_axis(R vel, R pm2, R pm1, R p0, R pp1, R pp2, const DCT<R>& d) {
     if (vel >= R(0.0)) {
         R dup_im = pm1 - pm2, ddn_im = p0 - pm1;
-        R r_im = (fabs(ddn_im) < R(SMALL)) ? R(1e9) : dup_im / ddn_im;
+        R r_im = (fabs(ddn_im) < R(SMALL)) ? R(1e9) : qdiv(dup_im, ddn_im);
         R phi_imh = pm1 + R(0.5) * superbee<R>(r_im) * ddn_im;
         R dup_i = p0 - pm1, ddn_i = pp1 - p0;
-        R r_i = (fabs(ddn_i) < R(SMALL)) ? R(1e9) : dup_i / ddn_i;
+        R r_i = (fabs(ddn_i) < R(SMALL)) ? R(1e9) : qdiv(dup_i, ddn_i);
         R phi_iph = p0 + R(0.5) * superbee<R>(r_i) * ddn_i;
         return cdv(vel * (phi_iph - phi_imh), d);
     } else {
         R dup_i = pp1 - p0, ddn_i = p0 - pm1;
-        R r_i = (fabs(ddn_i) < R(SMALL)) ? R(1e9) : dup_i / ddn_i;
+        R r_i = (fabs(ddn_i) < R(SMALL)) ? R(1e9) : qdiv(dup_i, ddn_i);
         R phi_imh = p0 - R(0.5) * superbee<R>(r_i) * ddn_i;
         R dup_ip = pp2 - pp1, ddn_ip = pp1 - p0;
-        R r_ip = (fabs(ddn_ip) < R(SMALL)) ? R(1e9) : dup_ip / ddn_ip;
+        R r_ip = (fabs(ddn_ip) < R(SMALL)) ? R(1e9) : qdiv(dup_ip, ddn_ip);
         R phi_iph = pp1 - R(0.5) * superbee<R>(r_ip) * ddn_ip;
         return cdv(vel * (phi_iph - phi_imh), d);
     }
@@ -670,7 +671,7 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::flow)
                     if (dGz > R(0.0)) dGz = R(0.0);
                 }
                 R df = Gl - (R)K.accel_center;
-                R window = exp(cdv(-(df * df), K.d_w2));
+                R window = qexp(cdv(-(df * df), K.d_w2));
                 // tip_mask is the literal 1.0 in the momentum source (:2638)
                 R cf = (R)K.accel_strength * r0 * window * R(1.0);
                 fx = cf * dGx * R(0.05);
@@ -728,14 +729,14 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::flow)
             gy = cdv(Gf[sJ] - Gf[-sJ], K.d_2dy);
             gz = cdv(Gf[1] - Gf[-1], K.d_2dz);
         }
-        R gmag = sqrt(gx * gx + gy * gy + gz * gz);
+        R gmag = qsqrt(gx * gx + gy * gy + gz * gz);
         R prop = P.ST[id] * gmag;
         R art = R(0);
         if (C.flame_accel) {
             R Gl = Gf[0];
             if (Gl > R(0.1) && Gl < R(0.99)) {
                 R df = Gl - (R)K.accel_center;
-                R window = exp(cdv(-(df * df), K.d_w2));
+                R window = qexp(cdv(-(df * df), K.d_w2));
                 // tip_mask = 1 - exp(-r^2 / 0^2) is exactly 1 for every fluid cell (j >= 1)
                 // because TIP_PROTECTION_RADIUS is 0.0 (:234, :2806-2807).
                 R adc = R(5.0) * (P.nu_t[id] + R(1.0e-5)) * window * R(1.0);
@@ -758,9 +759,9 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::flow)
 
 // C2: species (:2837-2904) and temperature (:2912-2962), then the RK4 bookkeeping.
 // stage: 0,1,2 -> intermediate stage with coefficient 0.5/0.5/1.0, 3 -> final combine.
-template <typename R>
+template <typename R, typename RS = R>
 __global__ void __launch_bounds__(NT, MinBlocks<R>::scalar)
-    k_rhs_scalar(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> F, PropBuf<R> P, F11<R> S0, F11<R> St,
+    k_rhs_scalar(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> F, PropBuf<R> P, F11<RS> S0, F11<R> St,
                  AccBuf<R> acc, KFlow<R> kf, KDbg<R> kd, const Scalars* __restrict__ Sc, int stage) {
     const auto& K = kc<R>(C);
     const int nx = C.nx, ny = C.ny, nz = C.nz;
@@ -777,18 +778,18 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::scalar)
         // rho_temp is only ever written on outlet/fluid cells (:1893), so it stays 0 on
         // inlet/wall/symmetry cells.  These values are the same for all stages of a step.
         if (stage == 0) {
-            R Y0[NSP];
+            RS Y0[NSP];
 #pragma unroll
             for (int q = 0; q < NSTATE; q++)
-                if (q != 5) St.p[q][id] = S0.p[q][id];
+                if (q != 5) St.p[q][id] = R(S0.p[q][id]);
 #pragma unroll
             for (int s = 0; s < NSP; s++) Y0[s] = S0.p[6 + s][id];
-            if (a == 2) St.p[5][id] = eos_rho<R>(C, S0.p[3][id], Y0, S0.p[5][id]);
+            if (a == 2) St.p[5][id] = R(eos_rho<RS>(C, S0.p[3][id], Y0, S0.p[5][id]));
         } else if (stage == 3 && a == 2) {
-            R Y0[NSP];
+            RS Y0[NSP];
 #pragma unroll
             for (int s = 0; s < NSP; s++) Y0[s] = S0.p[6 + s][id];
-            S0.p[5][id] = eos_rho<R>(C, S0.p[3][id], Y0, S0.p[5][id]);
+            S0.p[5][id] = eos_rho<RS>(C, S0.p[3][id], Y0, S0.p[5][id]);
         }
         if (kd.p[0]) {
 #pragma unroll
@@ -855,41 +856,48 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::scalar)
 #pragma unroll
         for (int q = 0; q < NACC; q++) incr[q] = acc.p[q][id] + kv[q];
     }
-    const R cdt = fin ? (R)(dt / 6.0) : (R)((stage == 2 ? 1.0 : 0.5) * dt);
-    const R rho_n = S0.p[5][id];
-    R Tn = S0.p[3][id] + cdt * incr[3];
-    R Gn = S0.p[4][id] + cdt * incr[4];
-    R Y[NSP];
+    // The update itself runs in the state's type: in the FP32 form the right-hand sides are
+    // FP32 and Phi_n, the stage update and the final combine FP64, so increments far below
+    // the state's FP32 ulp are not rounded away step after step.
+    const RS cdt = fin ? (RS)(dt / 6.0) : (RS)((stage == 2 ? 1.0 : 0.5) * dt);
+    const RS rho_n = S0.p[5][id];
+    RS Tn = S0.p[3][id] + cdt * (RS)incr[3];
+    RS Gn = S0.p[4][id] + cdt * (RS)incr[4];
+    RS Y[NSP];
 #pragma unroll
-    for (int s = 0; s < NSP; s++) Y[s] = S0.p[6 + s][id] + cdt * incr[5 + s];
-    Tn = fmax(R(200.0), fmin(R(3000.0), Tn));
-    Gn = fmax(R(0.0), fmin(R(1.0), Gn));
-    R sy = R(0);
+    for (int s = 0; s < NSP; s++) Y[s] = S0.p[6 + s][id] + cdt * (RS)incr[5 + s];
+    Tn = fmax(RS(200.0), fmin(RS(3000.0), Tn));
+    Gn = fmax(RS(0.0), fmin(RS(1.0), Gn));
+    RS sy = RS(0);
 #pragma unroll
     for (int s = 0; s < NSP; s++) {
-        Y[s] = fmax(R(0.0), fmin(R(1.0), Y[s]));
+        Y[s] = fmax(RS(0.0), fmin(RS(1.0), Y[s]));
         sy += Y[s];
     }
-    if (sy > R(SMALL)) {
+    if (sy > RS(SMALL)) {
 #pragma unroll
         for (int s = 0; s < NSP; s++) Y[s] /= sy;
     }
-    R rn = eos_rho<R>(C, Tn, Y, rho_n);
-    R vel[3];
+    RS rn = eos_rho<RS>(C, Tn, Y, rho_n);
+    RS vel[3];
 #pragma unroll
     for (int q = 0; q < 3; q++) {
-        R m = rho_n * S0.p[q][id] + cdt * incr[q];   // rhou = rho*u after the BC (:3146)
-        vel[q] = (rn > R(SMALL)) ? m / rn : R(0);
+        RS m = rho_n * S0.p[q][id] + cdt * (RS)incr[q];   // rhou = rho*u after the BC (:3146)
+        vel[q] = (rn > RS(SMALL)) ? qdiv(m, rn) : RS(0);
     }
-    R* const* out = fin ? S0.p : St.p;
-    out[0][id] = vel[0];
-    out[1][id] = vel[1];
-    out[2][id] = vel[2];
-    out[3][id] = Tn;
-    out[4][id] = Gn;
-    out[5][id] = rn;
+    if (fin) {
+        RS* const* out = S0.p;
+        out[0][id] = vel[0]; out[1][id] = vel[1]; out[2][id] = vel[2];
+        out[3][id] = Tn; out[4][id] = Gn; out[5][id] = rn;
 #pragma unroll
-    for (int s = 0; s < NSP; s++) out[6 + s][id] = Y[s];
+        for (int s = 0; s < NSP; s++) out[6 + s][id] = Y[s];
+    } else {
+        R* const* out = St.p;
+        out[0][id] = R(vel[0]); out[1][id] = R(vel[1]); out[2][id] = R(vel[2]);
+        out[3][id] = R(Tn); out[4][id] = R(Gn); out[5][id] = R(rn);
+#pragma unroll
+        for (int s = 0; s < NSP; s++) out[6 + s][id] = R(Y[s]);
+    }
 }
 
 // ------------------------------------------------------------------ boundary conditions
@@ -912,7 +920,7 @@ __device__ __forceinline__ void ambient_cell(const Consts& C, F11<R>& S, size_t 
     for (int s = 0; s < NSP; s++) S.p[6 + s][dst] = (R)K.ambientYk[s];
 }
 
-template <typename R>
+template <typename R, typename Form = R>
 __global__ void k_bc_iface(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> S,
                            const double* __restrict__ plane, const double* __restrict__ noise,
                            const int* __restrict__ inlet_pos) {
@@ -950,7 +958,7 @@ __global__ void k_bc_iface(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, 
     if (attr[in] == 2) copy_cell<R>(S, in, im);
 }
 
-template <typename R>
+template <typename R, typename Form = R>
 __global__ void k_bc_jface(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> S) {
     const int ny = C.ny, nz = C.nz;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -973,7 +981,7 @@ __global__ void k_bc_jface(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, 
     }
 }
 
-template <typename R>
+template <typename R, typename Form = R>
 __global__ void k_bc_kface(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> S) {
     const int ny = C.ny, nz = C.nz;
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -993,7 +1001,7 @@ __global__ void k_bc_kface(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, 
 
 // EOS + renormalisation everywhere (:3130-3160) fused with the max-velocity reduction
 // over inlet/fluid cells for the next dt (:1472-1485).
-template <typename R>
+template <typename R, typename Form = R>
 __global__ void __launch_bounds__(NT) k_bc_eos(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> S,
                                                double* __restrict__ part, Scalars* __restrict__ Sc) {
     const auto& K = kc<R>(C);
@@ -1015,7 +1023,7 @@ __global__ void __launch_bounds__(NT) k_bc_eos(LES_KERNEL_CONSTS, const uint8_t*
         R syw = R(0);
 #pragma unroll
         for (int s = 0; s < NSP; s++) syw += cdv(Y[s], K.d_mwk[s]);
-        R rho = (syw > R(1e-9) && T > R(1.0)) ? (R)P_CONST / ((R)R_UNIV / (R(1.0) / syw) * T) : R(1.2);
+        R rho = (syw > R(1e-9) && T > R(1.0)) ? qdiv((R)P_CONST, qdiv((R)R_UNIV, qdiv(R(1.0), syw)) * T) : R(1.2);
         S.p[5][id] = rho;
         if (a == 3 || a == 2 || a == 5) {
             R sy = R(0);
@@ -1023,7 +1031,7 @@ __global__ void __launch_bounds__(NT) k_bc_eos(LES_KERNEL_CONSTS, const uint8_t*
             for (int s = 0; s < NSP; s++) sy += Y[s];
             if (sy > R(1e-6)) {
 #pragma unroll
-                for (int s = 0; s < NSP; s++) S.p[6 + s][id] = Y[s] / sy;
+                for (int s = 0; s < NSP; s++) S.p[6 + s][id] = qdiv(Y[s], sy);
             }
         }
         if (a == 1 || a == 3) {
@@ -1054,7 +1062,7 @@ __global__ void __launch_bounds__(NT) k_bc_eos(LES_KERNEL_CONSTS, const uint8_t*
 }
 
 // Max velocity over inlet/fluid cells without touching the state (after an upload).
-template <typename R>
+template <typename R, typename Form = R>
 __global__ void __launch_bounds__(NT) k_umax(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> S,
                                              double* __restrict__ part, Scalars* __restrict__ Sc) {
     __shared__ double sh[NT / 32];
@@ -1097,7 +1105,7 @@ __global__ void __launch_bounds__(NT) k_umax(LES_KERNEL_CONSTS, const uint8_t* _
 
 // ------------------------------------------------------------------ diagnostics
 
-template <typename R>
+template <typename R, typename Form = R>
 __global__ void __launch_bounds__(NT) k_monitor(LES_KERNEL_CONSTS, F11<R> S, double* __restrict__ part,
                                                 Scalars* __restrict__ Sc, size_t n) {
     // write_monitor_log (:3884-3897)
@@ -1151,8 +1159,8 @@ __global__ void __launch_bounds__(NT) k_monitor(LES_KERNEL_CONSTS, F11<R> S, dou
     }
 }
 
-template <typename R>
-__global__ void k_probe(LES_KERNEL_CONSTS, F11<R> S, PropBuf<R> P, const int* __restrict__ st, int n, int kline,
+template <typename RS, typename R = RS>
+__global__ void k_probe(LES_KERNEL_CONSTS, F11<RS> S, PropBuf<R> P, const int* __restrict__ st, int n, int kline,
                         double* __restrict__ out) {
     const int ny = C.ny, nz = C.nz;
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1176,8 +1184,8 @@ static __global__ void k_set_step(Scalars* __restrict__ Sc, double dt, int t_loo
 
 // Device loop, after the boundary conditions: the probe lines of record_flame_region_data
 // (:3403-3471) and dt/|u|max of this step go to history slot run_step.
-template <typename R>
-__global__ void k_loop_post(LES_KERNEL_CONSTS, F11<R> S, PropBuf<R> P, const Scalars* __restrict__ Sc,
+template <typename RS, typename R = RS>
+__global__ void k_loop_post(LES_KERNEL_CONSTS, F11<RS> S, PropBuf<R> P, const Scalars* __restrict__ Sc,
                             const int* __restrict__ st, int n, int kline, int cap, double* __restrict__ hprobe,
                             double* __restrict__ hdt, double* __restrict__ humax) {
     const int ny = C.ny, nz = C.nz;
@@ -1202,7 +1210,7 @@ __global__ void k_loop_post(LES_KERNEL_CONSTS, F11<R> S, PropBuf<R> P, const Sca
 
 // Device loop: the monitor reductions (:3874-3918) on steps with t_loop % 10 == 0, written
 // to history slot run_step (other slots are left untouched).
-template <typename R>
+template <typename R, typename Form = R>
 __global__ void __launch_bounds__(NT) k_loop_monitor(LES_KERNEL_CONSTS, F11<R> S, double* __restrict__ part,
                                                      Scalars* __restrict__ Sc, size_t n, int cap,
                                                      double* __restrict__ hmon) {
@@ -1265,7 +1273,7 @@ static __global__ void k_loop_tick(Scalars* __restrict__ Sc) {
     Sc->run_step += 1;
 }
 
-template <typename R>
+template <typename R, typename Form = R>
 __global__ void k_check_finite(const R* __restrict__ x, size_t n, int* __restrict__ flag) {
     for (size_t id = (size_t)blockIdx.x * blockDim.x + threadIdx.x; id < n; id += (size_t)gridDim.x * blockDim.x)
         if (!isfinite((double)x[id])) atomicExch(flag, 1);

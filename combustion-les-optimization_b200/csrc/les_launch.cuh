@@ -7,6 +7,9 @@
 
 namespace les {
 
+// The state Phi_n is FP64 in both forms; R is the form's type of every other field.
+using RS = double;
+
 template <typename R>
 static F11<R> f11(void* const* p) {
     F11<R> f;
@@ -65,7 +68,8 @@ cudaError_t step_impl(DevCtx& c, double dt, int t_loop, bool device_mode) {
     const dim3 gC = cell_grid(c, SH_FLOW), bC = cell_block(c, SH_FLOW);
     const dim3 gD = cell_grid(c, SH_SCALAR), bD = cell_block(c, SH_SCALAR);
     const dim3 gE = cell_grid(c, SH_EOS), bE = cell_block(c, SH_EOS);
-    F11<R> S = f11<R>(c.S), St = f11<R>(c.St), F = f11<R>(c.F);
+    F11<RS> S = f11<RS>(c.S);
+    F11<R> St = f11<R>(c.St), F = f11<R>(c.F);
     PropBuf<R> P = props<R>(c);
     AccBuf<R> acc;
     for (int q = 0; q < NACC; q++) acc.p[q] = (R*)c.acc[q];
@@ -79,14 +83,24 @@ cudaError_t step_impl(DevCtx& c, double dt, int t_loop, bool device_mode) {
     int tm = tmark_begin(c, 0);
     if (device_mode) loop_pre(c);
     else k_set_step<<<1, 1, 0, st>>>(c.dS, dt, t_loop);
-    // SEM inflow plane (:943-1075)
-    sem_inflow(c);
+    // SEM inflow plane (:943-1075).  Only the boundary conditions read it, so it runs on a
+    // side stream beside the four RK stages (joined before the BC); with kernel timing on
+    // it runs in line so that its events bracket it alone.
+    const bool overlap = !c.timing && c.side && c.n_inlet > 0;
+    if (overlap) {
+        cudaEventRecord(c.ev_fork, st);
+        cudaStreamWaitEvent(c.side, c.ev_fork, 0);
+        sem_inflow(c, c.side);
+        cudaEventRecord(c.ev_join, c.side);
+    } else {
+        sem_inflow(c, st);
+    }
     tmark_end(c, tm);
     // four RK4 stages (:4428-4544)
     for (int s = 0; s < 4; s++) {
-        F11<R> in = (s == 0) ? S : St;
         tm = tmark_begin(c, 1);
-        k_filter_props<R><<<gA, bA, 0, st>>>(c.hC, c.attr, in, F, P, c.part, c.dS, s == 3 ? 1 : 0);
+        if (s == 0) k_filter_props<R, RS><<<gA, bA, 0, st>>>(c.hC, c.attr, S, F, P, c.part, c.dS, 0);
+        else k_filter_props<R, R><<<gA, bA, 0, st>>>(c.hC, c.attr, St, F, P, c.part, c.dS, s == 3 ? 1 : 0);
         tmark_end(c, tm);
         tm = tmark_begin(c, 2);
         k_strain<R><<<gB, bB, 0, st>>>(c.hC, c.attr, F, P);
@@ -97,26 +111,27 @@ cudaError_t step_impl(DevCtx& c, double dt, int t_loop, bool device_mode) {
         k_rhs_flow<R><<<gC, bC, 0, st>>>(c.hC, c.attr, F, P, kf, kds, c.dS);
         tmark_end(c, tm);
         tm = tmark_begin(c, 5);
-        k_rhs_scalar<R><<<gD, bD, 0, st>>>(c.hC, c.attr, F, P, S, St, acc, kf, kds, c.dS, s);
+        k_rhs_scalar<R, RS><<<gD, bD, 0, st>>>(c.hC, c.attr, F, P, S, St, acc, kf, kds, c.dS, s);
         tmark_end(c, tm);
     }
     // apply_boundary_conditions (:2967-3161)
+    if (overlap) cudaStreamWaitEvent(st, c.ev_join, 0);
     tm = tmark_begin(c, 4);
     {
         const int tpb = 128;
-        k_bc_iface<R><<<dim3((c.nz + tpb - 1) / tpb, c.ny), tpb, 0, st>>>(c.hC, c.attr, S, c.plane, c.noise,
-                                                                            c.inlet_pos);
+        k_bc_iface<RS, R><<<dim3((c.nz + tpb - 1) / tpb, c.ny), tpb, 0, st>>>(c.hC, c.attr, S, c.plane, c.noise,
+                                                                                c.inlet_pos);
         if (c.nx > 2) {
-            k_bc_jface<R><<<dim3((c.nz + tpb - 1) / tpb, c.nx - 2), tpb, 0, st>>>(c.hC, c.attr, S);
-            k_bc_kface<R><<<dim3((c.ny + tpb - 1) / tpb, c.nx - 2), tpb, 0, st>>>(c.hC, c.attr, S);
+            k_bc_jface<RS, R><<<dim3((c.nz + tpb - 1) / tpb, c.nx - 2), tpb, 0, st>>>(c.hC, c.attr, S);
+            k_bc_kface<RS, R><<<dim3((c.ny + tpb - 1) / tpb, c.nx - 2), tpb, 0, st>>>(c.hC, c.attr, S);
         }
-        k_bc_eos<R><<<gE, bE, 0, st>>>(c.hC, c.attr, S, c.part, c.dS);
+        k_bc_eos<RS, R><<<gE, bE, 0, st>>>(c.hC, c.attr, S, c.part, c.dS);
     }
     if (device_mode) {
         const int tpb = 64;
-        k_loop_post<R><<<dim3((c.ny + tpb - 1) / tpb, c.loop_nst > 0 ? c.loop_nst : 1), tpb, 0, st>>>(
+        k_loop_post<RS, R><<<dim3((c.ny + tpb - 1) / tpb, c.loop_nst > 0 ? c.loop_nst : 1), tpb, 0, st>>>(
             c.hC, S, P, c.dS, c.loop_st, c.loop_nst, c.loop_kline, c.loop_cap, c.hist_probe, c.hist_dt, c.hist_umax);
-        k_loop_monitor<R><<<MON_BLOCKS, NT, 0, st>>>(c.hC, S, c.part, c.dS, c.n, c.loop_cap, c.hist_mon);
+        k_loop_monitor<RS, R><<<MON_BLOCKS, NT, 0, st>>>(c.hC, S, c.part, c.dS, c.n, c.loop_cap, c.hist_mon);
         k_loop_tick<<<1, 1, 0, st>>>(c.dS);
     }
     tmark_end(c, tm);
@@ -132,7 +147,8 @@ template <typename R>
 cudaError_t rhs_only_impl(DevCtx& c, int t_loop) {
     cudaStream_t st = c.stream;
     if (!part_fits(c, cell_blocks(c, SH_FILTER), 3)) return cudaErrorInvalidValue;
-    F11<R> S = f11<R>(c.S), St = f11<R>(c.St), F = f11<R>(c.F);
+    F11<RS> S = f11<RS>(c.S);
+    F11<R> St = f11<R>(c.St), F = f11<R>(c.F);
     PropBuf<R> P = props<R>(c);
     AccBuf<R> acc;
     for (int q = 0; q < NACC; q++) acc.p[q] = (R*)c.acc[q];
@@ -142,8 +158,8 @@ cudaError_t rhs_only_impl(DevCtx& c, int t_loop) {
     for (int q = 0; q < 4; q++) kf.p[q] = (R*)c.kflow[q];
     k_set_step<<<1, 1, 0, st>>>(c.dS, 0.0, t_loop);
     int tm = tmark_begin(c, 1);
-    k_filter_props<R><<<cell_grid(c, SH_FILTER), cell_block(c, SH_FILTER), 0, st>>>(c.hC, c.attr, S, F, P, c.part,
-                                                                                   c.dS, 1);
+    k_filter_props<R, RS><<<cell_grid(c, SH_FILTER), cell_block(c, SH_FILTER), 0, st>>>(c.hC, c.attr, S, F, P,
+                                                                                       c.part, c.dS, 1);
     tmark_end(c, tm);
     tm = tmark_begin(c, 2);
     k_strain<R><<<cell_grid(c, SH_STRAIN), cell_block(c, SH_STRAIN), 0, st>>>(c.hC, c.attr, F, P);
@@ -152,8 +168,8 @@ cudaError_t rhs_only_impl(DevCtx& c, int t_loop) {
     k_rhs_flow<R><<<cell_grid(c, SH_FLOW), cell_block(c, SH_FLOW), 0, st>>>(c.hC, c.attr, F, P, kf, kd, c.dS);
     tmark_end(c, tm);
     tm = tmark_begin(c, 5);
-    k_rhs_scalar<R><<<cell_grid(c, SH_SCALAR), cell_block(c, SH_SCALAR), 0, st>>>(c.hC, c.attr, F, P, S, St, acc,
-                                                                                   kf, kd, c.dS, 0);
+    k_rhs_scalar<R, RS><<<cell_grid(c, SH_SCALAR), cell_block(c, SH_SCALAR), 0, st>>>(c.hC, c.attr, F, P, S, St,
+                                                                                       acc, kf, kd, c.dS, 0);
     tmark_end(c, tm);
     tmark_flush(c);
     return cudaGetLastError();
@@ -162,7 +178,8 @@ cudaError_t rhs_only_impl(DevCtx& c, int t_loop) {
 template <typename R>
 cudaError_t umax_impl(DevCtx& c) {
     if (!part_fits(c, cell_blocks(c, SH_EOS), 1)) return cudaErrorInvalidValue;
-    k_umax<R><<<cell_grid(c, SH_EOS), cell_block(c, SH_EOS), 0, c.stream>>>(c.hC, c.attr, f11<R>(c.S), c.part, c.dS);
+    k_umax<RS, R><<<cell_grid(c, SH_EOS), cell_block(c, SH_EOS), 0, c.stream>>>(c.hC, c.attr, f11<RS>(c.S), c.part,
+                                                                               c.dS);
     return cudaGetLastError();
 }
 
@@ -170,23 +187,23 @@ template <typename R>
 cudaError_t monitor_impl(DevCtx& c) {
     const int nb = MON_BLOCKS;
     if (!part_fits(c, nb, 6)) return cudaErrorInvalidValue;
-    k_monitor<R><<<nb, NT, 0, c.stream>>>(c.hC, f11<R>(c.S), c.part, c.dS, c.n);
+    k_monitor<RS, R><<<nb, NT, 0, c.stream>>>(c.hC, f11<RS>(c.S), c.part, c.dS, c.n);
     return cudaGetLastError();
 }
 
 template <typename R>
 cudaError_t probe_impl(DevCtx& c, int n, int kline) {
     const int tpb = 64;
-    k_probe<R><<<dim3((c.ny + tpb - 1) / tpb, n), tpb, 0, c.stream>>>(c.hC, f11<R>(c.S), props<R>(c), c.probe_st, n,
-                                                                      kline, c.probe_out);
+    k_probe<RS, R><<<dim3((c.ny + tpb - 1) / tpb, n), tpb, 0, c.stream>>>(c.hC, f11<RS>(c.S), props<R>(c), c.probe_st,
+                                                                          n, kline, c.probe_out);
     return cudaGetLastError();
 }
 
 template <typename R>
 cudaError_t check_impl(DevCtx& c, int field) {
     cudaMemsetAsync(c.flag, 0, sizeof(int), c.stream);
-    const R* x = (field < NSTATE) ? (const R*)c.S[field] : (const R*)c.nu_t;
-    k_check_finite<R><<<592, 256, 0, c.stream>>>(x, c.n, c.flag);
+    if (field < NSTATE) k_check_finite<RS, R><<<592, 256, 0, c.stream>>>((const RS*)c.S[field], c.n, c.flag);
+    else k_check_finite<R, R><<<592, 256, 0, c.stream>>>((const R*)c.nu_t, c.n, c.flag);
     return cudaGetLastError();
 }
 
