@@ -175,19 +175,28 @@ __device__ __forceinline__ float cdv(float x, const DCT<float>& d) { return x * 
 // reference does; the FP32 form uses the hardware approximations (MUFU ex2/lg2/rcp/sqrt,
 // ~2 ulp), which its stated error budget covers.
 __device__ __forceinline__ double qdiv(double a, double b) { return a / b; }
+#ifdef LES_FP32_IEEE_MATH
+// build option: the FP32 form with IEEE float operations (for error attribution)
+__device__ __forceinline__ float qdiv(float a, float b) { return a / b; }
+__device__ __forceinline__ float qexp(float x) { return expf(x); }
+__device__ __forceinline__ float qlog(float x) { return logf(x); }
+__device__ __forceinline__ float qpow(float a, float b) { return powf(a, b); }
+__device__ __forceinline__ float qsqrt(float x) { return sqrtf(x); }
+#else
 __device__ __forceinline__ float qdiv(float a, float b) { return __fdividef(a, b); }
-__device__ __forceinline__ double qexp(double x) { return exp(x); }
 __device__ __forceinline__ float qexp(float x) { return __expf(x); }
-__device__ __forceinline__ double qlog(double x) { return log(x); }
 __device__ __forceinline__ float qlog(float x) { return __logf(x); }
-__device__ __forceinline__ double qpow(double a, double b) { return pow(a, b); }
 __device__ __forceinline__ float qpow(float a, float b) { return __powf(a, b); }
-__device__ __forceinline__ double qsqrt(double x) { return sqrt(x); }
 __device__ __forceinline__ float qsqrt(float x) {
     float r;
     asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
 }
+#endif
+__device__ __forceinline__ double qexp(double x) { return exp(x); }
+__device__ __forceinline__ double qlog(double x) { return log(x); }
+__device__ __forceinline__ double qpow(double a, double b) { return pow(a, b); }
+__device__ __forceinline__ double qsqrt(double x) { return sqrt(x); }
 
 // x^3 and x^4 rounded once: glibc pow() returns the correctly rounded power for these
 // arguments, while a plain product rounds twice.  The exact square is split with fma,
