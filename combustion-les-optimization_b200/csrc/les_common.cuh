@@ -198,6 +198,22 @@ __device__ __forceinline__ double qlog(double x) { return log(x); }
 __device__ __forceinline__ double qpow(double a, double b) { return pow(a, b); }
 __device__ __forceinline__ double qsqrt(double x) { return sqrt(x); }
 
+// Division of FP64 state quantities (RK update, EOS, renormalisation).  The FP64 form divides
+// in IEEE double, as the reference does.  The FP32 form keeps its state in FP64 only so that
+// small increments survive; there a float reciprocal refined by one Newton step and one
+// quotient correction in double (relative error ~1e-15) replaces the division sequence.
+template <typename Form>
+__device__ __forceinline__ double sdiv(double a, double b);
+template <>
+__device__ __forceinline__ double sdiv<double>(double a, double b) { return a / b; }
+template <>
+__device__ __forceinline__ double sdiv<float>(double a, double b) {
+    double y = (double)__frcp_rn((float)b);
+    y = fma(y, fma(-b, y, 1.0), y);
+    const double q = a * y;
+    return fma(fma(-q, b, a), y, q);
+}
+
 // x^3 and x^4 rounded once: glibc pow() returns the correctly rounded power for these
 // arguments, while a plain product rounds twice.  The exact square is split with fma,
 // the rest is carried as a double-double and rounded once at the end.

@@ -80,7 +80,7 @@ struct KFlow {               // momentum and G right-hand sides handed from C1 t
 #define LES_MINB_FLOW_F32 8
 #endif
 #ifndef LES_MINB_SCALAR_F32
-#define LES_MINB_SCALAR_F32 6
+#define LES_MINB_SCALAR_F32 5
 #endif
 template <typename R>
 struct MinBlocks {
@@ -114,6 +114,19 @@ __device__ __forceinline__ R eos_rho(const Consts& C, R T, const R Y[NSP], R fal
         R W = qdiv(R(1.0), syw);
         R Rm = qdiv((R)R_UNIV, W);
         return qdiv((R)P_CONST, Rm * T);
+    }
+    return fallback;
+}
+// The same on the FP64 state, with the state division of the precision form Form.
+template <typename Form>
+__device__ __forceinline__ double eos_rho_state(const Consts& C, double T, const double Y[NSP], double fallback) {
+    double syw = 0.0;
+#pragma unroll
+    for (int s = 0; s < NSP; s++) syw += cdv(Y[s], C.d_mwk[s]);
+    if (syw > 1e-9 && T > 1.0) {
+        double W = sdiv<Form>(1.0, syw);
+        double Rm = sdiv<Form>(R_UNIV, W);
+        return sdiv<Form>(P_CONST, Rm * T);
     }
     return fallback;
 }
@@ -784,12 +797,12 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::scalar)
                 if (q != 5) St.p[q][id] = R(S0.p[q][id]);
 #pragma unroll
             for (int s = 0; s < NSP; s++) Y0[s] = S0.p[6 + s][id];
-            if (a == 2) St.p[5][id] = R(eos_rho<RS>(C, S0.p[3][id], Y0, S0.p[5][id]));
+            if (a == 2) St.p[5][id] = R(eos_rho_state<R>(C, S0.p[3][id], Y0, S0.p[5][id]));
         } else if (stage == 3 && a == 2) {
             RS Y0[NSP];
 #pragma unroll
             for (int s = 0; s < NSP; s++) Y0[s] = S0.p[6 + s][id];
-            S0.p[5][id] = eos_rho<RS>(C, S0.p[3][id], Y0, S0.p[5][id]);
+            S0.p[5][id] = eos_rho_state<R>(C, S0.p[3][id], Y0, S0.p[5][id]);
         }
         if (kd.p[0]) {
 #pragma unroll
@@ -876,14 +889,14 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::scalar)
     }
     if (sy > RS(SMALL)) {
 #pragma unroll
-        for (int s = 0; s < NSP; s++) Y[s] /= sy;
+        for (int s = 0; s < NSP; s++) Y[s] = sdiv<R>(Y[s], sy);
     }
-    RS rn = eos_rho<RS>(C, Tn, Y, rho_n);
+    RS rn = eos_rho_state<R>(C, Tn, Y, rho_n);
     RS vel[3];
 #pragma unroll
     for (int q = 0; q < 3; q++) {
         RS m = rho_n * S0.p[q][id] + cdt * (RS)incr[q];   // rhou = rho*u after the BC (:3146)
-        vel[q] = (rn > RS(SMALL)) ? qdiv(m, rn) : RS(0);
+        vel[q] = (rn > RS(SMALL)) ? sdiv<R>(m, rn) : RS(0);
     }
     if (fin) {
         RS* const* out = S0.p;
@@ -1023,7 +1036,8 @@ __global__ void __launch_bounds__(NT) k_bc_eos(LES_KERNEL_CONSTS, const uint8_t*
         R syw = R(0);
 #pragma unroll
         for (int s = 0; s < NSP; s++) syw += cdv(Y[s], K.d_mwk[s]);
-        R rho = (syw > R(1e-9) && T > R(1.0)) ? qdiv((R)P_CONST, qdiv((R)R_UNIV, qdiv(R(1.0), syw)) * T) : R(1.2);
+        R rho = (syw > R(1e-9) && T > R(1.0)) ? sdiv<Form>(P_CONST, sdiv<Form>(R_UNIV, sdiv<Form>(1.0, syw)) * T)
+                                              : R(1.2);
         S.p[5][id] = rho;
         if (a == 3 || a == 2 || a == 5) {
             R sy = R(0);
@@ -1031,7 +1045,7 @@ __global__ void __launch_bounds__(NT) k_bc_eos(LES_KERNEL_CONSTS, const uint8_t*
             for (int s = 0; s < NSP; s++) sy += Y[s];
             if (sy > R(1e-6)) {
 #pragma unroll
-                for (int s = 0; s < NSP; s++) S.p[6 + s][id] = qdiv(Y[s], sy);
+                for (int s = 0; s < NSP; s++) S.p[6 + s][id] = sdiv<Form>(Y[s], sy);
             }
         }
         if (a == 1 || a == 3) {
