@@ -409,7 +409,7 @@ void lesgpu_destroy(lesgpu_ctx* ctx) {
     DevCtx& d = ctx->d;
     if (d.stream) cudaStreamSynchronize(d.stream);
     void* bufs[] = {d.arena, d.attr, d.dC, d.dS, d.part, d.plane, d.noise, d.vort, d.inlet_list, d.inlet_pos,
-                    d.probe_st, d.probe_out, d.flag, d.dbg_cp, d.dbg_lam, d.dbg_alpha};
+                    d.probe_st, d.probe_out, d.flag, d.dbg_cp, d.dbg_lam, d.dbg_alpha, d.avg};
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (int q = 0; q < les::NACC; q++)
@@ -954,6 +954,64 @@ int lesgpu_autotune(lesgpu_ctx* ctx, int reps, int tiles_out[5], double* ms_out)
     if (ms_out)
         for (int c = 0; c < 4; c++)
             for (int t = 0; t < les::NSHAPES; t++) ms_out[c * les::NSHAPES + t] = ms[c][t];
+    return LESGPU_OK;
+}
+
+// ---------------------------------------------------------------- time averages
+
+int lesgpu_avg_begin(lesgpu_ctx* ctx, int start_step) {
+    if (!ctx) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    CK(cudaStreamSynchronize(d.stream));
+    const size_t bytes = (size_t)les::NAVG * d.n * sizeof(double);
+    if (!d.avg) {
+        CK(cudaMalloc(&d.avg, bytes));
+        d.total_bytes += bytes;
+    }
+    CK(cudaMemsetAsync(d.avg, 0, bytes, d.stream));
+    CK(cudaMemsetAsync((char*)d.dS + offsetof(les::Scalars, avg_steps), 0, sizeof(int), d.stream));
+    CK(cudaStreamSynchronize(d.stream));
+    d.avg_start = start_step;
+    drop_graph(d);
+    return LESGPU_OK;
+}
+
+int lesgpu_avg_end(lesgpu_ctx* ctx) {
+    if (!ctx) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    CK(cudaStreamSynchronize(d.stream));
+    if (d.avg) {
+        cudaFree(d.avg);
+        d.avg = nullptr;
+        d.total_bytes -= (size_t)les::NAVG * d.n * sizeof(double);
+    }
+    drop_graph(d);
+    return LESGPU_OK;
+}
+
+int lesgpu_avg_download(lesgpu_ctx* ctx, double* const* sums, int* count) {
+    if (!ctx || !sums || !count) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    if (!d.avg) return fail(ctx, LESGPU_ESTATE, "time averages are not enabled (lesgpu_avg_begin)");
+    CK(cudaStreamSynchronize(d.stream));
+    for (int q = 0; q < les::NAVG; q++) {
+        if (!sums[q]) return LESGPU_EINVAL;
+        CK(cudaMemcpy(sums[q], d.avg + (size_t)q * d.n, d.n * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    CK(cudaMemcpy(count, (char*)d.dS + offsetof(les::Scalars, avg_steps), sizeof(int), cudaMemcpyDeviceToHost));
+    return LESGPU_OK;
+}
+
+int lesgpu_avg_upload(lesgpu_ctx* ctx, const double* const* sums, int count) {
+    if (!ctx || !sums || count < 0) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    if (!d.avg) return fail(ctx, LESGPU_ESTATE, "time averages are not enabled (lesgpu_avg_begin)");
+    CK(cudaStreamSynchronize(d.stream));
+    for (int q = 0; q < les::NAVG; q++) {
+        if (!sums[q]) return LESGPU_EINVAL;
+        CK(cudaMemcpy(d.avg + (size_t)q * d.n, sums[q], d.n * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    CK(cudaMemcpy((char*)d.dS + offsetof(les::Scalars, avg_steps), &count, sizeof(int), cudaMemcpyHostToDevice));
     return LESGPU_OK;
 }
 

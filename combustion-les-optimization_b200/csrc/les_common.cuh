@@ -150,6 +150,15 @@ struct Scalars {
     double umax_used;                   // |u|max that produced dt (after the inlet fallback)
     int t_loop;                         // reference time-step index of the step being computed
     int run_step;                       // index of the step within the current device-loop run
+    int avg_steps;                      // steps summed into the time averages (time_avg_steps)
+    int pad1;
+};
+
+// Running sums of update_time_averages (les_combustion_solver.c:3166-3191), in the order of
+// stats_backup.bin (:3740-3754): u v w uu vv ww uv uw vw G.
+constexpr int NAVG = 10;
+struct AvgBuf {
+    double* p[NAVG];
 };
 
 // rand() stream state of the device-resident loop (les_devloop.cuh).

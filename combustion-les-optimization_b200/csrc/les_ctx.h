@@ -100,6 +100,9 @@ struct DevCtx {
     cudaGraphExec_t graph = nullptr;    // one captured device-loop step
     bool graph_ok = false;
     int shape[NSH_CLASSES] = {0, 0, 0, 0, 0};   // tile (index into kShapes) per kernel class
+    // time averages (lesgpu_avg_*): NAVG running sums, FP64, in one allocation
+    double* avg = nullptr;
+    int avg_start = 0;
     // kernel timing: event pairs recorded around each kernel class during a step
     bool timing = false;
     std::vector<cudaEvent_t> ev_pool;

@@ -1281,6 +1281,28 @@ __global__ void __launch_bounds__(NT) k_loop_monitor(LES_KERNEL_CONSTS, F11<R> S
     }
 }
 
+// update_time_averages (:3166-3191) after the boundary conditions of steps with
+// t_loop >= start (:4577-4579): first and second moments summed per cell in FP64.
+template <typename RS, typename Form = RS>
+__global__ void __launch_bounds__(NT) k_time_avg(F11<RS> S, AvgBuf A, Scalars* __restrict__ Sc, size_t n, int start) {
+    if (Sc->t_loop < start) return;            // uniform across the grid
+    for (size_t id = (size_t)blockIdx.x * NT + threadIdx.x; id < n; id += (size_t)gridDim.x * NT) {
+        const double u = (double)S.p[0][id], v = (double)S.p[1][id], w = (double)S.p[2][id];
+        const double G = (double)S.p[4][id];
+        A.p[0][id] += u;
+        A.p[1][id] += v;
+        A.p[2][id] += w;
+        A.p[9][id] += G;
+        A.p[3][id] += u * u;
+        A.p[4][id] += v * v;
+        A.p[5][id] += w * w;
+        A.p[6][id] += u * v;
+        A.p[7][id] += u * w;
+        A.p[8][id] += v * w;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) Sc->avg_steps += 1;
+}
+
 // Device loop, last launch of a step: advance the step counters.
 static __global__ void k_loop_tick(Scalars* __restrict__ Sc) {
     Sc->t_loop += 1;

@@ -127,6 +127,11 @@ cudaError_t step_impl(DevCtx& c, double dt, int t_loop, bool device_mode) {
         }
         k_bc_eos<RS, R><<<gE, bE, 0, st>>>(c.hC, c.attr, S, c.part, c.dS);
     }
+    if (c.avg) {
+        AvgBuf A;
+        for (int q = 0; q < NAVG; q++) A.p[q] = c.avg + (size_t)q * c.n;
+        k_time_avg<RS, R><<<MON_BLOCKS, NT, 0, st>>>(S, A, c.dS, c.n, c.avg_start);
+    }
     if (device_mode) {
         const int tpb = 64;
         k_loop_post<RS, R><<<dim3((c.ny + tpb - 1) / tpb, c.loop_nst > 0 ? c.loop_nst : 1), tpb, 0, st>>>(

@@ -53,6 +53,8 @@ static double rng01(les_rng* g) { return (double)les_rng_next(g) / (double)LES_R
 
 /* ------------------------------------------------------------------ solver object */
 
+#define LES_MAX_LINES 16      /* probe stations + measurement-point stations */
+
 struct les_solver {
     lesgpu_config cfg;
     lesgpu_species sp;
@@ -71,10 +73,16 @@ struct les_solver {
     char out_dir[1024];
     int out_flags;
     int probe_i[7];
-    double* probe_buf;
+    double* probe_buf;    /* LES_MAX_LINES lines of NY x 6 */
+    /* measurement points of setup_measurement_points (:3780-3822) and their buffers */
+    int npt;
+    int pt_i[4], pt_j[4], pt_line[4], pt_count[4];
+    double* pt_buf[4];    /* PT_MAX x {u, v, w, G} */
+    /* time averages (lesgpu_avg_*) */
+    int avg_on, avg_start;
     /* device-loop session (les_solver_loop_*) */
-    int loop_on, l_chunk, l_m;
-    int l_st[7], l_slot[7];
+    int loop_on, l_chunk, l_m, l_lines;
+    int l_st[LES_MAX_LINES], l_slot[LES_MAX_LINES];
     double *l_dt, *l_umax, *l_mon, *l_probe;
     char err[256];
 };
@@ -85,6 +93,7 @@ static int serr(les_solver* s, int code, const char* msg) {
 }
 
 static const double PROBE_X[7] = {0.010, 0.015, 0.020, 0.025, 0.030, 0.035, 0.040};   /* :274 */
+#define PT_MAX 50000          /* MAX_DATA_POINTS (:199) */
 
 /* initialize_vortices (:861-897): three discarded test draws, then 7 draws per vortex. */
 void les_vortices_init(les_rng* g, const lesgpu_config* c, double* vort) {
@@ -285,7 +294,7 @@ int les_solver_create(const lesgpu_config* cfg, const char* chem_path, const cha
     s->attr = (int*)malloc(s->n * sizeof(int));
     s->vort = (double*)calloc(cfg->num_vortices > 0 ? (size_t)cfg->num_vortices * 7 : 7, sizeof(double));
     s->noise = (double*)calloc(3 * (size_t)s->ny * s->nz, sizeof(double));
-    s->probe_buf = (double*)malloc(7 * (size_t)s->ny * 6 * sizeof(double));
+    s->probe_buf = (double*)malloc(LES_MAX_LINES * (size_t)s->ny * 6 * sizeof(double));
     if (!s->attr || !s->vort || !s->noise || !s->probe_buf) {
         les_solver_destroy(s);
         return LESGPU_ENOMEM;
@@ -306,16 +315,32 @@ int les_solver_create(const lesgpu_config* cfg, const char* chem_path, const cha
     les_rng_seed(&s->rng, cfg->seed);
     les_vortices_init(&s->rng, cfg, s->vort);
     for (int q = 0; q < 7; q++) s->probe_i[q] = (int)(PROBE_X[q] / s->dx);
+    /* setup_measurement_points (:3780-3822): at 4D and 8D downstream (D = 2 x inlet radius),
+     * on the axis (j = 0) and in the shear layer (j = R / DY), k = NZ/2 */
+    {
+        const int j_shear = (int)(cfg->inlet_radius / s->dy);
+        const int i_locs[2] = {(int)((4.0 * cfg->inlet_radius) / s->dx), (int)((8.0 * cfg->inlet_radius) / s->dx)};
+        s->npt = 0;
+        for (int q = 0; q < 2; q++) {
+            if (i_locs[q] >= s->nx) continue;
+            s->pt_i[s->npt] = i_locs[q]; s->pt_j[s->npt] = 0; s->npt++;
+            s->pt_i[s->npt] = i_locs[q]; s->pt_j[s->npt] = j_shear; s->npt++;
+        }
+    }
     s->t_loop = start_step;
     *out = s;
     return LESGPU_OK;
 }
 
+static void flush_points(les_solver* s);
+
 void les_solver_destroy(les_solver* s) {
     if (!s) return;
     if (s->loop_on) les_solver_loop_end(s);
+    flush_points(s);
     if (s->ctx) lesgpu_destroy(s->ctx);
     free(s->attr); free(s->vort); free(s->noise); free(s->probe_buf);
+    for (int q = 0; q < 4; q++) free(s->pt_buf[q]);
     free(s);
 }
 
@@ -409,13 +434,66 @@ static void append_probe_rows(les_solver* s, int t_loop, const double* lines, in
     }
 }
 
-static int write_probes(les_solver* s, int t_loop) {
-    int st[7], slot[7];
+/* The lines read back each step: the m probe stations first, then one line per distinct
+ * measurement-point station (pt_line maps each point to its line).  Returns the count. */
+static int line_stations(les_solver* s, int* st, int* slot, int* m_out) {
     int m = probe_stations(s, st, slot);
-    if (m == 0) return LESGPU_OK;
-    int rc = lesgpu_probe_lines(s->ctx, st, m, s->nz / 2, s->probe_buf);
+    int L = m;
+    for (int p = 0; p < s->npt; p++) {
+        int found = -1;
+        for (int q = m; q < L; q++)
+            if (st[q] == s->pt_i[p]) found = q;
+        if (found < 0 && L < LES_MAX_LINES) { st[L] = s->pt_i[p]; slot[L] = -1; found = L++; }
+        s->pt_line[p] = found;
+    }
+    *m_out = m;
+    return L;
+}
+
+/* flush_point_data (:3824-3850): append the buffered rows, then empty the buffers. */
+static void flush_points(les_solver* s) {
+    if (!(s->out_flags & LES_OUT_POINTS) || !s->out_dir[0]) return;
+    for (int p = 0; p < s->npt; p++) {
+        if (s->pt_count[p] == 0 || !s->pt_buf[p]) continue;
+        char name[160], path[1300];
+        snprintf(name, sizeof(name), "LES_point_data_phi%.2f_i%d_j%d_k%d.csv", s->cfg.equivalence_ratio, s->pt_i[p],
+                 s->pt_j[p], s->nz / 2);
+        join_path(path, sizeof(path), s->out_dir, name);
+        FILE* fp = fopen(path, "a");
+        if (!fp) continue;
+        fseek(fp, 0, SEEK_END);
+        if (ftell(fp) == 0) fprintf(fp, "u,v,w,G\n");
+        const double* b = s->pt_buf[p];
+        for (int q = 0; q < s->pt_count[p]; q++)
+            fprintf(fp, "%.6f,%.6f,%.6f,%.6f\n", b[4 * q], b[4 * q + 1], b[4 * q + 2], b[4 * q + 3]);
+        fclose(fp);
+        s->pt_count[p] = 0;
+    }
+}
+
+/* The point buffer of the time loop (:4557-4568): u, v, w, G of every point after the BC. */
+static void record_points(les_solver* s, const double* lines) {
+    for (int p = 0; p < s->npt; p++) {
+        if (s->pt_line[p] < 0 || s->pt_count[p] >= PT_MAX) continue;
+        if (!s->pt_buf[p]) {
+            s->pt_buf[p] = (double*)malloc((size_t)PT_MAX * 4 * sizeof(double));
+            if (!s->pt_buf[p]) continue;
+        }
+        const double* r = lines + ((size_t)s->pt_line[p] * s->ny + s->pt_j[p]) * 6;
+        double* b = s->pt_buf[p] + 4 * (size_t)s->pt_count[p];
+        b[0] = r[0]; b[1] = r[1]; b[2] = r[2]; b[3] = r[3];
+        s->pt_count[p]++;
+    }
+}
+
+static int write_probes(les_solver* s, int t_loop) {
+    int st[LES_MAX_LINES], slot[LES_MAX_LINES], m;
+    int L = line_stations(s, st, slot, &m);
+    if (L == 0) return LESGPU_OK;
+    int rc = lesgpu_probe_lines(s->ctx, st, L, s->nz / 2, s->probe_buf);
     if (rc) return rc;
-    append_probe_rows(s, t_loop, s->probe_buf, m, slot);
+    if ((s->out_flags & LES_OUT_PROBES) && m > 0) append_probe_rows(s, t_loop, s->probe_buf, m, slot);
+    if (s->out_flags & LES_OUT_POINTS) record_points(s, s->probe_buf);
     return LESGPU_OK;
 }
 
@@ -440,6 +518,25 @@ static int write_monitor(les_solver* s, int step, double dt) {
     return LESGPU_OK;
 }
 
+/* The checkpoint block of the time loop (:4583-4589) at t > 0, t % 50 == 0:
+ * checkpoint.bin + restart_info.txt, stats_backup.bin (time averages on), point data. */
+static int checkpoint_step(les_solver* s, int t) {
+    if (!(t > 0 && t % 50 == 0) || !s->out_dir[0]) return LESGPU_OK;
+    if (s->out_flags & LES_OUT_CHECKPOINT) {
+        char path[1200];
+        join_path(path, sizeof(path), s->out_dir, "checkpoint.bin");
+        int rc = les_solver_save_checkpoint(s, path, t);
+        if (rc) return rc;
+        if (s->avg_on) {
+            join_path(path, sizeof(path), s->out_dir, "stats_backup.bin");
+            rc = les_solver_save_stats(s, path);
+            if (rc) return rc;
+        }
+    }
+    flush_points(s);
+    return LESGPU_OK;
+}
+
 int les_solver_step(les_solver* s) {
     if (!s) return LESGPU_EINVAL;
     if (s->loop_on) return serr(s, LESGPU_ESTATE, "end the device loop before host-driven steps");
@@ -457,16 +554,12 @@ int les_solver_step(les_solver* s) {
     rc = lesgpu_set_inflow(s->ctx, s->vort, c->num_vortices, s->noise);
     if (rc == LESGPU_OK) rc = lesgpu_step(s->ctx, dt, s->t_loop);
     if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
-    if ((s->out_flags & LES_OUT_PROBES) && s->out_dir[0]) {
+    if ((s->out_flags & (LES_OUT_PROBES | LES_OUT_POINTS)) && s->out_dir[0]) {
         rc = write_probes(s, s->t_loop);
         if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
     }
-    if ((s->out_flags & LES_OUT_CHECKPOINT) && s->out_dir[0] && s->t_loop > 0 && s->t_loop % 50 == 0) {
-        char path[1200];
-        join_path(path, sizeof(path), s->out_dir, "checkpoint.bin");
-        rc = les_solver_save_checkpoint(s, path, s->t_loop);
-        if (rc) return rc;
-    }
+    rc = checkpoint_step(s, s->t_loop);
+    if (rc) return rc;
     if ((s->out_flags & LES_OUT_MONITOR) && s->out_dir[0]) {
         rc = write_monitor(s, s->t_loop, dt);
         if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
@@ -491,14 +584,14 @@ int les_solver_loop_begin(les_solver* s, int chunk) {
     for (int j = 0; j < 31; j++) win[j] = (unsigned int)s->rng.r[(s->rng.f + j) % 31];
     int rc = lesgpu_loop_begin(s->ctx, win, s->vort, s->cfg.num_vortices, s->t_loop);
     if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
-    s->l_m = probe_stations(s, s->l_st, s->l_slot);
-    rc = lesgpu_loop_config(s->ctx, s->l_st, s->l_m, s->nz / 2, chunk);
+    s->l_lines = line_stations(s, s->l_st, s->l_slot, &s->l_m);
+    rc = lesgpu_loop_config(s->ctx, s->l_st, s->l_lines, s->nz / 2, chunk);
     if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
     s->l_chunk = chunk;
     s->l_dt = (double*)malloc((size_t)chunk * sizeof(double));
     s->l_umax = (double*)malloc((size_t)chunk * sizeof(double));
     s->l_mon = (double*)malloc((size_t)chunk * 6 * sizeof(double));
-    s->l_probe = (double*)malloc((size_t)chunk * (s->l_m > 0 ? s->l_m : 1) * s->ny * 6 * sizeof(double));
+    s->l_probe = (double*)malloc((size_t)chunk * (s->l_lines > 0 ? s->l_lines : 1) * s->ny * 6 * sizeof(double));
     if (!s->l_dt || !s->l_umax || !s->l_mon || !s->l_probe) {
         loop_free(s);
         return serr(s, LESGPU_ENOMEM, "host history buffers");
@@ -530,26 +623,38 @@ int les_solver_loop_collect(les_solver* s, int n) {
     if (n > s->l_chunk) return serr(s, LESGPU_EINVAL, "more steps than the history holds");
     if (n == 0) return LESGPU_OK;
     const int want_probes = (s->out_flags & LES_OUT_PROBES) && s->out_dir[0];
+    const int want_points = (s->out_flags & LES_OUT_POINTS) && s->out_dir[0];
     const int want_mon = (s->out_flags & LES_OUT_MONITOR) && s->out_dir[0];
-    const int want_ckpt = (s->out_flags & LES_OUT_CHECKPOINT) && s->out_dir[0];
-    const int m = s->l_m;
-    int rc = lesgpu_loop_history(s->ctx, n, s->l_dt, s->l_umax, want_probes ? s->l_probe : NULL,
+    const int m = s->l_m, L = s->l_lines;
+    int rc = lesgpu_loop_history(s->ctx, n, s->l_dt, s->l_umax, (want_probes || want_points) ? s->l_probe : NULL,
                                  want_mon ? s->l_mon : NULL);
     if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
     for (int q = 0; q < n; q++) {
         const int t = s->t_loop + q;
-        if (want_probes && m > 0) append_probe_rows(s, t, s->l_probe + (size_t)q * m * s->ny * 6, m, s->l_slot);
+        const double* lines = s->l_probe + (size_t)q * L * s->ny * 6;
+        if (want_probes && m > 0) append_probe_rows(s, t, lines, m, s->l_slot);
+        if (want_points) {
+            record_points(s, lines);
+            if (t > 0 && t % 50 == 0) flush_points(s);
+        }
         if (want_mon && t % 10 == 0) append_monitor_row(s, t, s->l_dt[q], s->l_mon + 6 * (size_t)q);
     }
     s->dt = s->l_dt[n - 1];
     s->umax = s->l_umax[n - 1];
     s->t_loop += n;
+    /* checkpoint.bin and stats_backup.bin need the state of their step: les_solver_next_chunk
+     * ends every chunk on a checkpoint step when checkpoints are written */
     const int tl = s->t_loop - 1;
-    if (want_ckpt && tl > 0 && tl % 50 == 0) {
+    if ((s->out_flags & LES_OUT_CHECKPOINT) && s->out_dir[0] && tl > 0 && tl % 50 == 0) {
         char path[1200];
         join_path(path, sizeof(path), s->out_dir, "checkpoint.bin");
         rc = les_solver_save_checkpoint(s, path, tl);
         if (rc) return rc;
+        if (s->avg_on) {
+            join_path(path, sizeof(path), s->out_dir, "stats_backup.bin");
+            rc = les_solver_save_stats(s, path);
+            if (rc) return rc;
+        }
     }
     return LESGPU_OK;
 }
@@ -653,5 +758,117 @@ int les_solver_load_checkpoint(les_solver* s, const char* path, int* t_out) {
     free_fields(f);
     if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
     if (t_out) *t_out = t;
+    return LESGPU_OK;
+}
+
+/* ------------------------------------------------------------------ time averages */
+
+int les_solver_set_averaging(les_solver* s, int start_step) {
+    if (!s) return LESGPU_EINVAL;
+    if (s->loop_on) return serr(s, LESGPU_ESTATE, "end the device loop before changing the averaging");
+    int rc;
+    if (start_step < 0) {
+        rc = lesgpu_avg_end(s->ctx);
+        s->avg_on = 0;
+    } else {
+        rc = lesgpu_avg_begin(s->ctx, start_step);
+        s->avg_on = (rc == LESGPU_OK);
+        s->avg_start = start_step;
+    }
+    if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
+    return LESGPU_OK;
+}
+
+static int avg_fields(les_solver* s, double** f) {
+    for (int q = 0; q < 10; q++) {
+        f[q] = (double*)malloc(s->n * sizeof(double));
+        if (!f[q]) {
+            for (int r = 0; r < q; r++) free(f[r]);
+            return LESGPU_ENOMEM;
+        }
+    }
+    return LESGPU_OK;
+}
+
+/* save_statistics_backup (:3736-3756): int time_avg_steps, then the ten sums. */
+int les_solver_save_stats(les_solver* s, const char* path) {
+    if (!s || !path) return LESGPU_EINVAL;
+    if (!s->avg_on) return serr(s, LESGPU_ESTATE, "time averages are not enabled");
+    double* f[10];
+    if (avg_fields(s, f)) return serr(s, LESGPU_ENOMEM, "host buffers");
+    int count = 0;
+    int rc = lesgpu_avg_download(s->ctx, (double* const*)f, &count);
+    if (rc == LESGPU_OK) {
+        FILE* fp = fopen(path, "wb");
+        if (!fp) {
+            rc = serr(s, LESGPU_EIO, "cannot open stats backup for writing");
+        } else {
+            int ok = fwrite(&count, sizeof(int), 1, fp) == 1;
+            for (int q = 0; q < 10 && ok; q++) ok = fwrite(f[q], sizeof(double), s->n, fp) == s->n;
+            fclose(fp);
+            if (!ok) rc = serr(s, LESGPU_EIO, "short stats backup write");
+        }
+    } else {
+        serr(s, rc, lesgpu_last_error(s->ctx));
+    }
+    for (int q = 0; q < 10; q++) free(f[q]);
+    return rc;
+}
+
+/* load_statistics_backup (:3758-3778). */
+int les_solver_load_stats(les_solver* s, const char* path) {
+    if (!s || !path) return LESGPU_EINVAL;
+    if (!s->avg_on) return serr(s, LESGPU_ESTATE, "enable the time averages first");
+    FILE* fp = fopen(path, "rb");
+    if (!fp) return serr(s, LESGPU_EIO, "cannot open stats backup");
+    double* f[10];
+    if (avg_fields(s, f)) { fclose(fp); return serr(s, LESGPU_ENOMEM, "host buffers"); }
+    int count = 0;
+    int ok = fread(&count, sizeof(int), 1, fp) == 1 && count >= 0;
+    for (int q = 0; q < 10 && ok; q++) ok = fread(f[q], sizeof(double), s->n, fp) == s->n;
+    fclose(fp);
+    int rc = ok ? lesgpu_avg_upload(s->ctx, (const double* const*)f, count) : LESGPU_EIO;
+    for (int q = 0; q < 10; q++) free(f[q]);
+    if (!ok) return serr(s, LESGPU_EIO, "truncated or invalid stats backup");
+    if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
+    return LESGPU_OK;
+}
+
+/* calculate_resolved_reynolds_stresses (:3194-3217): <u'u'>, <v'v'>, <w'w'>, <u'v'>, <u'w'>,
+ * <v'w'> and the mean G, from the sums and time_avg_steps (left unchanged here; the
+ * reference divides G_mean in place). */
+int les_solver_reynolds_stresses(les_solver* s, double* const* out, int* count) {
+    if (!s || !out) return LESGPU_EINVAL;
+    for (int q = 0; q < 7; q++)
+        if (!out[q]) return LESGPU_EINVAL;
+    if (!s->avg_on) return serr(s, LESGPU_ESTATE, "time averages are not enabled");
+    double* f[10];
+    if (avg_fields(s, f)) return serr(s, LESGPU_ENOMEM, "host buffers");
+    int n = 0;
+    int rc = lesgpu_avg_download(s->ctx, (double* const*)f, &n);
+    if (rc == LESGPU_OK && n > 0) {
+        for (size_t c = 0; c < s->n; c++) {
+            double au = f[0][c] / n, av = f[1][c] / n, aw = f[2][c] / n;
+            out[0][c] = (f[3][c] / n) - (au * au);
+            out[1][c] = (f[4][c] / n) - (av * av);
+            out[2][c] = (f[5][c] / n) - (aw * aw);
+            out[3][c] = (f[6][c] / n) - (au * av);
+            out[4][c] = (f[7][c] / n) - (au * aw);
+            out[5][c] = (f[8][c] / n) - (av * aw);
+            out[6][c] = f[9][c] / n;
+        }
+    } else if (rc == LESGPU_OK) {
+        for (int q = 0; q < 7; q++) memset(out[q], 0, s->n * sizeof(double));
+    }
+    for (int q = 0; q < 10; q++) free(f[q]);
+    if (count) *count = n;
+    if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
+    return LESGPU_OK;
+}
+
+/* Final output of a run (:4604-4623): the remaining point rows. */
+int les_solver_flush(les_solver* s) {
+    if (!s) return LESGPU_EINVAL;
+    flush_points(s);
     return LESGPU_OK;
 }

@@ -32,7 +32,9 @@ FIELD_IDS.update({name: 100 + q for q, name in enumerate(_INSPECT)})
 ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "EIO", -5: "ESTATE", -6: "ENONFINITE"}
 LESGPU_EINVAL, LESGPU_ECUDA, LESGPU_ENOMEM, LESGPU_EIO, LESGPU_ESTATE, LESGPU_ENONFINITE = -1, -2, -3, -4, -5, -6
 
-LES_OUT_PROBES, LES_OUT_MONITOR, LES_OUT_CHECKPOINT = 1, 2, 4
+LES_OUT_PROBES, LES_OUT_MONITOR, LES_OUT_CHECKPOINT, LES_OUT_POINTS = 1, 2, 4, 8
+AVG_NAMES = ["u", "v", "w", "uu", "vv", "ww", "uv", "uw", "vw", "G"]
+STRESS_NAMES = ["uu", "vv", "ww", "uv", "uw", "vw", "G_mean"]
 
 
 class LesgpuError(RuntimeError):
@@ -145,6 +147,15 @@ def lib():
         _sig(L, "les_solver_loop_run", C.c_int, [vp, C.c_int])
         _sig(L, "les_solver_loop_end", C.c_int, [vp])
         _sig(L, "les_solver_next_chunk", C.c_int, [vp, C.c_int])
+        _sig(L, "les_solver_set_averaging", C.c_int, [vp, C.c_int])
+        _sig(L, "les_solver_save_stats", C.c_int, [vp, C.c_char_p])
+        _sig(L, "les_solver_load_stats", C.c_int, [vp, C.c_char_p])
+        _sig(L, "les_solver_reynolds_stresses", C.c_int, [vp, vp, C.POINTER(C.c_int)])
+        _sig(L, "les_solver_flush", C.c_int, [vp])
+        _sig(L, "lesgpu_avg_begin", C.c_int, [vp, C.c_int])
+        _sig(L, "lesgpu_avg_end", C.c_int, [vp])
+        _sig(L, "lesgpu_avg_download", C.c_int, [vp, vp, C.POINTER(C.c_int)])
+        _sig(L, "lesgpu_avg_upload", C.c_int, [vp, vp, C.c_int])
         _sig(L, "les_solver_loop_collect", C.c_int, [vp, C.c_int])
         _sig(L, "lesgpu_autotune", C.c_int, [vp, C.c_int, vp, dp])
         _sig(L, "lesgpu_set_tiles", C.c_int, [vp, vp])
@@ -428,6 +439,36 @@ class Solver:
 
     def loop_begin(self, chunk: int = 64):
         self._check(lib().les_solver_loop_begin(self._h, chunk), "loop_begin")
+
+    def set_averaging(self, start_step: int):
+        """Sum the time averages from t_loop >= start_step on (< 0: off)."""
+        self._check(lib().les_solver_set_averaging(self._h, start_step), "set_averaging")
+
+    def save_stats(self, path: str):
+        self._check(lib().les_solver_save_stats(self._h, path.encode()), "save_stats")
+
+    def load_stats(self, path: str):
+        self._check(lib().les_solver_load_stats(self._h, path.encode()), "load_stats")
+
+    def average_sums(self):
+        """The ten running sums (AVG_NAMES) and the number of steps summed."""
+        out = {k: np.empty(self.shape) for k in AVG_NAMES}
+        ptrs = (C.c_void_p * 10)(*[out[k].ctypes.data for k in AVG_NAMES])
+        n = C.c_int(0)
+        rc = lib().lesgpu_avg_download(self.ctx._h, ptrs, C.byref(n))
+        if rc:
+            raise LesgpuError(rc, "lesgpu_avg_download failed")
+        return out, n.value
+
+    def reynolds_stresses(self):
+        out = {k: np.empty(self.shape) for k in STRESS_NAMES}
+        ptrs = (C.c_void_p * 7)(*[out[k].ctypes.data for k in STRESS_NAMES])
+        n = C.c_int(0)
+        self._check(lib().les_solver_reynolds_stresses(self._h, ptrs, C.byref(n)), "reynolds_stresses")
+        return out, n.value
+
+    def flush(self):
+        self._check(lib().les_solver_flush(self._h), "flush")
 
     def loop_run(self, n: int):
         self._check(lib().les_solver_loop_run(self._h, n), "loop_run")

@@ -227,6 +227,18 @@ int lesgpu_kernel_times(lesgpu_ctx* ctx, double* ms, long long* launches, int n)
 int lesgpu_selfcheck_division(const double* divisors, int nd, size_t n, unsigned long long seed,
                               unsigned long long* mismatches);
 
+/* Time averages: update_time_averages (:3166-3191) on the device.  lesgpu_avg_begin allocates
+ * ten FP64 running sums per cell (zeroed) and from then on every step -- host-driven or
+ * device loop -- adds the state after its boundary conditions to them when its t_loop is
+ * >= start_step (the reference's start_avg_step, :4382, :4577).  The sums are in the order
+ * of stats_backup.bin (:3740-3754): u, v, w, u*u, v*v, w*w, u*v, u*w, v*w, G; `count` is the
+ * number of steps summed (time_avg_steps).  download/upload move the sums and the count
+ * (save_statistics_backup / load_statistics_backup, :3736-3778). */
+int lesgpu_avg_begin(lesgpu_ctx* ctx, int start_step);
+int lesgpu_avg_end(lesgpu_ctx* ctx);
+int lesgpu_avg_download(lesgpu_ctx* ctx, double* const* sums, int* count);
+int lesgpu_avg_upload(lesgpu_ctx* ctx, const double* const* sums, int count);
+
 /* Thread-block tiles of the per-cell kernels (no reference counterpart; the reference is
  * serial C).  tiles[c] for the classes {filter, strain, rhs_flow, rhs_scalar, eos} indexes
  * the shapes 0 = 32x8, 1 = 64x4, 2 = 16x16, 3 = 128x2 (k extent x j extent, 256 threads).

@@ -45,7 +45,12 @@ typedef struct les_solver les_solver;
 /* Output switches for les_solver_set_outputs. */
 #define LES_OUT_PROBES 1       /* probe_data_flame_region_loc*.csv every step (:4572-4574) */
 #define LES_OUT_MONITOR 2      /* simulation_monitor.csv every 10 steps (:4592) */
-#define LES_OUT_CHECKPOINT 4   /* checkpoint.bin + restart_info.txt every 50 steps (:4583-4589) */
+#define LES_OUT_CHECKPOINT 4   /* checkpoint.bin + restart_info.txt every 50 steps (:4583-4589), with
+                                  stats_backup.bin when time averages are on */
+#define LES_OUT_POINTS 8       /* LES_point_data_phi*_i*_j*_k*.csv: the point time series
+                                  (:4557-4568, flush_point_data :3824-3850) at 4D and 8D, on the
+                                  axis and in the shear layer (:3780-3822), flushed every 50 steps,
+                                  by les_solver_flush and when the solver is destroyed */
 
 /* Load the species files, create the GPU context, build the attribute map and the initial
  * state exactly as initialize()+setting() (:1085-1285), seed rand() and place the SEM
@@ -93,6 +98,19 @@ int les_solver_attribute(const les_solver* s, int* out);
  * load also restores rho*u momentum as load_quick_checkpoint does (:3716-3726). */
 int les_solver_save_checkpoint(les_solver* s, const char* path, int t);
 int les_solver_load_checkpoint(les_solver* s, const char* path, int* t_out);
+
+/* Time averages (update_time_averages, :3166-3191) summed on the device from the step whose
+ * t_loop reaches start_step (the reference's start_avg_step); start_step < 0 turns them off.
+ * save/load: stats_backup.bin (:3736-3778); reynolds_stresses: the seven fields of
+ * calculate_resolved_reynolds_stresses (:3194-3217) -- uu, vv, ww, uv, uw, vw, mean G -- each
+ * NX*NY*NZ, and the number of steps summed. */
+int les_solver_set_averaging(les_solver* s, int start_step);
+int les_solver_save_stats(les_solver* s, const char* path);
+int les_solver_load_stats(les_solver* s, const char* path);
+int les_solver_reynolds_stresses(les_solver* s, double* const* out, int* count);
+/* Write what the end of the reference's run writes and the library still buffers (the point
+ * rows). */
+int les_solver_flush(les_solver* s);
 
 /* Vortex table (nv x 7) and rand() draw count, for inspection. */
 int les_solver_vortices(const les_solver* s, double* out);
