@@ -5,6 +5,9 @@ Writes a seeded synthetic probe file in the solver's CSV layout, then runs on it
   * bayesian_optimizer.load_and_compute_reynolds_stress (returns the G-binned <u'v'>),
   * analysis.task_1_3_flame_profile and analysis.task_1_6_reynolds_stress_vs_g_binned,
     whose profiles are the arguments they hand to the plotting calls;
+and, for the optimiser, bayesian_optimizer's experimental_reynolds_stress, smooth_profile,
+compute_score (on seeded profiles) and BayesianOptimizer._acquisition / suggest_next (on a
+seeded history, with numpy's global generator seeded before each call);
 with stand-in matplotlib / seaborn modules that record those plotting calls (neither
 library is installed here).  The reference modules are imported from their source tree,
 unmodified.  Output: ``tests/golden/stats_ref.npz`` holding the probe file's text
@@ -127,6 +130,37 @@ def main():
     names = ["uu_cond", "vv_cond", "uv_cond"]
     for q, (tag, (x, y), label) in enumerate(Recorder.calls):
         out[f"stress_vs_G.{names[q]}.x"], out[f"stress_vs_G.{names[q]}.y"] = x, y
+    # ---- optimiser pieces
+    rng = np.random.default_rng(11)
+    g = np.linspace(0.0, 1.0, 41)
+    out["exp_G"], out["exp_val"] = g, bo.experimental_reynolds_stress(g)
+    profiles = []
+    for q in range(6):
+        centers = 0.5 * (np.linspace(0, 1, 21)[:-1] + np.linspace(0, 1, 21)[1:])
+        val = 0.02 * np.exp(-(3 + 5 * q) * centers) + 0.002 * rng.standard_normal(20)
+        val[rng.random(20) < 0.15 * q] = np.nan
+        profiles.append(val)
+    out["prof_G"] = centers
+    out["prof_val"] = np.array(profiles)
+    out["prof_score"] = np.array([bo.compute_score(centers, p) for p in profiles])
+    sm = [bo.smooth_profile(centers[~np.isnan(p)], p[~np.isnan(p)]) for p in profiles[:3]]
+    out["smooth_G"] = np.array([a for a, b in sm])
+    out["smooth_val"] = np.array([b for a, b in sm])
+    out["uv_score"] = np.array([bo.compute_score(out["uv_G_centers"], out["uv_stress"])])
+    with tempfile.TemporaryDirectory() as d:
+        opt = bo.BayesianOptimizer(history_file=os.path.join(d, "h.json"))
+        lo, hi = opt.bounds[:, 0], opt.bounds[:, 1]
+        X = rng.uniform(lo, hi, size=(12, 6))
+        y = np.array([float(np.sum(((x - lo) / (hi - lo) - 0.4) ** 2)) for x in X])
+        opt.X_obs, opt.y_obs = [list(map(float, x)) for x in X], list(map(float, y))
+        np.random.seed(5)
+        Xc = np.random.uniform(lo, hi, size=(300, 6))
+        np.random.seed(6)
+        out["ei"] = opt._acquisition(Xc)
+        out["ei_X"], out["ei_y"], out["ei_cand"] = X, y, Xc
+        np.random.seed(9)
+        nxt = opt.suggest_next(n_candidates=500)
+        out["next"] = np.array([nxt[k] for k in opt.param_names])
     np.savez_compressed(os.path.join(HERE, "stats_ref.npz"), **out)
     print(sorted(out))
 

@@ -148,3 +148,19 @@ def test_group_requires_loop_sessions(N):
     assert L.lesgpu_group_create(dup, 2, C.byref(g)) == N.LESGPU_EINVAL
     s.loop_end()
     s.close()
+
+
+def test_optimisation_campaign_on_ensembles(N, tmp_path):
+    """Two rounds of three proposals, each round one ensemble; every trial is scored from its
+    own probe file and registered."""
+    from lesgpu.config import preset
+    from lesgpu.optimizer import run_campaign
+    opt = run_campaign(preset("small", seed=4), rounds=2, batch=3, steps=25, precision=N.FP32,
+                       workdir=str(tmp_path), seed=1, log=lambda *_: None)
+    assert len(opt.y_obs) == 6
+    assert all(np.isfinite(opt.y_obs))
+    assert os.path.exists(tmp_path / "optimization_history.json")
+    trials = sorted(p for p in os.listdir(tmp_path) if p.startswith("round"))
+    assert len(trials) == 6
+    for t in trials:
+        assert os.path.exists(tmp_path / t / "probe_data_flame_region_loc0.csv")
