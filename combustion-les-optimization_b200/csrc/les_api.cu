@@ -409,7 +409,7 @@ void lesgpu_destroy(lesgpu_ctx* ctx) {
     DevCtx& d = ctx->d;
     if (d.stream) cudaStreamSynchronize(d.stream);
     void* bufs[] = {d.arena, d.attr, d.dC, d.dS, d.part, d.plane, d.noise, d.vort, d.inlet_list, d.inlet_pos,
-                    d.probe_st, d.probe_out, d.flag, d.dbg_cp, d.dbg_lam, d.dbg_alpha, d.avg};
+                    d.probe_st, d.probe_out, d.flag, d.dbg_cp, d.dbg_lam, d.dbg_alpha, d.avg, d.grad_g};
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (int q = 0; q < les::NACC; q++)
@@ -559,6 +559,10 @@ int lesgpu_get_field(lesgpu_ctx* ctx, int id, double* out) {
     if (id >= LESGPU_F_U && id <= LESGPU_F_Y4) src = d.S[id];
     else if (id == LESGPU_F_NU_T) src = d.nu_t;
     else if (id == LESGPU_F_S_MAG) src = d.S_mag;
+    else if (id == LESGPU_F_GRAD_G) {
+        if (!d.grad_g) return fail(ctx, LESGPU_ESTATE, "enable lesgpu_keep_grad_g before the step to read this field");
+        src = d.grad_g;
+    }
     else if (id >= LESGPU_F_U_F && id <= LESGPU_F_Y4_F) src = d.F[id - LESGPU_F_U_F];
     else if (id == LESGPU_F_NU) src = d.nu;
     else if (id == LESGPU_F_MU_MIX) src = d.mu_mix;
@@ -954,6 +958,24 @@ int lesgpu_autotune(lesgpu_ctx* ctx, int reps, int tiles_out[5], double* ms_out)
     if (ms_out)
         for (int c = 0; c < 4; c++)
             for (int t = 0; t < les::NSHAPES; t++) ms_out[c * les::NSHAPES + t] = ms[c][t];
+    return LESGPU_OK;
+}
+
+int lesgpu_keep_grad_g(lesgpu_ctx* ctx, int enable) {
+    if (!ctx) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    CK(cudaStreamSynchronize(d.stream));
+    if (enable && !d.grad_g) {
+        const size_t bytes = d.n * d.esz;
+        CK(cudaMalloc(&d.grad_g, bytes));
+        CK(cudaMemset(d.grad_g, 0, bytes));   // non-fluid cells stay 0, as in the reference (:2820)
+        d.total_bytes += bytes;
+    } else if (!enable && d.grad_g) {
+        cudaFree(d.grad_g);
+        d.grad_g = nullptr;
+        d.total_bytes -= d.n * d.esz;
+    }
+    drop_graph(d);
     return LESGPU_OK;
 }
 

@@ -60,6 +60,7 @@ struct DevCtx {
     void* dbg_lam = nullptr;
     void* dbg_alpha = nullptr;
     void* kd[NACC] = {};
+    void* grad_g = nullptr;             // optional |grad G| field (lesgpu_keep_grad_g)
     bool debug = false;
     double* part = nullptr;             // per-block partials of the reductions
     size_t part_len = 0;

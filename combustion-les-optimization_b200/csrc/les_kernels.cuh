@@ -42,6 +42,7 @@ struct PropBuf {
     R* dbg_cp;               // optional (nullptr): Cp, lambda, alpha for inspection
     R* dbg_lam;
     R* dbg_alpha;
+    R* grad_g;               // optional (nullptr): |grad G| of the last RHS evaluation
 };
 template <typename R>
 struct AccBuf {              // RK4 running sum of k: rhou rhov rhow T G Y0..Y4
@@ -743,6 +744,7 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::flow)
             gz = cdv(Gf[1] - Gf[-1], K.d_2dz);
         }
         R gmag = qsqrt(gx * gx + gy * gy + gz * gz);
+        if (P.grad_g) P.grad_g[id] = gmag;   // grad_G_magnitude_for_debug (:2783)
         R prop = P.ST[id] * gmag;
         R art = R(0);
         if (C.flame_accel) {

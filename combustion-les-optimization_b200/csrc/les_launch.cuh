@@ -31,6 +31,7 @@ static PropBuf<R> props(const DevCtx& c) {
     P.dbg_cp = c.debug ? (R*)c.dbg_cp : nullptr;
     P.dbg_lam = c.debug ? (R*)c.dbg_lam : nullptr;
     P.dbg_alpha = c.debug ? (R*)c.dbg_alpha : nullptr;
+    P.grad_g = (R*)c.grad_g;
     return P;
 }
 

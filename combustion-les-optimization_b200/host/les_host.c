@@ -367,8 +367,16 @@ static void join_path(char* dst, size_t cap, const char* dir, const char* name) 
     snprintf(dst, cap, "%s/%s", dir, name);
 }
 
+static int write_vtk_step(les_solver* s, int t);
+
 int les_solver_set_outputs(les_solver* s, const char* dir, int flags) {
     if (!s || (flags && !dir)) return LESGPU_EINVAL;
+    if (s->loop_on && ((flags ^ s->out_flags) & LES_OUT_VTK))
+        return serr(s, LESGPU_ESTATE, "end the device loop before switching VTK output");
+    if ((flags & LES_OUT_VTK) != (s->out_flags & LES_OUT_VTK)) {
+        int rc = lesgpu_keep_grad_g(s->ctx, (flags & LES_OUT_VTK) ? 1 : 0);
+        if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
+    }
     s->out_flags = flags;
     if (!dir) return LESGPU_OK;
     snprintf(s->out_dir, sizeof(s->out_dir), "%s", dir);
@@ -564,6 +572,10 @@ int les_solver_step(les_solver* s) {
         rc = write_monitor(s, s->t_loop, dt);
         if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
     }
+    if (s->t_loop > 0 && s->t_loop % 500 == 0) {
+        rc = write_vtk_step(s, s->t_loop);
+        if (rc) return rc;
+    }
     s->t_loop++;
     return LESGPU_OK;
 }
@@ -606,10 +618,12 @@ int les_solver_loop_begin(les_solver* s, int chunk) {
 int les_solver_next_chunk(const les_solver* s, int left) {
     if (!s || left <= 0 || !s->loop_on) return 0;
     int n = left < s->l_chunk ? left : s->l_chunk;
-    if ((s->out_flags & LES_OUT_CHECKPOINT) && s->out_dir[0]) {
+    const int ck = (s->out_flags & LES_OUT_CHECKPOINT) && s->out_dir[0];
+    const int vtk = (s->out_flags & LES_OUT_VTK) && s->out_dir[0];
+    if (ck || vtk) {
         for (int q = 0; q < n; q++) {
             int t = s->t_loop + q;
-            if (t > 0 && t % 50 == 0) { n = q + 1; break; }
+            if ((ck && t > 0 && t % 50 == 0) || (vtk && t > 0 && t % 500 == 0)) { n = q + 1; break; }
         }
     }
     return n;
@@ -655,6 +669,10 @@ int les_solver_loop_collect(les_solver* s, int n) {
             rc = les_solver_save_stats(s, path);
             if (rc) return rc;
         }
+    }
+    if (tl > 0 && tl % 500 == 0) {
+        rc = write_vtk_step(s, tl);
+        if (rc) return rc;
     }
     return LESGPU_OK;
 }
@@ -866,9 +884,109 @@ int les_solver_reynolds_stresses(les_solver* s, double* const* out, int* count) 
     return LESGPU_OK;
 }
 
-/* Final output of a run (:4604-4623): the remaining point rows. */
+/* Final output of a run (:4604-4623): the VTK file of the last step (when VTK output is on)
+ * and the remaining point rows. */
 int les_solver_flush(les_solver* s) {
     if (!s) return LESGPU_EINVAL;
+    if (s->loop_on) return serr(s, LESGPU_ESTATE, "end the device loop first");
+    int rc = write_vtk_step(s, s->t_loop);
     flush_points(s);
+    return rc;
+}
+
+/* ------------------------------------------------------------------ VTK */
+
+/* output_vtk (:3473-3668): legacy ASCII structured grid, points and values in k-j-i order,
+ * non-finite values written as 0.  Fields: velocity, temperature, G, the five mass
+ * fractions, density, omega (never computed by the reference: 0), mu_mix, nu_mix (the
+ * reference's defaults on non-fluid cells), ST_turbulent, nu_t, |grad G| (0 unless
+ * lesgpu_keep_grad_g is on), the six resolved Reynolds stresses and G_mean (0 without time
+ * averages).  The reference divides G_mean by time_avg_steps in place before writing it
+ * (:3215), so with averages on its file carries sum/n^2; here it is sum/n. */
+int les_solver_write_vtk(les_solver* s, const char* path) {
+    if (!s || !path) return LESGPU_EINVAL;
+    const size_t n = s->n;
+    const int nf = 11 + 5 + 10;
+    double* buf = (double*)malloc((size_t)nf * n * sizeof(double));
+    if (!buf) return serr(s, LESGPU_ENOMEM, "host buffers");
+    double* st[11];
+    for (int q = 0; q < 11; q++) st[q] = buf + (size_t)q * n;
+    double* mu = buf + 11 * n; double* nu = buf + 12 * n; double* ST = buf + 13 * n;
+    double* nut = buf + 14 * n; double* gg = buf + 15 * n;
+    double* av[10];
+    for (int q = 0; q < 10; q++) av[q] = buf + (size_t)(16 + q) * n;
+    int rc = lesgpu_download_state(s->ctx, (double* const*)st, 11);
+    if (rc == LESGPU_OK) rc = lesgpu_get_field(s->ctx, LESGPU_F_MU_MIX, mu);
+    if (rc == LESGPU_OK) rc = lesgpu_get_field(s->ctx, LESGPU_F_NU, nu);
+    if (rc == LESGPU_OK) rc = lesgpu_get_field(s->ctx, LESGPU_F_ST, ST);
+    if (rc == LESGPU_OK) rc = lesgpu_get_field(s->ctx, LESGPU_F_NU_T, nut);
+    if (rc == LESGPU_OK && lesgpu_get_field(s->ctx, LESGPU_F_GRAD_G, gg) != LESGPU_OK) memset(gg, 0, n * sizeof(double));
+    int navg = 0;
+    if (rc == LESGPU_OK && s->avg_on) rc = lesgpu_avg_download(s->ctx, (double* const*)av, &navg);
+    if (rc) { free(buf); return serr(s, rc, lesgpu_last_error(s->ctx)); }
+    for (size_t c = 0; c < n; c++)
+        if (s->attr[c] != 3) { mu[c] = 1.8e-5; nu[c] = 1.5e-5; }     /* update_nu_mix defaults (:1556-1561) */
+    FILE* fp = fopen(path, "w");
+    if (!fp) { free(buf); return serr(s, LESGPU_EIO, "cannot open the VTK file"); }
+    static char iobuf[1 << 20];
+    setvbuf(fp, iobuf, _IOFBF, sizeof(iobuf));
+    const int NXv = s->nx, NYv = s->ny, NZv = s->nz;
+#define VTK_LOOP for (int k = 0; k < NZv; k++) for (int j = 0; j < NYv; j++) for (int i = 0; i < NXv; i++)
+#define VTK_ID ((((size_t)i * NYv) + j) * NZv + k)
+#define FIN(x) (isfinite(x) ? (x) : 0.0)
+    fprintf(fp, "# vtk DataFile Version 3.0\nVTK output\nASCII\nDATASET STRUCTURED_GRID\n");
+    fprintf(fp, "DIMENSIONS %d %d %d\n", NXv, NYv, NZv);
+    fprintf(fp, "POINTS %d float\n", NXv * NYv * NZv);
+    VTK_LOOP fprintf(fp, "%.6f %.6f %.6f\n", (double)i * s->dx, (double)j * s->dy, (double)k * s->dz);
+    fprintf(fp, "\nPOINT_DATA %d\n", NXv * NYv * NZv);
+    fprintf(fp, "VECTORS velocity float\n");
+    VTK_LOOP { size_t c = VTK_ID; fprintf(fp, "%.6f %.6f %.6f\n", FIN(st[0][c]), FIN(st[1][c]), FIN(st[2][c])); }
+    static const char* names6[] = {"temperature", "G_value", "Y_C3H8", "Y_O2", "Y_N2", "Y_CO2", "Y_H2O", "density"};
+    const double* f6[] = {st[3], st[4], st[6], st[7], st[8], st[9], st[10], st[5]};
+    for (int q = 0; q < 8; q++) {
+        fprintf(fp, "SCALARS %s float\nLOOKUP_TABLE default\n", names6[q]);
+        VTK_LOOP fprintf(fp, "%.6f\n", FIN(f6[q][VTK_ID]));
+    }
+    fprintf(fp, "SCALARS omega float\nLOOKUP_TABLE default\n");
+    VTK_LOOP fprintf(fp, "%.6e\n", 0.0);
+    static const char* names_e[] = {"mu_mix", "nu_mix", "ST_turbulent", "nu_t", "grad_G_magnitude"};
+    const double* fe[] = {mu, nu, ST, nut, gg};
+    for (int q = 0; q < 5; q++) {
+        fprintf(fp, "SCALARS %s float\nLOOKUP_TABLE default\n", names_e[q]);
+        VTK_LOOP fprintf(fp, "%.6e\n", FIN(fe[q][VTK_ID]));
+    }
+    /* re_stress_xy = <xy> - <x><y>, 0 before any averaged step (:3586-3655) */
+    static const char* rs[] = {"re_stress_uu", "re_stress_vv", "re_stress_ww", "re_stress_uv", "re_stress_uw",
+                               "re_stress_vw"};
+    static const int ra[6] = {0, 1, 2, 0, 0, 1}, rb[6] = {0, 1, 2, 1, 2, 2}, rp[6] = {3, 4, 5, 6, 7, 8};
+    for (int q = 0; q < 6; q++) {
+        fprintf(fp, "SCALARS %s float\nLOOKUP_TABLE default\n", rs[q]);
+        VTK_LOOP {
+            double v = 0.0;
+            if (navg > 0) {
+                size_t c = VTK_ID;
+                double aa = av[ra[q]][c] / navg, ab = av[rb[q]][c] / navg;
+                v = (av[rp[q]][c] / navg) - (aa * ab);
+            }
+            fprintf(fp, "%.6e\n", FIN(v));
+        }
+    }
+    fprintf(fp, "SCALARS G_mean float\nLOOKUP_TABLE default\n");
+    VTK_LOOP fprintf(fp, "%.6f\n", navg > 0 ? FIN(av[9][VTK_ID] / navg) : 0.0);
+#undef VTK_LOOP
+#undef VTK_ID
+#undef FIN
+    int bad = ferror(fp);
+    fclose(fp);
+    free(buf);
+    if (bad) return serr(s, LESGPU_EIO, "VTK write failed");
     return LESGPU_OK;
+}
+
+static int write_vtk_step(les_solver* s, int t) {
+    if (!(s->out_flags & LES_OUT_VTK) || !s->out_dir[0]) return LESGPU_OK;
+    char name[64], path[1200];
+    snprintf(name, sizeof(name), "Premixed_C3H8_Air_%04d.vtk", t);
+    join_path(path, sizeof(path), s->out_dir, name);
+    return les_solver_write_vtk(s, path);
 }

@@ -32,7 +32,7 @@ FIELD_IDS.update({name: 100 + q for q, name in enumerate(_INSPECT)})
 ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "EIO", -5: "ESTATE", -6: "ENONFINITE"}
 LESGPU_EINVAL, LESGPU_ECUDA, LESGPU_ENOMEM, LESGPU_EIO, LESGPU_ESTATE, LESGPU_ENONFINITE = -1, -2, -3, -4, -5, -6
 
-LES_OUT_PROBES, LES_OUT_MONITOR, LES_OUT_CHECKPOINT, LES_OUT_POINTS = 1, 2, 4, 8
+LES_OUT_PROBES, LES_OUT_MONITOR, LES_OUT_CHECKPOINT, LES_OUT_POINTS, LES_OUT_VTK = 1, 2, 4, 8, 16
 AVG_NAMES = ["u", "v", "w", "uu", "vv", "ww", "uv", "uw", "vw", "G"]
 STRESS_NAMES = ["uu", "vv", "ww", "uv", "uw", "vw", "G_mean"]
 

@@ -83,6 +83,7 @@ enum {
     LESGPU_F_Y0, LESGPU_F_Y1, LESGPU_F_Y2, LESGPU_F_Y3, LESGPU_F_Y4,
     LESGPU_F_NU_T = 11,               /* eddy viscosity of the last RHS evaluation */
     LESGPU_F_S_MAG = 12,              /* |S| of the last RHS evaluation */
+    LESGPU_F_GRAD_G = 13,             /* |grad G| of the last RHS evaluation (lesgpu_keep_grad_g) */
     /* intermediates of the last RHS evaluation (filtered fields, properties, k-arrays) */
     LESGPU_F_U_F = 100, LESGPU_F_V_F, LESGPU_F_W_F, LESGPU_F_T_F, LESGPU_F_G_F, LESGPU_F_RHO_F,
     LESGPU_F_Y0_F, LESGPU_F_Y1_F, LESGPU_F_Y2_F, LESGPU_F_Y3_F, LESGPU_F_Y4_F,
@@ -226,6 +227,11 @@ int lesgpu_kernel_times(lesgpu_ctx* ctx, double* ms, long long* launches, int n)
  * IEEE division.  Runs on the current device; allocates a few bytes of device memory. */
 int lesgpu_selfcheck_division(const double* divisors, int nd, size_t n, unsigned long long seed,
                               unsigned long long* mismatches);
+
+/* Keep |grad G| of every RHS evaluation in a field (grad_G_magnitude_for_debug, :2783,
+ * :2820; written to the VTK files, :3579-3583), readable as LESGPU_F_GRAD_G.  Off by default:
+ * one more store per fluid cell and stage. */
+int lesgpu_keep_grad_g(lesgpu_ctx* ctx, int enable);
 
 /* Time averages: update_time_averages (:3166-3191) on the device.  lesgpu_avg_begin allocates
  * ten FP64 running sums per cell (zeroed) and from then on every step -- host-driven or

@@ -51,6 +51,8 @@ typedef struct les_solver les_solver;
                                   (:4557-4568, flush_point_data :3824-3850) at 4D and 8D, on the
                                   axis and in the shear layer (:3780-3822), flushed every 50 steps,
                                   by les_solver_flush and when the solver is destroyed */
+#define LES_OUT_VTK 16         /* Premixed_C3H8_Air_%04d.vtk every 500 steps (:4594-4598) and at
+                                  les_solver_flush (:4611) */
 
 /* Load the species files, create the GPU context, build the attribute map and the initial
  * state exactly as initialize()+setting() (:1085-1285), seed rand() and place the SEM
@@ -108,9 +110,11 @@ int les_solver_set_averaging(les_solver* s, int start_step);
 int les_solver_save_stats(les_solver* s, const char* path);
 int les_solver_load_stats(les_solver* s, const char* path);
 int les_solver_reynolds_stresses(les_solver* s, double* const* out, int* count);
-/* Write what the end of the reference's run writes and the library still buffers (the point
- * rows). */
+/* Write what the end of the reference's run writes and the library still buffers: the VTK
+ * file of the current step (with LES_OUT_VTK) and the point rows. */
 int les_solver_flush(les_solver* s);
+/* output_vtk (:3473-3668) to `path`, from the current device state. */
+int les_solver_write_vtk(les_solver* s, const char* path);
 
 /* Vortex table (nv x 7) and rand() draw count, for inspection. */
 int les_solver_vortices(const les_solver* s, double* out);

@@ -152,3 +152,82 @@ def test_point_time_series(N, oracle_mod, tmp_path):
             np.testing.assert_allclose(r[t], ref, atol=1.5e-6, rtol=0)
     orc.close()
     h.close()
+
+
+def _golden_outputs():
+    from conftest import GOLDEN
+    return np.load(os.path.join(GOLDEN, "outputs_ref.npz"))
+
+
+def _vtk_sections(text):
+    """{name: values} of a legacy ASCII VTK file; 'points' for the coordinates."""
+    lines = text.splitlines()
+    out, q = {}, 0
+    while q < len(lines):
+        ln = lines[q]
+        if ln.startswith("POINTS"):
+            n = int(ln.split()[1])
+            out["points"] = np.array([list(map(float, lines[q + 1 + r].split())) for r in range(n)])
+            q += n + 1
+        elif ln.startswith("VECTORS") or ln.startswith("SCALARS"):
+            name = ln.split()[1]
+            q += 1
+            if lines[q].startswith("LOOKUP_TABLE"):
+                q += 1
+            vals = []
+            while q < len(lines) and lines[q] and not lines[q][0].isalpha():
+                vals.append(list(map(float, lines[q].split())))
+                q += 1
+            out[name] = np.array(vals)
+        else:
+            q += 1
+    return out
+
+
+def test_vtk_matches_reference_file(N, tmp_path):
+    """output_vtk of the 24x12x16 case after 10 steps, against the reference's own file;
+    values agree to the file's printed precision."""
+    from lesgpu.config import preset
+    z = _golden_outputs()
+    ref_text = z["vtk_tiny_s10"].tobytes().decode()
+    s = N.Solver(preset("tiny"))
+    s.set_outputs(str(tmp_path), N.LES_OUT_VTK)
+    s.step(10)
+    s.flush()
+    s.close()
+    ours_text = open(tmp_path / "Premixed_C3H8_Air_0010.vtk").read()
+    assert ours_text.splitlines()[:6] == ref_text.splitlines()[:6]
+    a, b = _vtk_sections(ours_text), _vtk_sections(ref_text)
+    assert list(a) == list(b)
+    for k in b:
+        assert a[k].shape == b[k].shape, k
+        scale = np.maximum(np.abs(b[k]), 1e-30)
+        err = np.abs(a[k] - b[k])
+        # %.6f fields: 1e-6 absolute; %.6e fields: 1e-6 relative (plus one unit of rounding)
+        ok = (err <= 1.5e-6) | (err <= 2e-6 * scale)
+        assert ok.all(), (k, float(err.max()))
+    assert np.abs(a["grad_G_magnitude"]).max() > 0
+
+
+def test_point_files_match_reference(N, tmp_path):
+    """The point time series of the 40x16x24 case (seed 77) over 60 steps -- flushed at step 50
+    and at the end of the run -- against the reference's files."""
+    from lesgpu.config import preset
+    z = _golden_outputs()
+    names = [str(x) for x in z["point_names"]]
+    assert names
+    s = N.Solver(preset("small", seed=77))
+    s.set_outputs(str(tmp_path), N.LES_OUT_POINTS)
+    s.run_device(60, chunk=32)
+    s.flush()
+    s.close()
+    got = sorted(f for f in os.listdir(tmp_path) if f.startswith("LES_point_data"))
+    assert got == names
+    for q, f in enumerate(names):
+        ref = z[f"point_{q}"].tobytes().decode().splitlines()
+        ours = open(tmp_path / f).read().splitlines()
+        assert ours[0] == ref[0] == "u,v,w,G"
+        a = np.array([list(map(float, r.split(","))) for r in ours[1:]])
+        b = np.array([list(map(float, r.split(","))) for r in ref[1:]])
+        assert a.shape == b.shape == (60, 4)
+        np.testing.assert_allclose(a, b, atol=1.5e-6, rtol=0)
