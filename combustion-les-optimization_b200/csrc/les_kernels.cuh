@@ -21,6 +21,8 @@
 // values are IEEE divisions.
 #pragma once
 
+#include <type_traits>
+
 #include "les_common.cuh"
 
 namespace les {
@@ -177,8 +179,17 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
         aT = (rhof > R(1e-6) && Cp > R(1e-6)) ? qdiv(lam, rhof * Cp) : R(0);
         return;
     }
+    // The FP32 form takes reciprocals once where the FP64 form (the reference's arithmetic)
+    // divides per term.
+    constexpr bool kF32 = std::is_same<R, float>::value;
+    if constexpr (kF32) {
+        const R isyw = qdiv(R(1.0), syw);
 #pragma unroll
-    for (int s = 0; s < NSP; s++) X[s] = qdiv(ym[s], syw);
+        for (int s = 0; s < NSP; s++) X[s] = ym[s] * isyw;
+    } else {
+#pragma unroll
+        for (int s = 0; s < NSP; s++) X[s] = qdiv(ym[s], syw);
+    }
     const R L = qlog(Tl);
     const R L2 = L * L;
     const R L3 = pow3_rn(L);
@@ -192,6 +203,14 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
     // Wilke (:1530-1546) and Wassiljew (:1842-1863) share the same phi_ij, the same skip
     // rule and the same summation order, so one denominator per species serves both.
     R mu = R(0), lam = R(0);
+    R smu[NSP], rsmu[NSP];   // FP32: sqrt(mu_k) and 1/sqrt(mu_k), so sqrt(mu_a/mu_b) = smu_a * rsmu_b
+    if constexpr (kF32) {
+#pragma unroll
+        for (int s = 0; s < NSP; s++) {
+            smu[s] = qsqrt(muk[s]);
+            rsmu[s] = rsqrtf(muk[s]);
+        }
+    }
 #pragma unroll
     for (int a = 0; a < NSP; a++) {
         if (X[a] < R(1e-12)) continue;
@@ -199,14 +218,26 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
 #pragma unroll
         for (int b = 0; b < NSP; b++) {
             if (X[b] < R(1e-12)) continue;
-            R sr = qsqrt(qdiv(muk[a], muk[b]));
+            R sr;
+            if constexpr (kF32) {
+                sr = smu[a] * rsmu[b];
+            } else {
+                // mu_a / mu_a is exactly 1 for a positive finite mu_a, and sqrt(1) = 1
+                sr = (a == b && muk[a] > R(0) && muk[a] <= R(1e300)) ? R(1.0) : qsqrt(qdiv(muk[a], muk[b]));
+            }
             R t = R(1.0) + sr * (R)K.wpow[a][b];
             R ph = cdv(t * t, K.d_wden[a][b]);
             den += X[b] * ph;
         }
         if (den > R(1e-9)) {
-            mu += qdiv(X[a] * muk[a], den);
-            lam += qdiv(X[a] * lamk[a], den);
+            if constexpr (kF32) {
+                const R iden = qdiv(R(1.0), den);
+                mu += (X[a] * muk[a]) * iden;
+                lam += (X[a] * lamk[a]) * iden;
+            } else {
+                mu += qdiv(X[a] * muk[a], den);
+                lam += qdiv(X[a] * lamk[a], den);
+            }
         }
     }
     mu_mix = fmax(R(1e-7), mu);
@@ -230,6 +261,7 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
                 R v = R(0);
                 if (X[a] > R(1e-12) || X[b] > R(1e-12))
                     v = fit_prop<R>(K.dco[a][b], C.dco_zero[a][b], L, L2, L3) * R(1e-4);
+                if constexpr (kF32) v = (v > R(1e-12)) ? qdiv(R(1.0), v) : R(0);   // FP32: 1/D_ab
                 Dm[a][b] = v;
                 Dm[b][a] = v;
             }
@@ -251,7 +283,12 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
             if (a == b) continue;
             if (X[b] > R(1e-12)) {
                 R Dv = Dm[a][b];
-                if (Dv > R(1e-12)) sx += qdiv(X[b], Dv);
+                if constexpr (kF32) {
+                    if (C.dco_sym) sx += X[b] * Dv;                  // Dv holds 1/D_ab (0 when D_ab <= 1e-12)
+                    else if (Dv > R(1e-12)) sx += qdiv(X[b], Dv);
+                } else {
+                    if (Dv > R(1e-12)) sx += qdiv(X[b], Dv);
+                }
             }
         }
         R Dv;
