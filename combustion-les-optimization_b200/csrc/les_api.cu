@@ -130,6 +130,14 @@ void build_consts(const lesgpu_config& g, const lesgpu_species& sp, les::Consts&
         C.d_mwk[a] = dc(C.mwk[a]);
         for (int b = 0; b < les::NSP; b++) C.d_wden[a][b] = dc(C.wden[a][b]);
     }
+    // TENO weight sums w0 + w1 + w2 (w = d * {0.1, 0.6, 0.3}) for each cut-off pattern, with
+    // the kernel's operation order (teno5_reconstruct, :2224-2231)
+    for (int q = 0; q < 8; q++) {
+        const int d0 = q & 1, d1 = (q >> 1) & 1, d2 = (q >> 2) & 1;
+        const double w0 = (double)d0 * 0.1, w1 = (double)d1 * 0.6, w2 = (double)d2 * 0.3;
+        const double ws = w0 + w1 + w2;
+        C.d_tenows[q] = dc(q == 0 ? 1.0 : ws);
+    }
     C.ssr_exp = 2.0 - C.d3;                                             // :1946
     les::fill_float_consts(C);
 }

@@ -187,8 +187,9 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
 #pragma unroll
         for (int s = 0; s < NSP; s++) X[s] = ym[s] * isyw;
     } else {
+        const R ysyw = qdiv(R(1.0), syw);
 #pragma unroll
-        for (int s = 0; s < NSP; s++) X[s] = qdiv(ym[s], syw);
+        for (int s = 0; s < NSP; s++) X[s] = mdiv(ym[s], syw, ysyw);
     }
     const R L = qlog(Tl);
     const R L2 = L * L;
@@ -204,12 +205,16 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
     // rule and the same summation order, so one denominator per species serves both.
     R mu = R(0), lam = R(0);
     R smu[NSP], rsmu[NSP];   // FP32: sqrt(mu_k) and 1/sqrt(mu_k), so sqrt(mu_a/mu_b) = smu_a * rsmu_b
+    R ymu[NSP];              // FP64: 1/mu_k for the shared-denominator quotients
     if constexpr (kF32) {
 #pragma unroll
         for (int s = 0; s < NSP; s++) {
             smu[s] = qsqrt(muk[s]);
             rsmu[s] = rsqrtf(muk[s]);
         }
+    } else {
+#pragma unroll
+        for (int s = 0; s < NSP; s++) ymu[s] = qdiv(R(1.0), muk[s]);
     }
 #pragma unroll
     for (int a = 0; a < NSP; a++) {
@@ -223,7 +228,7 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
                 sr = smu[a] * rsmu[b];
             } else {
                 // mu_a / mu_a is exactly 1 for a positive finite mu_a, and sqrt(1) = 1
-                sr = (a == b && muk[a] > R(0) && muk[a] <= R(1e300)) ? R(1.0) : qsqrt(qdiv(muk[a], muk[b]));
+                sr = (a == b && muk[a] > R(0) && muk[a] <= R(1e300)) ? R(1.0) : qsqrt(mdiv(muk[a], muk[b], ymu[b]));
             }
             R t = R(1.0) + sr * (R)K.wpow[a][b];
             R ph = cdv(t * t, K.d_wden[a][b]);
@@ -235,8 +240,9 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
                 mu += (X[a] * muk[a]) * iden;
                 lam += (X[a] * lamk[a]) * iden;
             } else {
-                mu += qdiv(X[a] * muk[a], den);
-                lam += qdiv(X[a] * lamk[a], den);
+                const R yden = qdiv(R(1.0), den);
+                mu += mdiv(X[a] * muk[a], den, yden);
+                lam += mdiv(X[a] * lamk[a], den, yden);
             }
         }
     }
@@ -250,47 +256,38 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
     if (qok) q = qdiv(lmix, rhof * Cp);
     alpha = fmax(R(1e-7), qok ? q : R(1.8e-5));
     aT = q;
-    // Hirschfelder-Curtiss (:1716-1749).  Binary coefficients D_kj are evaluated once per
-    // unordered pair when the fit table is symmetric.
-    R Dm[NSP][NSP];
+    // Hirschfelder-Curtiss (:1716-1749): sx_a = sum over b != a (ascending b) of X_b / D_ab.
+    // With a symmetric fit table each D_ab is evaluated once per unordered pair and both
+    // sums take their term from it; the rows are visited in ascending order, so each sx_a
+    // still receives its terms in ascending b.  The quotient uses one reciprocal per pair.
+    R sxa[NSP];
+#pragma unroll
+    for (int a = 0; a < NSP; a++) sxa[a] = R(0);
     if (C.dco_sym) {
 #pragma unroll
         for (int a = 0; a < NSP; a++)
 #pragma unroll
             for (int b = a + 1; b < NSP; b++) {
-                R v = R(0);
-                if (X[a] > R(1e-12) || X[b] > R(1e-12))
-                    v = fit_prop<R>(K.dco[a][b], C.dco_zero[a][b], L, L2, L3) * R(1e-4);
-                if constexpr (kF32) v = (v > R(1e-12)) ? qdiv(R(1.0), v) : R(0);   // FP32: 1/D_ab
-                Dm[a][b] = v;
-                Dm[b][a] = v;
+                if (!(X[a] > R(1e-12) || X[b] > R(1e-12))) continue;
+                const R v = fit_prop<R>(K.dco[a][b], C.dco_zero[a][b], L, L2, L3) * R(1e-4);
+                if (!(v > R(1e-12))) continue;
+                const R y = qdiv(R(1.0), v);
+                if (X[b] > R(1e-12)) sxa[a] += mdiv(X[b], v, y);
+                if (X[a] > R(1e-12)) sxa[b] += mdiv(X[a], v, y);
             }
     } else {
 #pragma unroll
         for (int a = 0; a < NSP; a++)
 #pragma unroll
             for (int b = 0; b < NSP; b++) {
-                R v = R(0);
-                if (a != b && X[b] > R(1e-12)) v = fit_prop<R>(K.dco[a][b], C.dco_zero[a][b], L, L2, L3) * R(1e-4);
-                Dm[a][b] = v;
+                if (a == b || !(X[b] > R(1e-12))) continue;
+                const R v = fit_prop<R>(K.dco[a][b], C.dco_zero[a][b], L, L2, L3) * R(1e-4);
+                if (v > R(1e-12)) sxa[a] += qdiv(X[b], v);
             }
     }
 #pragma unroll
     for (int a = 0; a < NSP; a++) {
-        R sx = R(0);
-#pragma unroll
-        for (int b = 0; b < NSP; b++) {
-            if (a == b) continue;
-            if (X[b] > R(1e-12)) {
-                R Dv = Dm[a][b];
-                if constexpr (kF32) {
-                    if (C.dco_sym) sx += X[b] * Dv;                  // Dv holds 1/D_ab (0 when D_ab <= 1e-12)
-                    else if (Dv > R(1e-12)) sx += qdiv(X[b], Dv);
-                } else {
-                    if (Dv > R(1e-12)) sx += qdiv(X[b], Dv);
-                }
-            }
-        }
+        const R sx = sxa[a];
         R Dv;
         if (fabs(R(1.0) - X[a]) < R(1e-9)) {
             int o = (a != N2) ? N2 : O2;
@@ -493,7 +490,8 @@ __device__ __forceinline__ R teno5_rec(const Consts& C, R v0, R v1, R v2, R v3, 
     R w0 = (R)d0 * R(0.1), w1 = (R)d1 * R(0.6), w2 = (R)d2 * R(0.3);
     R ws = w0 + w1 + w2;
     if (ws < R(1e-40)) return p1;
-    return qdiv(w0 * p0 + w1 * p1 + w2 * p2, ws);
+    // ws takes one of seven values: divide by the tabulated divisor (same bits as x / ws)
+    return cdv(w0 * p0 + w1 * p1 + w2 * p2, K.d_tenows[d0 + 2 * d1 + 4 * d2]);
 }
 
 // One axis of the TENO5 G-advection (:2258-2295).
@@ -531,7 +529,8 @@ __device__ __forceinline__ R weno5_grad(const Consts& C, const R* __restrict__ q
     R e0 = eps + i0, e1 = eps + i1, e2 = eps + i2;
     R a0 = qdiv(R(3.0 / 10.0), e0 * e0), a1 = qdiv(R(6.0 / 10.0), e1 * e1), a2 = qdiv(R(1.0 / 10.0), e2 * e2);
     R sa = a0 + a1 + a2;
-    R w0 = qdiv(a0, sa), w1 = qdiv(a1, sa), w2 = qdiv(a2, sa);
+    R ysa = qdiv(R(1.0), sa);
+    R w0 = mdiv(a0, sa, ysa), w1 = mdiv(a1, sa, ysa), w2 = mdiv(a2, sa, ysa);
     R s0 = cdv(R(2.0) * p1 - R(7.0) * p2 + R(11.0) * p3, K.d_six);
     R s1 = cdv(-p2 + R(5.0) * p3 + R(2.0) * p4, K.d_six);
     R s2 = cdv(R(2.0) * p3 + R(5.0) * p4 - p5, K.d_six);
@@ -540,7 +539,8 @@ __device__ __forceinline__ R weno5_grad(const Consts& C, const R* __restrict__ q
     e0 = eps + i0; e1 = eps + i1; e2 = eps + i2;
     a0 = qdiv(R(1.0 / 10.0), e0 * e0); a1 = qdiv(R(6.0 / 10.0), e1 * e1); a2 = qdiv(R(3.0 / 10.0), e2 * e2);
     sa = a0 + a1 + a2;
-    w0 = qdiv(a0, sa); w1 = qdiv(a1, sa); w2 = qdiv(a2, sa);
+    ysa = qdiv(R(1.0), sa);
+    w0 = mdiv(a0, sa, ysa); w1 = mdiv(a1, sa, ysa); w2 = mdiv(a2, sa, ysa);
     R m0 = cdv(-p0 + R(5.0) * p1 + R(2.0) * p2, K.d_six);
     R m1 = cdv(R(2.0) * p1 + R(5.0) * p2 - p3, K.d_six);
     R m2 = cdv(R(11.0) * p2 - R(7.0) * p3 + R(2.0) * p4, K.d_six);

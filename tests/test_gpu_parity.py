@@ -277,7 +277,22 @@ def test_constant_division_matches_ieee(N):
             divs += [d, 2.0 * d, d * d]
         divs.append(2.0 * c.accel_width * c.accel_width)
     divs += [m / 1000.0 for m in props.synthetic_species().mw]
+    # the TENO weight sums w0 + w1 + w2 of every cut-off pattern (kernel operation order)
+    for q in range(1, 8):
+        divs.append((q & 1) * 0.1 + ((q >> 1) & 1) * 0.6 + ((q >> 2) & 1) * 0.3)
     assert N.selfcheck_division(divs, 1 << 21) == 0
+
+
+def test_shared_denominator_division_matches_ieee(N):
+    """Quotients sharing a denominator are computed from one reciprocal y = 1/b (IEEE) and a
+    corrected product; the same check with random divisors over the exponent range the
+    properties use (and significands near 1 and 2) must find no difference from IEEE."""
+    rng = np.random.default_rng(5)
+    sig = rng.uniform(1.0, 2.0, 2048)
+    sig[:128] = 2.0 - rng.integers(1, 1 << 20, 128) * 2.0 ** -52
+    sig[128:256] = 1.0 + rng.integers(1, 1 << 20, 128) * 2.0 ** -52
+    d = np.ldexp(sig, rng.integers(-40, 40, 2048)) * np.where(rng.random(2048) < 0.5, 1.0, -1.0)
+    assert N.selfcheck_division(d, 1 << 17, seed=99) == 0
 
 
 def test_device_loop_matches_host_loop(N, tmp_path):
