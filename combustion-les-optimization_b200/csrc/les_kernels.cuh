@@ -557,26 +557,40 @@ __device__ __forceinline__ R superbee(R r) {
     return fmax(t1, t2);
 }
 
-// MUSCL-superbee along one axis (:2058-2094); values at offsets -2..+2.
+// superbee(dup / ddn) as the reference evaluates it (r = 1e9 when |ddn| < SMALL, :2064),
+// dividing only where the limiter depends on the quotient's value.  For quotients <= 0, in
+// (0.5, 1] or >= 2 the limiter is exactly 0, 1 or 2 whatever the rounding (division is
+// monotonic and 0.5, 1, 2 are representable), and exact comparisons of |dup| with |ddn|
+// decide those cases; NaN operands take the division.
+template <typename R>
+__device__ __forceinline__ R superbee_of(R dup, R ddn) {
+    const R addn = fabs(ddn);
+    if (addn < R(SMALL)) return R(2.0);                   // superbee(1e9)
+    const R adup = fabs(dup);
+    if (adup == adup && addn == addn) {
+        if (dup == R(0) || ((dup > R(0)) != (ddn > R(0)))) return R(0.0);
+        if (adup >= R(2.0) * addn) return R(2.0);
+        if (adup <= addn && adup > R(0.5) * addn) return R(1.0);
+    }
+    return superbee<R>(qdiv(dup, ddn));
+}
+
+// MUSCL-superbee along one axis (:2058-2094); values at offsets -2..+2.  Both faces have
+// the same ddn for either sign of the velocity; the sign only selects the upwind value and
+// dup, so the two branches of the reference become selects (base + x or base - x, the same
+// roundings as the reference's two expressions).
 template <typename R>
 __device__ __forceinline__ R muscl_axis(R vel, R pm2, R pm1, R p0, R pp1, R pp2, const DCT<R>& d) {
-    if (vel >= R(0.0)) {
-        R dup_im = pm1 - pm2, ddn_im = p0 - pm1;
-        R r_im = (fabs(ddn_im) < R(SMALL)) ? R(1e9) : qdiv(dup_im, ddn_im);
-        R phi_imh = pm1 + R(0.5) * superbee<R>(r_im) * ddn_im;
-        R dup_i = p0 - pm1, ddn_i = pp1 - p0;
-        R r_i = (fabs(ddn_i) < R(SMALL)) ? R(1e9) : qdiv(dup_i, ddn_i);
-        R phi_iph = p0 + R(0.5) * superbee<R>(r_i) * ddn_i;
-        return cdv(vel * (phi_iph - phi_imh), d);
-    } else {
-        R dup_i = pp1 - p0, ddn_i = p0 - pm1;
-        R r_i = (fabs(ddn_i) < R(SMALL)) ? R(1e9) : qdiv(dup_i, ddn_i);
-        R phi_imh = p0 - R(0.5) * superbee<R>(r_i) * ddn_i;
-        R dup_ip = pp2 - pp1, ddn_ip = pp1 - p0;
-        R r_ip = (fabs(ddn_ip) < R(SMALL)) ? R(1e9) : qdiv(dup_ip, ddn_ip);
-        R phi_iph = pp1 - R(0.5) * superbee<R>(r_ip) * ddn_ip;
-        return cdv(vel * (phi_iph - phi_imh), d);
-    }
+    const bool pos = vel >= R(0.0);
+    const R ddn_m = p0 - pm1;
+    const R dup_m = pos ? (pm1 - pm2) : (pp1 - p0);
+    const R x_m = R(0.5) * superbee_of<R>(dup_m, ddn_m) * ddn_m;
+    const R phi_imh = pos ? pm1 + x_m : p0 - x_m;
+    const R ddn_p = pp1 - p0;
+    const R dup_p = pos ? (p0 - pm1) : (pp2 - pp1);
+    const R x_p = R(0.5) * superbee_of<R>(dup_p, ddn_p) * ddn_p;
+    const R phi_iph = pos ? p0 + x_p : pp1 - x_p;
+    return cdv(vel * (phi_iph - phi_imh), d);
 }
 
 // First-order upwind fallback used by the non-conservative schemes near faces
