@@ -61,17 +61,18 @@ struct KFlow {               // momentum and G right-hand sides handed from C1 t
 
 #define LES_KERNEL_CONSTS const __grid_constant__ Consts C
 
-// Minimum resident blocks per SM requested from the register allocator.  These kernels are
-// latency-bound; on B200 the 256x128x128 FP64 step was fastest with 4/4/3 (measured sweep
-// over 2..4: 13.4 ms at 2/2/2, 10.8 ms at 3/3/3, 10.5 ms at 4/4/4).
+// Minimum resident blocks per SM requested from the register allocator (filter / flow /
+// scalar).  These kernels are latency-bound; swept on B200 at 256x128x128: FP64 5/4/4 (the
+// scalar pass at 3 blocks 3.41 ms, at 4 3.17 ms; the filter at 4 3.14 ms, at 5 3.02 ms; the
+// flow pass at 5 slower), FP32 8/8/5.
 #ifndef LES_MINB_FILTER
-#define LES_MINB_FILTER 4
+#define LES_MINB_FILTER 5
 #endif
 #ifndef LES_MINB_FLOW
 #define LES_MINB_FLOW 4
 #endif
 #ifndef LES_MINB_SCALAR
-#define LES_MINB_SCALAR 3
+#define LES_MINB_SCALAR 4
 #endif
 #ifndef LES_MINB_FILTER_F32
 #define LES_MINB_FILTER_F32 8
