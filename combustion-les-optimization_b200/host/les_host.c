@@ -928,8 +928,8 @@ int les_solver_write_vtk(les_solver* s, const char* path) {
         if (s->attr[c] != 3) { mu[c] = 1.8e-5; nu[c] = 1.5e-5; }     /* update_nu_mix defaults (:1556-1561) */
     FILE* fp = fopen(path, "w");
     if (!fp) { free(buf); return serr(s, LESGPU_EIO, "cannot open the VTK file"); }
-    static char iobuf[1 << 20];
-    setvbuf(fp, iobuf, _IOFBF, sizeof(iobuf));
+    char* iobuf = (char*)malloc(1 << 20);     /* per call: solvers may write from several threads */
+    if (iobuf) setvbuf(fp, iobuf, _IOFBF, 1 << 20);
     const int NXv = s->nx, NYv = s->ny, NZv = s->nz;
 #define VTK_LOOP for (int k = 0; k < NZv; k++) for (int j = 0; j < NYv; j++) for (int i = 0; i < NXv; i++)
 #define VTK_ID ((((size_t)i * NYv) + j) * NZv + k)
@@ -978,6 +978,7 @@ int les_solver_write_vtk(les_solver* s, const char* path) {
 #undef FIN
     int bad = ferror(fp);
     fclose(fp);
+    free(iobuf);
     free(buf);
     if (bad) return serr(s, LESGPU_EIO, "VTK write failed");
     return LESGPU_OK;
