@@ -930,6 +930,7 @@ int lesgpu_autotune(lesgpu_ctx* ctx, int reps, int tiles_out[5], double* ms_out)
     int old[les::NSH_CLASSES];
     for (int q = 0; q < les::NSH_CLASSES; q++) old[q] = d.shape[q];
     const int cls_of[4] = {LESGPU_K_FILTER, LESGPU_K_STRAIN, LESGPU_K_RHS_FLOW, LESGPU_K_RHS_SCALAR};
+    static_assert(les::NSHAPES == LESGPU_NTILES, "tile table and ABI disagree");
     double ms[4][les::NSHAPES];
     cudaError_t e = cudaSuccess;
     for (int t = 0; t < les::NSHAPES && e == cudaSuccess; t++) {

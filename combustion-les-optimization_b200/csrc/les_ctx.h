@@ -11,20 +11,22 @@
 
 namespace les {
 
-// Thread-block tiles of the per-cell kernels, (k extent, j extent), 256 threads each.  Every
-// kernel indexes through blockDim, so the tile is a launch parameter chosen per kernel class
-// (lesgpu_set_tiles / lesgpu_autotune); the results do not depend on it except through the
-// order of the block partial sums of <rho_f>.
+// Thread-block tiles of the per-cell kernels, (k extent, j extent, i extent), 256 threads each.
+// Every kernel indexes through blockDim, so the tile is a launch parameter chosen per kernel
+// class (lesgpu_set_tiles / lesgpu_autotune); the results do not depend on it except through
+// the order of the block partial sums of <rho_f>.  Tiles spanning several i-planes keep the
+// i-neighbours a block reads in its own SM's L1.
 struct Shape {
-    int bx, by;
+    int bx, by, bz;
 };
-constexpr int NSHAPES = 4;
-constexpr Shape kShapes[NSHAPES] = {{32, 8}, {64, 4}, {16, 16}, {128, 2}};
+constexpr int NSHAPES = 8;
+constexpr Shape kShapes[NSHAPES] = {{32, 8, 1}, {64, 4, 1}, {16, 16, 1}, {128, 2, 1},
+                                    {32, 4, 2}, {16, 8, 2}, {32, 2, 4}, {16, 4, 4}};
 enum { SH_FILTER = 0, SH_STRAIN = 1, SH_FLOW = 2, SH_SCALAR = 3, SH_EOS = 4, NSH_CLASSES = 5 };
 
 inline size_t blocks_for_shape(int nx, int ny, int nz, int s) {
     const Shape t = kShapes[s];
-    return (size_t)((nz + t.bx - 1) / t.bx) * (size_t)((ny + t.by - 1) / t.by) * (size_t)nx;
+    return (size_t)((nz + t.bx - 1) / t.bx) * (size_t)((ny + t.by - 1) / t.by) * (size_t)((nx + t.bz - 1) / t.bz);
 }
 inline size_t max_cell_blocks(int nx, int ny, int nz) {
     size_t m = 0;

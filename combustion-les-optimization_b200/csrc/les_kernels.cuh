@@ -316,11 +316,11 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::filter)
     const int nx = C.nx, ny = C.ny, nz = C.nz;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int i = blockIdx.z * blockDim.z + threadIdx.z;
+    const int tid = (threadIdx.z * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
     const ptrdiff_t sI = (ptrdiff_t)ny * nz, sJ = (ptrdiff_t)nz;
     double mass = 0.0, mnu = 0.0, mal = 0.0;
-    if (k < nz && j < ny) {
+    if (k < nz && j < ny && i < C.nx) {
         const size_t id = cid(i, j, k, ny, nz);
         const int a = attr[id];
         const bool filt = (a == 3) && i >= 1 && i < nx - 1 && j >= 1 && j < ny - 1 && k >= 1 && k < nz - 1;
@@ -403,8 +403,8 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::strain)
     const int nx = C.nx, ny = C.ny, nz = C.nz;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
-    if (k >= nz || j >= ny) return;
+    const int i = blockIdx.z * blockDim.z + threadIdx.z;
+    if (k >= nz || j >= ny || i >= C.nx) return;
     const ptrdiff_t sI = (ptrdiff_t)ny * nz, sJ = (ptrdiff_t)nz;
     const size_t id = cid(i, j, k, ny, nz);
     const bool interior = i >= 1 && i < nx - 1 && j >= 1 && j < ny - 1 && k >= 1 && k < nz - 1;
@@ -668,8 +668,8 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::flow)
     const int nx = C.nx, ny = C.ny, nz = C.nz;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
-    if (k >= nz || j >= ny) return;
+    const int i = blockIdx.z * blockDim.z + threadIdx.z;
+    if (k >= nz || j >= ny || i >= C.nx) return;
     const ptrdiff_t sI = (ptrdiff_t)ny * nz, sJ = (ptrdiff_t)nz;
     const size_t id = cid(i, j, k, ny, nz);
     if (attr[id] != 3) return;
@@ -834,8 +834,8 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::scalar)
     const int nx = C.nx, ny = C.ny, nz = C.nz;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
-    if (k >= nz || j >= ny) return;
+    const int i = blockIdx.z * blockDim.z + threadIdx.z;
+    if (k >= nz || j >= ny || i >= C.nx) return;
     const ptrdiff_t sI = (ptrdiff_t)ny * nz, sJ = (ptrdiff_t)nz;
     const size_t id = cid(i, j, k, ny, nz);
     const int a = attr[id];
@@ -1077,10 +1077,10 @@ __global__ void __launch_bounds__(NT) k_bc_eos(LES_KERNEL_CONSTS, const uint8_t*
     const int ny = C.ny, nz = C.nz;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int i = blockIdx.z * blockDim.z + threadIdx.z;
+    const int tid = (threadIdx.z * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
     double vmax = 0.0;
-    if (k < nz && j < ny) {
+    if (k < nz && j < ny && i < C.nx) {
         const size_t id = cid(i, j, k, ny, nz);
         const int a = attr[id];
         R Y[NSP];
@@ -1138,10 +1138,10 @@ __global__ void __launch_bounds__(NT) k_umax(LES_KERNEL_CONSTS, const uint8_t* _
     const int ny = C.ny, nz = C.nz;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int i = blockIdx.z * blockDim.z + threadIdx.z;
+    const int tid = (threadIdx.z * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
     double vmax = 0.0;
-    if (k < nz && j < ny) {
+    if (k < nz && j < ny && i < C.nx) {
         const size_t id = cid(i, j, k, ny, nz);
         const int a = attr[id];
         if (a == 1 || a == 3) {

@@ -37,11 +37,12 @@ static PropBuf<R> props(const DevCtx& c) {
 
 static inline dim3 cell_block(const DevCtx& c, int cls) {
     const Shape t = kShapes[c.shape[cls]];
-    return dim3((unsigned)t.bx, (unsigned)t.by);
+    return dim3((unsigned)t.bx, (unsigned)t.by, (unsigned)t.bz);
 }
 static inline dim3 cell_grid(const DevCtx& c, int cls) {
     const Shape t = kShapes[c.shape[cls]];
-    return dim3((unsigned)((c.nz + t.bx - 1) / t.bx), (unsigned)((c.ny + t.by - 1) / t.by), (unsigned)c.nx);
+    return dim3((unsigned)((c.nz + t.bx - 1) / t.bx), (unsigned)((c.ny + t.by - 1) / t.by),
+                (unsigned)((c.nx + t.bz - 1) / t.bz));
 }
 
 // Every launch that writes per-block partials checks the buffer first: `per_block` values

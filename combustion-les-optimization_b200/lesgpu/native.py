@@ -336,16 +336,17 @@ class Context:
         self._check(lib().lesgpu_elapsed_ms(self._h, a, b, C.byref(v)), "elapsed_ms")
         return v.value
 
-    # thread-block tiles (k extent, j extent) indexed by lesgpu_set_tiles, per class
-    # {filter, strain, rhs_flow, rhs_scalar, eos}
-    TILES = [(32, 8), (64, 4), (16, 16), (128, 2)]
+    # thread-block tiles (k extent, j extent, i extent) indexed by lesgpu_set_tiles, per
+    # class {filter, strain, rhs_flow, rhs_scalar, eos}
+    TILES = [(32, 8, 1), (64, 4, 1), (16, 16, 1), (128, 2, 1), (32, 4, 2), (16, 8, 2), (32, 2, 4), (16, 4, 4)]
 
     def autotune(self, reps: int = 3):
-        """Install the fastest tile per kernel class; returns (tiles[5], ms[4 classes, 4 tiles])."""
+        """Install the fastest tile per kernel class; returns (tiles[5], ms[4 classes, tiles])."""
+        nt = len(self.TILES)
         tiles = np.zeros(5, dtype=np.int32)
-        ms = np.zeros(16)
+        ms = np.zeros(4 * nt)
         self._check(lib().lesgpu_autotune(self._h, reps, tiles.ctypes.data, ms.ctypes.data), "autotune")
-        return tiles.tolist(), ms.reshape(4, 4)
+        return tiles.tolist(), ms.reshape(4, nt)
 
     def set_tiles(self, tiles):
         t = np.ascontiguousarray(tiles, dtype=np.int32)

@@ -247,13 +247,15 @@ int lesgpu_avg_upload(lesgpu_ctx* ctx, const double* const* sums, int count);
 
 /* Thread-block tiles of the per-cell kernels (no reference counterpart; the reference is
  * serial C).  tiles[c] for the classes {filter, strain, rhs_flow, rhs_scalar, eos} indexes
- * the shapes 0 = 32x8, 1 = 64x4, 2 = 16x16, 3 = 128x2 (k extent x j extent, 256 threads).
+ * the LESGPU_NTILES shapes (k extent x j extent x i extent, 256 threads): 0 = 32x8x1,
+ * 1 = 64x4x1, 2 = 16x16x1, 3 = 128x2x1, 4 = 32x4x2, 5 = 16x8x2, 6 = 32x2x4, 7 = 16x4x4.
  * lesgpu_autotune times `reps` evaluations of the four stage kernels per shape at the
  * current state, picks the fastest shape per class (eos follows filter), installs it and
- * optionally returns it and the times (ms_out: 4 classes x 4 shapes, ms per launch).  It
+ * optionally returns it and the times (ms_out: 4 classes x LESGPU_NTILES, ms per launch).  It
  * leaves the state, the dt inputs and the step counters as they were.  The tile changes
  * only the launch geometry; results change only through the summation order of the block
  * partials of <rho_f> (rounding level). */
+#define LESGPU_NTILES 8
 int lesgpu_set_tiles(lesgpu_ctx* ctx, const int tiles[5]);
 int lesgpu_get_tiles(const lesgpu_ctx* ctx, int tiles[5]);
 int lesgpu_autotune(lesgpu_ctx* ctx, int reps, int tiles_out[5], double* ms_out);

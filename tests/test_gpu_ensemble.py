@@ -51,7 +51,7 @@ def test_ensemble_members_match_solo_runs(N, tmp_path):
     t_loops = [m.t_loop for m in ens.members]
     ens.close()
     for q, (cfg, st, tl) in enumerate(zip(cfgs, got, tiles)):
-        assert all(0 <= t < 4 for t in tl)
+        assert all(0 <= t < len(N.Context.TILES) for t in tl)
         solo = N.Solver(cfg)
         solo.ctx.set_tiles(tl)
         d = tmp_path / f"solo{q}"
@@ -89,7 +89,7 @@ def test_tiles_change_only_rounding(N):
     from lesgpu.config import preset
     cfg = preset("small")
     ref = None
-    for t in range(4):
+    for t in range(len(N.Context.TILES)):
         s = N.Solver(cfg)
         s.ctx.set_tiles([t] * 5)
         assert s.ctx.get_tiles() == [t] * 5
@@ -110,8 +110,9 @@ def test_autotune_leaves_state_and_dt_inputs(N):
     a.step(2)
     before = a.ctx.dt_inputs()
     tiles, ms = a.ctx.autotune(reps=2)
-    assert len(tiles) == 5 and all(0 <= t < 4 for t in tiles)
-    assert ms.shape == (4, 4) and np.all(ms > 0) and np.all(np.isfinite(ms))
+    nt = len(N.Context.TILES)
+    assert len(tiles) == 5 and all(0 <= t < nt for t in tiles)
+    assert ms.shape == (4, nt) and np.all(ms > 0) and np.all(np.isfinite(ms))
     assert tiles[4] == tiles[0]
     for c in range(4):
         assert ms[c, tiles[c]] == ms[c].min()
