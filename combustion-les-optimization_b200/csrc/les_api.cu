@@ -3,6 +3,7 @@
 // Owns the device arena of one solver context, the host-side derivation of the constant
 // table (with the same operations the reference applies to its macros and loaded species
 // data), uploads/downloads in the reference's [i][j][k] order, and the stream-ordered step.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stddef.h>
@@ -157,6 +158,48 @@ unsigned char* read_record(FILE* fp, int* len) {
 // 11 state fields (Phi_n, always 8-byte) and 48 fields of the form's element size.
 constexpr size_t kStateFields = 11;
 size_t fields_for_precision() { return 59; }
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+// Tensor maps of the scalar pass's staged fields (filtered Y_0..Y_4, T, then nu_t): 3-D
+// (k, j, i) views of the arena fields; boxes of (BW x BH x 1) with BH = 12 for the fields and
+// 10 for nu_t; zero fill outside the grid.  Built only when a row (NZ values) is a multiple
+// of 16 bytes, as tensor copies require.
+bool make_tma_maps(DevCtx& d) {
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc || (d.nz * d.esz) % 16 != 0) return false;
+    const bool f64 = d.esz == 8;
+    const cuuint64_t dims[3] = {(cuuint64_t)d.nz, (cuuint64_t)d.ny, (cuuint64_t)d.nx};
+    const cuuint64_t strides[2] = {(cuuint64_t)d.nz * d.esz, (cuuint64_t)d.ny * d.nz * d.esz};
+    const cuuint32_t bw = f64 ? 36 : 40;
+    const cuuint32_t boxf[3] = {bw, 12, 1}, boxn[3] = {bw, 10, 1}, es[3] = {1, 1, 1};
+    const CUtensorMapDataType dt = f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    CUtensorMap* m = reinterpret_cast<CUtensorMap*>(d.tma_maps);
+    void* src[7] = {d.F[6], d.F[7], d.F[8], d.F[9], d.F[10], d.F[3], d.nu_t};
+    for (int q = 0; q < 7; q++) {
+        CUresult r = enc(&m[q], dt, 3, src[q], dims, strides, q < 6 ? boxf : boxn, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return false;
+    }
+    return true;
+}
 
 void free_loop(DevCtx& d);
 
@@ -398,6 +441,12 @@ int lesgpu_create(const lesgpu_config* cfg, const lesgpu_species* sp, lesgpu_ctx
         d.h_pinned = nullptr;
         d.h_pinned_len = 0;
     }
+    static_assert(sizeof(les::TmaMapsStorage) == sizeof(d.tma_maps), "tensor map storage");
+    if (make_tma_maps(d)) {
+        cudaError_t pe = (d.precision == LESGPU_FP64) ? les::prepare_tma_f64() : les::prepare_tma_f32();
+        d.tma_ok = (pe == cudaSuccess);
+        if (pe != cudaSuccess) cudaGetLastError();
+    }
     cudaMemsetAsync(d.dS, 0, sizeof(les::Scalars), d.stream);
     cudaMemsetAsync(d.attr, 0, d.n, d.stream);
     cudaMemsetAsync(d.plane, 0, 3 * planes * sizeof(double), d.stream);
@@ -596,6 +645,7 @@ int lesgpu_dt_inputs(lesgpu_ctx* ctx, double* umax, double* numax, double* alpha
     les::Scalars h;
     CK(cudaMemcpyAsync(&h, d.dS, sizeof(h), cudaMemcpyDeviceToHost, d.stream));
     CK(cudaStreamSynchronize(d.stream));
+    if (h.nonfinite & 4) return fail(ctx, LESGPU_ECUDA, "a tensor copy of the staged scalar pass timed out");
     *umax = h.umax > 1e-10 ? h.umax : ctx->cfg.inlet_velocity;   // :1484
     *numax = h.numax;
     *alphamax = h.alphamax;
@@ -753,6 +803,7 @@ int lesgpu_loop_history(lesgpu_ctx* ctx, int nsteps, double* dt, double* umax, d
     les::Scalars h;
     CK(cudaMemcpy(&h, d.dS, sizeof(h), cudaMemcpyDeviceToHost));
     if (h.nonfinite & 2) return fail(ctx, LESGPU_ESTATE, "rand() jump table too short");
+    if (h.nonfinite & 4) return fail(ctx, LESGPU_ECUDA, "a tensor copy of the staged scalar pass timed out");
     if (nsteps == 0) return LESGPU_OK;
     if (dt) CK(cudaMemcpy(dt, d.hist_dt, nsteps * sizeof(double), cudaMemcpyDeviceToHost));
     if (umax) CK(cudaMemcpy(umax, d.hist_umax, nsteps * sizeof(double), cudaMemcpyDeviceToHost));
@@ -779,6 +830,7 @@ int lesgpu_loop_end(lesgpu_ctx* ctx, unsigned int rng_window[31], double* vortic
     d.total_bytes -= (size_t)d.jrows * 31 * sizeof(unsigned int);
     free_loop(d);
     if (h.nonfinite & 2) return fail(ctx, LESGPU_ESTATE, "rand() jump table too short");
+    if (h.nonfinite & 4) return fail(ctx, LESGPU_ECUDA, "a tensor copy of the staged scalar pass timed out");
     return LESGPU_OK;
 }
 
@@ -912,6 +964,18 @@ int lesgpu_set_tiles(lesgpu_ctx* ctx, const int tiles[5]) {
     return LESGPU_OK;
 }
 
+int lesgpu_set_scalar_staging(lesgpu_ctx* ctx, int enable) {
+    if (!ctx) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    if (enable && !d.tma_ok) return fail(ctx, LESGPU_EINVAL, "staged scalar pass unavailable for this grid");
+    CK(cudaStreamSynchronize(d.stream));
+    d.scalar_tma = enable != 0;
+    drop_graph(d);
+    return LESGPU_OK;
+}
+
+int lesgpu_get_scalar_staging(const lesgpu_ctx* ctx) { return (ctx && ctx->d.scalar_tma) ? 1 : 0; }
+
 int lesgpu_get_tiles(const lesgpu_ctx* ctx, int tiles[5]) {
     if (!ctx || !tiles) return LESGPU_EINVAL;
     for (int q = 0; q < les::NSH_CLASSES; q++) tiles[q] = ctx->d.shape[q];
@@ -961,6 +1025,26 @@ int lesgpu_autotune(lesgpu_ctx* ctx, int reps, int tiles_out[5], double* ms_out)
     }
     best[les::SH_EOS] = best[les::SH_FILTER];
     for (int q = 0; q < les::NSH_CLASSES; q++) d.shape[q] = best[q];
+    // the staged scalar pass against the best tile of the plain one
+    d.scalar_tma = false;
+    if (d.tma_ok) {
+        double ms_plain = ms[3][best[les::SH_SCALAR]], ms_tma = 1e30;
+        d.scalar_tma = true;
+        d.timing = false;
+        e = (d.precision == LESGPU_FP64) ? les::rhs_only_f64(d, 0) : les::rhs_only_f32(d, 0);
+        d.timing = true;
+        for (int q = 0; q < 8; q++) { d.kms[q] = 0.0; d.kcount[q] = 0; }
+        for (int r = 0; r < reps && e == cudaSuccess; r++)
+            e = (d.precision == LESGPU_FP64) ? les::rhs_only_f64(d, 0) : les::rhs_only_f32(d, 0);
+        if (d.kcount[LESGPU_K_RHS_SCALAR] > 0) ms_tma = d.kms[LESGPU_K_RHS_SCALAR] / (double)d.kcount[LESGPU_K_RHS_SCALAR];
+        d.timing = was_timing;
+        for (int q = 0; q < 8; q++) { d.kms[q] = 0.0; d.kcount[q] = 0; }
+        cudaError_t e3 = cudaStreamSynchronize(d.stream);
+        if (e == cudaSuccess) e = e3;
+        if (e == cudaSuccess) e = cudaMemcpy(d.dS, &saved, sizeof(saved), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) { d.scalar_tma = false; return cuda_fail(ctx, e, "autotune (staged pass)"); }
+        d.scalar_tma = ms_tma < ms_plain;
+    }
     drop_graph(d);
     if (tiles_out)
         for (int q = 0; q < les::NSH_CLASSES; q++) tiles_out[q] = best[q];

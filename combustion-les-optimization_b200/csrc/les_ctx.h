@@ -103,6 +103,11 @@ struct DevCtx {
     cudaGraphExec_t graph = nullptr;    // one captured device-loop step
     bool graph_ok = false;
     int shape[NSH_CLASSES] = {0, 0, 0, 0, 0};   // tile (index into kShapes) per kernel class
+    // scalar pass with TMA-staged stencil fields (les_tma.cuh): tensor maps of the six
+    // filtered scalars and nu_t (7 CUtensorMap, 128 bytes each), built at create time
+    alignas(64) unsigned char tma_maps[7 * 128] = {};
+    bool tma_ok = false;                // maps built (row stride a multiple of 16 bytes)
+    bool scalar_tma = false;            // the scalar pass uses them
     // time averages (lesgpu_avg_*): NAVG running sums, FP64, in one allocation
     double* avg = nullptr;
     int avg_start = 0;
@@ -115,6 +120,11 @@ struct DevCtx {
     double kms[8] = {0};
     long long kcount[8] = {0};
     std::string err;
+};
+
+// Storage size of the tensor maps (7 CUtensorMap of 128 bytes).
+struct TmaMapsStorage {
+    unsigned char b[7 * 128];
 };
 
 // Kernel-timing helpers (les_api.cu): tmark_begin returns a pair slot or -1.
@@ -138,5 +148,7 @@ cudaError_t umax_f32(DevCtx& c);
 cudaError_t monitor_f32(DevCtx& c);
 cudaError_t probe_f32(DevCtx& c, int n, int kline);
 cudaError_t check_f32(DevCtx& c, int field);
+cudaError_t prepare_tma_f64();
+cudaError_t prepare_tma_f32();
 
 }  // namespace les

@@ -14,4 +14,6 @@ cudaError_t monitor_f32(DevCtx& c) { return monitor_impl<float>(c); }
 cudaError_t probe_f32(DevCtx& c, int n, int kline) { return probe_impl<float>(c, n, kline); }
 cudaError_t check_f32(DevCtx& c, int field) { return check_impl<float>(c, field); }
 
+cudaError_t prepare_tma_f32() { return prepare_scalar_tma<float, double>(); }
+
 }  // namespace les

@@ -74,4 +74,6 @@ cudaError_t monitor_f64(DevCtx& c) { return monitor_impl<double>(c); }
 cudaError_t probe_f64(DevCtx& c, int n, int kline) { return probe_impl<double>(c, n, kline); }
 cudaError_t check_f64(DevCtx& c, int field) { return check_impl<double>(c, field); }
 
+cudaError_t prepare_tma_f64() { return prepare_scalar_tma<double, double>(); }
+
 }  // namespace les

@@ -594,31 +594,54 @@ __device__ __forceinline__ R muscl_axis(R vel, R pm2, R pm1, R p0, R pp1, R pp2,
     return cdv(vel * (phi_iph - phi_imh), d);
 }
 
+// Stencil access to one field around the current cell, q(di, dj, dk): global memory (the
+// cell's address and the i/j strides) or the shared-memory planes of a staged tile.  The
+// helpers below take either, so both read paths run the same arithmetic.
+template <typename R>
+struct GAcc {
+    const R* __restrict__ p;
+    ptrdiff_t sI, sJ;
+    __device__ __forceinline__ R operator()(int di, int dj, int dk) const { return p[di * sI + dj * sJ + dk]; }
+};
+template <typename R>
+__device__ __forceinline__ GAcc<R> gacc(const R* p, ptrdiff_t sI, ptrdiff_t sJ) {
+    GAcc<R> a;
+    a.p = p; a.sI = sI; a.sJ = sJ;
+    return a;
+}
+// NP planes centred on the cell (di in [-NP/2, NP/2]); pl[d] points at the cell's (j, k) in
+// plane i + d - NP/2, rows bw apart.  Every call site passes constant offsets, so pl[] stays
+// in registers.
+template <typename R, int NP>
+struct SAcc {
+    const R* pl[NP];
+    int bw;
+    __device__ __forceinline__ R operator()(int di, int dj, int dk) const { return pl[di + NP / 2][dj * bw + dk]; }
+};
+
 // First-order upwind fallback used by the non-conservative schemes near faces
 // (:642-651, :2043-2052).
-template <typename R>
-__device__ __forceinline__ R upwind3(const Consts& C, const R* __restrict__ q, ptrdiff_t sI, ptrdiff_t sJ, R u, R v,
-                                     R w) {
+template <typename R, typename A>
+__device__ __forceinline__ R upwind3(const Consts& C, const A& q, R u, R v, R w) {
     const auto& K = kc<R>(C);
     R f;
-    if (u >= R(0.0)) f = cdv(u * (q[0] - q[-sI]), K.d_dx);
-    else f = cdv(u * (q[sI] - q[0]), K.d_dx);
-    if (v >= R(0.0)) f += cdv(v * (q[0] - q[-sJ]), K.d_dy);
-    else f += cdv(v * (q[sJ] - q[0]), K.d_dy);
-    if (w >= R(0.0)) f += cdv(w * (q[0] - q[-1]), K.d_dz);
-    else f += cdv(w * (q[1] - q[0]), K.d_dz);
+    if (u >= R(0.0)) f = cdv(u * (q(0, 0, 0) - q(-1, 0, 0)), K.d_dx);
+    else f = cdv(u * (q(1, 0, 0) - q(0, 0, 0)), K.d_dx);
+    if (v >= R(0.0)) f += cdv(v * (q(0, 0, 0) - q(0, -1, 0)), K.d_dy);
+    else f += cdv(v * (q(0, 1, 0) - q(0, 0, 0)), K.d_dy);
+    if (w >= R(0.0)) f += cdv(w * (q(0, 0, 0) - q(0, 0, -1)), K.d_dz);
+    else f += cdv(w * (q(0, 0, 1) - q(0, 0, 0)), K.d_dz);
     return f;
 }
 
 // calculate_convection_muscl (:2037-2159)
-template <typename R>
-__device__ __forceinline__ R conv_muscl(const Consts& C, const R* __restrict__ q, ptrdiff_t sI, ptrdiff_t sJ, bool band2,
-                                        R u, R v, R w) {
+template <typename R, typename A>
+__device__ __forceinline__ R conv_muscl(const Consts& C, const A& q, bool band2, R u, R v, R w) {
     const auto& K = kc<R>(C);
-    if (band2) return upwind3<R>(C, q, sI, sJ, u, v, w);
-    R cx = muscl_axis<R>(u, q[-2 * sI], q[-sI], q[0], q[sI], q[2 * sI], K.d_dx);
-    R cy = muscl_axis<R>(v, q[-2 * sJ], q[-sJ], q[0], q[sJ], q[2 * sJ], K.d_dy);
-    R cz = muscl_axis<R>(w, q[-2], q[-1], q[0], q[1], q[2], K.d_dz);
+    if (band2) return upwind3<R>(C, q, u, v, w);
+    R cx = muscl_axis<R>(u, q(-2, 0, 0), q(-1, 0, 0), q(0, 0, 0), q(1, 0, 0), q(2, 0, 0), K.d_dx);
+    R cy = muscl_axis<R>(v, q(0, -2, 0), q(0, -1, 0), q(0, 0, 0), q(0, 1, 0), q(0, 2, 0), K.d_dy);
+    R cz = muscl_axis<R>(w, q(0, 0, -2), q(0, 0, -1), q(0, 0, 0), q(0, 0, 1), q(0, 0, 2), K.d_dz);
     return cx + cy + cz;
 }
 
@@ -628,33 +651,32 @@ template <typename R>
 struct SgsFaces {
     R iph, imh, jph, jmh, kph, kmh;
 };
-template <typename R>
-__device__ __forceinline__ SgsFaces<R> sgs_faces(const R* __restrict__ nut, ptrdiff_t sI, ptrdiff_t sJ, const DCT<R>& c2) {
-    R n0 = nut[0];
+template <typename R, typename A>
+__device__ __forceinline__ SgsFaces<R> sgs_faces(const A& nut, const DCT<R>& c2) {
+    R n0 = nut(0, 0, 0);
     SgsFaces<R> g;
-    g.iph = cdv(nut[sI] + n0, c2); g.imh = cdv(n0 + nut[-sI], c2);
-    g.jph = cdv(nut[sJ] + n0, c2); g.jmh = cdv(n0 + nut[-sJ], c2);
-    g.kph = cdv(nut[1] + n0, c2); g.kmh = cdv(n0 + nut[-1], c2);
+    g.iph = cdv(nut(1, 0, 0) + n0, c2); g.imh = cdv(n0 + nut(-1, 0, 0), c2);
+    g.jph = cdv(nut(0, 1, 0) + n0, c2); g.jmh = cdv(n0 + nut(0, -1, 0), c2);
+    g.kph = cdv(nut(0, 0, 1) + n0, c2); g.kmh = cdv(n0 + nut(0, 0, -1), c2);
     return g;
 }
-template <typename R>
-__device__ __forceinline__ R sgs_div(const Consts& C, const R* __restrict__ q, const SgsFaces<R>& g, ptrdiff_t sI,
-                                     ptrdiff_t sJ) {
+template <typename R, typename A>
+__device__ __forceinline__ R sgs_div(const Consts& C, const A& q, const SgsFaces<R>& g) {
     const auto& K = kc<R>(C);
-    R p0 = q[0];
-    R sx = cdv(cdv(g.iph * (q[sI] - p0), K.d_dx) - cdv(g.imh * (p0 - q[-sI]), K.d_dx), K.d_dx);
-    R sy = cdv(cdv(g.jph * (q[sJ] - p0), K.d_dy) - cdv(g.jmh * (p0 - q[-sJ]), K.d_dy), K.d_dy);
-    R sz = cdv(cdv(g.kph * (q[1] - p0), K.d_dz) - cdv(g.kmh * (p0 - q[-1]), K.d_dz), K.d_dz);
+    R p0 = q(0, 0, 0);
+    R sx = cdv(cdv(g.iph * (q(1, 0, 0) - p0), K.d_dx) - cdv(g.imh * (p0 - q(-1, 0, 0)), K.d_dx), K.d_dx);
+    R sy = cdv(cdv(g.jph * (q(0, 1, 0) - p0), K.d_dy) - cdv(g.jmh * (p0 - q(0, -1, 0)), K.d_dy), K.d_dy);
+    R sz = cdv(cdv(g.kph * (q(0, 0, 1) - p0), K.d_dz) - cdv(g.kmh * (p0 - q(0, 0, -1)), K.d_dz), K.d_dz);
     return sx + sy + sz;
 }
 
-template <typename R>
-__device__ __forceinline__ R lap3(const Consts& C, const R* __restrict__ q, ptrdiff_t sI, ptrdiff_t sJ) {
+template <typename R, typename A>
+__device__ __forceinline__ R lap3(const Consts& C, const A& q) {
     const auto& K = kc<R>(C);
-    R p0 = q[0];
-    R a = cdv(q[sI] - R(2.0) * p0 + q[-sI], K.d_dxx);
-    R b = cdv(q[sJ] - R(2.0) * p0 + q[-sJ], K.d_dyy);
-    R c = cdv(q[1] - R(2.0) * p0 + q[-1], K.d_dzz);
+    R p0 = q(0, 0, 0);
+    R a = cdv(q(1, 0, 0) - R(2.0) * p0 + q(-1, 0, 0), K.d_dxx);
+    R b = cdv(q(0, 1, 0) - R(2.0) * p0 + q(0, -1, 0), K.d_dyy);
+    R c = cdv(q(0, 0, 1) - R(2.0) * p0 + q(0, 0, -1), K.d_dzz);
     return a + b + c;
 }
 
@@ -718,7 +740,7 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::flow)
             }
             R conv = cdv(mf_iph * p_iph - mf_imh * p_imh, K.d_dx) + cdv(mf_jph * p_jph - mf_jmh * p_jmh, K.d_dy) +
                      cdv(mf_kph * p_kph - mf_kmh * p_kmh, K.d_dz);
-            kmom[q] = -conv + mu_eff * lap3<R>(C, ph, sI, sJ);
+            kmom[q] = -conv + mu_eff * lap3<R>(C, gacc(ph, sI, sJ));
         }
         R grav = (r0 - (R)Sc->rho_avg) * R(G_GRAVITY);
         R fx = R(0), fy = R(0), fz = R(0);
@@ -764,7 +786,7 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::flow)
         R conv;
         if (band3) {
             if (band2) {
-                conv = upwind3<R>(C, Gf, sI, sJ, u0, v0, w0);
+                conv = upwind3<R>(C, gacc(Gf, sI, sJ), u0, v0, w0);
             } else {
                 // calculate_convection_non_conservative interior branch (:652-677); the
                 // zero UW2 coefficient again makes both upwind branches identical.
@@ -783,8 +805,8 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::flow)
             R fza = teno_axis<R>(C, w0, Gf, 1, K.d_dz);
             conv = fxa + fya + fza;
         }
-        SgsFaces<R> gf = sgs_faces<R>(P.nu_t + id, sI, sJ, K.d_sct2);
-        R sgs = sgs_div<R>(C, Gf, gf, sI, sJ);
+        SgsFaces<R> gf = sgs_faces<R>(gacc<R>(P.nu_t + id, sI, sJ), K.d_sct2);
+        R sgs = sgs_div<R>(C, gacc(Gf, sI, sJ), gf);
         R gx, gy, gz;
         if (Sc->t_loop >= C.weno_step && !band3) {
             gx = weno5_grad<R>(C, Gf, sI, K.d_dx);
@@ -807,7 +829,7 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::flow)
                 // tip_mask = 1 - exp(-r^2 / 0^2) is exactly 1 for every fluid cell (j >= 1)
                 // because TIP_PROTECTION_RADIUS is 0.0 (:234, :2806-2807).
                 R adc = R(5.0) * (P.nu_t[id] + R(1.0e-5)) * window * R(1.0);
-                art = adc * lap3<R>(C, Gf, sI, sJ);
+                art = adc * lap3<R>(C, gacc(Gf, sI, sJ));
             }
         }
         kG = -conv + prop + sgs + art;
@@ -826,17 +848,28 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::flow)
 
 // C2: species (:2837-2904) and temperature (:2912-2962), then the RK4 bookkeeping.
 // stage: 0,1,2 -> intermediate stage with coefficient 0.5/0.5/1.0, 3 -> final combine.
-template <typename R, typename RS = R>
-__global__ void __launch_bounds__(NT, MinBlocks<R>::scalar)
-    k_rhs_scalar(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> F, PropBuf<R> P, F11<RS> S0, F11<R> St,
-                 AccBuf<R> acc, KFlow<R> kf, KDbg<R> kd, const Scalars* __restrict__ Sc, int stage) {
+// Where the scalar pass reads its stencil fields (filtered T and Y_k, nu_t): global memory,
+// or the shared-memory tile of the staged kernel (les_tma.cuh).
+template <typename R>
+struct GSrc {
+    const R* T;
+    const R* Y[NSP];
+    const R* nut;
+    ptrdiff_t sI, sJ;
+    __device__ __forceinline__ GAcc<R> y(int s) const { return gacc(Y[s], sI, sJ); }
+    __device__ __forceinline__ GAcc<R> t() const { return gacc(T, sI, sJ); }
+    __device__ __forceinline__ GAcc<R> nu() const { return gacc(nut, sI, sJ); }
+};
+
+// One cell of the scalar pass (the body shared by both read paths).
+template <typename R, typename RS, typename Src>
+__device__ __forceinline__ void rhs_scalar_cell(const Consts& C, const uint8_t* __restrict__ attr, const F11<R>& F,
+                                                const PropBuf<R>& P, const F11<RS>& S0, const F11<R>& St,
+                                                const AccBuf<R>& acc, const KFlow<R>& kf, const KDbg<R>& kd,
+                                                const Scalars* __restrict__ Sc, int stage, int i, int j, int k,
+                                                const Src& src) {
     const auto& K = kc<R>(C);
     const int nx = C.nx, ny = C.ny, nz = C.nz;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z * blockDim.z + threadIdx.z;
-    if (k >= nz || j >= ny || i >= C.nx) return;
-    const ptrdiff_t sI = (ptrdiff_t)ny * nz, sJ = (ptrdiff_t)nz;
     const size_t id = cid(i, j, k, ny, nz);
     const int a = attr[id];
 
@@ -871,31 +904,31 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::scalar)
     R g = F.p[4][id];
     if (g < R(0.0)) g = R(0.0);
     if (g > R(1.0)) g = R(1.0);
-    const SgsFaces<R> gs = sgs_faces<R>(P.nu_t + id, sI, sJ, K.d_sct2);
+    const SgsFaces<R> gs = sgs_faces<R>(src.nu(), K.d_sct2);
     const R relax = (R)K.relax;
 #pragma unroll
     for (int s = 0; s < NSP; s++) {
-        const R* __restrict__ Yf = F.p[6 + s] + id;
-        R conv = conv_muscl<R>(C, Yf, sI, sJ, band2, u0, v0, w0);
-        R mol = P.D[s][id] * lap3<R>(C, Yf, sI, sJ);
-        R sgs = sgs_div<R>(C, Yf, gs, sI, sJ);
+        const auto qY = src.y(s);
+        R conv = conv_muscl<R>(C, qY, band2, u0, v0, w0);
+        R mol = P.D[s][id] * lap3<R>(C, qY);
+        R sgs = sgs_div<R>(C, qY, gs);
         R tgt;
         if (s == C3H8) tgt = (R)K.inletYk[C3H8] * (R(1.0) - g);
         else if (s == O2) tgt = fmax(R(0.0), (R)K.inletYk[O2] - (R)K.cons_o2 * g);
         else if (s == CO2) tgt = (R)K.inletYk[CO2] + (R)K.prod_co2 * g;
         else if (s == H2O) tgt = (R)K.inletYk[H2O] + (R)K.prod_h2o * g;
         else tgt = (R)K.inletYk[N2];
-        R nud = relax * (tgt - Yf[0]);
+        R nud = relax * (tgt - qY(0, 0, 0));
         kv[5 + s] = -conv + mol + sgs + nud;
     }
     {
-        const R* __restrict__ Tf = F.p[3] + id;
-        R conv = conv_muscl<R>(C, Tf, sI, sJ, band2, u0, v0, w0);
-        R mol = P.aT[id] * lap3<R>(C, Tf, sI, sJ);
-        const SgsFaces<R> gt = sgs_faces<R>(P.nu_t + id, sI, sJ, K.d_prt2);
-        R sgs = sgs_div<R>(C, Tf, gt, sI, sJ);
+        const auto qT = src.t();
+        R conv = conv_muscl<R>(C, qT, band2, u0, v0, w0);
+        R mol = P.aT[id] * lap3<R>(C, qT);
+        const SgsFaces<R> gt = sgs_faces<R>(src.nu(), K.d_prt2);
+        R sgs = sgs_div<R>(C, qT, gt);
         R Tt = (R)K.t_in + g * (R)K.t_burnt_span;
-        R nud = relax * (Tt - Tf[0]);
+        R nud = relax * (Tt - qT(0, 0, 0));
         kv[3] = -conv + mol + sgs + nud;
     }
     kv[0] = kf.p[0][id];
@@ -965,6 +998,26 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::scalar)
 #pragma unroll
         for (int s = 0; s < NSP; s++) out[6 + s][id] = R(Y[s]);
     }
+}
+
+template <typename R, typename RS = R>
+__global__ void __launch_bounds__(NT, MinBlocks<R>::scalar)
+    k_rhs_scalar(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> F, PropBuf<R> P, F11<RS> S0, F11<R> St,
+                 AccBuf<R> acc, KFlow<R> kf, KDbg<R> kd, const Scalars* __restrict__ Sc, int stage) {
+    const int ny = C.ny, nz = C.nz;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = blockIdx.z * blockDim.z + threadIdx.z;
+    if (k >= nz || j >= ny || i >= C.nx) return;
+    const size_t id = cid(i, j, k, ny, nz);
+    GSrc<R> src;
+    src.sI = (ptrdiff_t)ny * nz;
+    src.sJ = (ptrdiff_t)nz;
+    src.T = F.p[3] + id;
+#pragma unroll
+    for (int s = 0; s < NSP; s++) src.Y[s] = F.p[6 + s] + id;
+    src.nut = P.nu_t + id;
+    rhs_scalar_cell<R, RS>(C, attr, F, P, S0, St, acc, kf, kd, Sc, stage, i, j, k, src);
 }
 
 // ------------------------------------------------------------------ boundary conditions

@@ -4,6 +4,7 @@
 
 #include "les_ctx.h"
 #include "les_kernels.cuh"
+#include "les_tma.cuh"
 
 namespace les {
 
@@ -113,7 +114,8 @@ cudaError_t step_impl(DevCtx& c, double dt, int t_loop, bool device_mode) {
         k_rhs_flow<R><<<gC, bC, 0, st>>>(c.hC, c.attr, F, P, kf, kds, c.dS);
         tmark_end(c, tm);
         tm = tmark_begin(c, 5);
-        k_rhs_scalar<R, RS><<<gD, bD, 0, st>>>(c.hC, c.attr, F, P, S, St, acc, kf, kds, c.dS, s);
+        if (c.scalar_tma && c.tma_ok) launch_scalar_tma<R, RS>(c, st, F, P, S, St, acc, kf, kds, s);
+        else k_rhs_scalar<R, RS><<<gD, bD, 0, st>>>(c.hC, c.attr, F, P, S, St, acc, kf, kds, c.dS, s);
         tmark_end(c, tm);
     }
     // apply_boundary_conditions (:2967-3161)
@@ -175,8 +177,11 @@ cudaError_t rhs_only_impl(DevCtx& c, int t_loop) {
     k_rhs_flow<R><<<cell_grid(c, SH_FLOW), cell_block(c, SH_FLOW), 0, st>>>(c.hC, c.attr, F, P, kf, kd, c.dS);
     tmark_end(c, tm);
     tm = tmark_begin(c, 5);
-    k_rhs_scalar<R, RS><<<cell_grid(c, SH_SCALAR), cell_block(c, SH_SCALAR), 0, st>>>(c.hC, c.attr, F, P, S, St,
-                                                                                       acc, kf, kd, c.dS, 0);
+    if (c.scalar_tma && c.tma_ok)
+        launch_scalar_tma<R, RS>(c, st, F, P, S, St, acc, kf, kd, 0);
+    else
+        k_rhs_scalar<R, RS><<<cell_grid(c, SH_SCALAR), cell_block(c, SH_SCALAR), 0, st>>>(c.hC, c.attr, F, P, S, St,
+                                                                                           acc, kf, kd, c.dS, 0);
     tmark_end(c, tm);
     tmark_flush(c);
     return cudaGetLastError();

@@ -158,6 +158,8 @@ def lib():
         _sig(L, "lesgpu_avg_upload", C.c_int, [vp, vp, C.c_int])
         _sig(L, "les_solver_loop_collect", C.c_int, [vp, C.c_int])
         _sig(L, "lesgpu_autotune", C.c_int, [vp, C.c_int, vp, dp])
+        _sig(L, "lesgpu_set_scalar_staging", C.c_int, [vp, C.c_int])
+        _sig(L, "lesgpu_get_scalar_staging", C.c_int, [vp])
         _sig(L, "lesgpu_set_tiles", C.c_int, [vp, vp])
         _sig(L, "lesgpu_get_tiles", C.c_int, [vp, vp])
         _sig(L, "lesgpu_group_create", C.c_int, [vp, C.c_int, C.POINTER(vp)])
@@ -351,6 +353,13 @@ class Context:
     def set_tiles(self, tiles):
         t = np.ascontiguousarray(tiles, dtype=np.int32)
         self._check(lib().lesgpu_set_tiles(self._h, t.ctypes.data), "set_tiles")
+
+    def set_scalar_staging(self, enable: bool):
+        """The scalar pass with TMA-staged stencil fields (same arithmetic, same bits)."""
+        self._check(lib().lesgpu_set_scalar_staging(self._h, 1 if enable else 0), "set_scalar_staging")
+
+    def get_scalar_staging(self) -> bool:
+        return bool(lib().lesgpu_get_scalar_staging(self._h))
 
     def get_tiles(self):
         t = np.zeros(5, dtype=np.int32)

@@ -259,6 +259,12 @@ int lesgpu_avg_upload(lesgpu_ctx* ctx, const double* const* sums, int count);
 int lesgpu_set_tiles(lesgpu_ctx* ctx, const int tiles[5]);
 int lesgpu_get_tiles(const lesgpu_ctx* ctx, int tiles[5]);
 int lesgpu_autotune(lesgpu_ctx* ctx, int reps, int tiles_out[5], double* ms_out);
+/* The scalar pass with its stencil fields staged in shared memory by tensor copies
+ * (cp.async.bulk.tensor, a (32 x 8) tile marching through i-planes; the same arithmetic, so
+ * the same bits).  Available when a grid row (NZ values) is a multiple of 16 bytes;
+ * lesgpu_autotune switches it on when it times faster than the best plain tile. */
+int lesgpu_set_scalar_staging(lesgpu_ctx* ctx, int enable);
+int lesgpu_get_scalar_staging(const lesgpu_ctx* ctx);
 
 /* Block until all work queued on the context's stream has finished. */
 int lesgpu_sync(lesgpu_ctx* ctx);

@@ -165,3 +165,25 @@ def test_optimisation_campaign_on_ensembles(N, tmp_path):
     assert len(trials) == 6
     for t in trials:
         assert os.path.exists(tmp_path / t / "probe_data_flame_region_loc0.csv")
+
+
+@pytest.mark.parametrize("name,prec", [("c1", "fp64"), ("small", "fp64"), ("c1", "fp32"), ("e96", "fp64")])
+def test_staged_scalar_pass_gives_the_same_bits(N, name, prec):
+    """The scalar pass reading its stencil fields from shared-memory planes filled by tensor
+    copies runs the same arithmetic as the plain pass: identical states (device loop, all
+    four RK stages, the final combine) and no copy timed out."""
+    from lesgpu.config import preset
+    P = N.FP64 if prec == "fp64" else N.FP32
+    cfg = preset(name, seed=17)
+    out = []
+    for staged in (False, True):
+        s = N.Solver(cfg, precision=P)
+        if staged:
+            s.ctx.set_scalar_staging(True)
+            assert s.ctx.get_scalar_staging()
+        s.run_device(9, chunk=4)
+        s.step(2)
+        out.append(s.state())
+        s.close()
+    for f in STATE:
+        np.testing.assert_array_equal(out[0][f], out[1][f], err_msg=f)
