@@ -42,6 +42,7 @@ typedef struct serve_req {
 typedef struct tile_entry {
     int nx, ny, nz, precision;
     int tiles[5];
+    int staged;                   /* scalar pass through the staged (TMA) kernel */
 } tile_entry;
 
 struct les_serve {
@@ -174,10 +175,10 @@ int les_serve_cancel(les_serve* s, long long id) {
     return LESGPU_OK;
 }
 
-static const int* cached_tiles(les_serve* s, const lesgpu_config* c) {
+static const tile_entry* cached_tiles(les_serve* s, const lesgpu_config* c) {
     for (int q = 0; q < s->n_tiles; q++) {
         const tile_entry* t = &s->tiles[q];
-        if (t->nx == c->nx && t->ny == c->ny && t->nz == c->nz && t->precision == c->precision) return t->tiles;
+        if (t->nx == c->nx && t->ny == c->ny && t->nz == c->nz && t->precision == c->precision) return t;
     }
     return NULL;
 }
@@ -187,9 +188,12 @@ static int admit(les_serve* s, serve_req* q) {
     if (rc) return rc;
     lesgpu_ctx* ctx = les_solver_ctx(q->sol);
     if (s->opt.autotune) {
-        const int* t = cached_tiles(s, &q->cfg);
+        /* one autotuning per grid shape and precision; later requests of that shape get the
+           same tiles and scalar-pass form, so their results do not depend on arrival order */
+        const tile_entry* t = cached_tiles(s, &q->cfg);
         if (t) {
-            rc = lesgpu_set_tiles(ctx, t);
+            rc = lesgpu_set_tiles(ctx, t->tiles);
+            if (rc == LESGPU_OK) rc = lesgpu_set_scalar_staging(ctx, t->staged);
         } else {
             int tl[5];
             rc = lesgpu_autotune(ctx, 3, tl, NULL);
@@ -197,6 +201,7 @@ static int admit(les_serve* s, serve_req* q) {
                 tile_entry* e = &s->tiles[s->n_tiles++];
                 e->nx = q->cfg.nx; e->ny = q->cfg.ny; e->nz = q->cfg.nz; e->precision = q->cfg.precision;
                 memcpy(e->tiles, tl, sizeof(tl));
+                e->staged = lesgpu_get_scalar_staging(ctx);
             }
         }
     }

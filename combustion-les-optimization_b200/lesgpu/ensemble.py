@@ -7,10 +7,17 @@ sets at once, each member with its own grid, constants, seed and output files.
 [0.08, 0.22], the flame-acceleration strength uniform in [0, 2] x its default, the nudging
 coefficient uniform in [0, 1] x its default, members alternating between the 128x64x64 and
 96x48x48 grids.
+
+Measurement (one JSON line; wall time of a long run, set-up of each run included):
+
+    python -m lesgpu.ensemble --members 64 --precision fp32 --steps 200 [--sequential]
 """
 from __future__ import annotations
 
 import ctypes as C
+import json
+import time
+from collections import Counter
 from typing import List, Sequence
 
 import numpy as np
@@ -67,3 +74,65 @@ class Ensemble:
             self.close()
         except Exception:
             pass
+
+
+def _timed(f) -> float:
+    """Wall seconds of f(); every call into the library returns after the device finished."""
+    t = time.perf_counter()
+    f()
+    return time.perf_counter() - t
+
+
+def main(argv=None) -> int:
+    import argparse
+    ap = argparse.ArgumentParser(description="Time an ensemble of solvers stepped by one multi-stream graph")
+    ap.add_argument("--members", type=int, default=64)
+    ap.add_argument("--grids", default="e128,e96", help="comma-separated presets, assigned round-robin")
+    ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp32")
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--chunk", type=int, default=64)
+    ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--sequential", action="store_true",
+                    help="also time one solo solver per grid and sum them over the members")
+    a = ap.parse_args(argv)
+    prec = N.FP32 if a.precision == "fp32" else N.FP64
+    grids = tuple(a.grids.split(","))
+    cfgs = ensemble_configs(a.members, grids=grids)
+    out = {"members": a.members, "grids": dict(Counter(grids[q % len(grids)] for q in range(a.members))),
+           "precision": a.precision, "steps": a.steps, "chunk": a.chunk, "autotune": not a.no_autotune}
+    t = time.perf_counter()
+    ens = Ensemble(cfgs, precision=prec, autotune=not a.no_autotune)
+    out["create_s"] = time.perf_counter() - t
+    tiles = {}
+    for q, m in enumerate(ens.members):
+        tiles.setdefault(grids[q % len(grids)], Counter())[tuple(m.ctx.get_tiles())] += 1
+    out["tiles"] = {g: [list(k) + [n] for k, n in c.most_common()] for g, c in tiles.items()}
+    if a.warmup:
+        ens.run(a.warmup, chunk=a.chunk)
+    w = _timed(lambda: ens.run(a.steps, chunk=a.chunk))
+    out["ms_per_step"] = w * 1e3 / a.steps
+    out["cells"] = ens.cells
+    out["cell_steps_per_s"] = ens.cells * a.steps / w
+    out["finite"] = all(bool(np.isfinite(m.state()["u"]).all()) for m in ens.members)
+    ens.close()
+    if a.sequential:
+        solo = {}
+        for g in grids:
+            q = grids.index(g)
+            s = N.Solver(cfgs[q], precision=prec)
+            if not a.no_autotune:
+                s.ctx.autotune(3)
+            s.run_device(a.warmup or 1, chunk=a.chunk)
+            solo[g] = _timed(lambda: s.run_device(a.steps, chunk=a.chunk)) * 1e3 / a.steps
+            s.close()
+        seq = sum(solo[grids[q % len(grids)]] for q in range(a.members))
+        out["solo_ms_per_step"] = solo
+        out["sequential_ms_per_step"] = seq
+        out["speedup_vs_sequential"] = seq / out["ms_per_step"]
+    print(json.dumps(out))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

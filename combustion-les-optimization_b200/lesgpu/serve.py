@@ -5,10 +5,15 @@
 256x128x128, step counts uniform over an integer range, model constants drawn as for the
 batched ensemble); ``replay`` submits the requests at their arrival times while stepping the
 server and returns the latency / throughput summary.
+
+Measurement (one JSON line):
+
+    python -m lesgpu.serve --requests 100 --rate 20 --steps 50 200 --quantum 16
 """
 from __future__ import annotations
 
 import ctypes as C
+import json
 import time
 from dataclasses import dataclass
 from typing import Dict, List, Optional, Sequence
@@ -198,3 +203,30 @@ def replay(server: Server, requests: Sequence[Request], precision: int = N.FP32,
         for rid in ids:
             server.release(rid)
     return s
+
+
+def main(argv=None) -> int:
+    import argparse
+    ap = argparse.ArgumentParser(description="Replay a seeded Poisson request stream through the serving loop")
+    ap.add_argument("--requests", type=int, default=100)
+    ap.add_argument("--rate", type=float, default=20.0, help="mean arrivals per second")
+    ap.add_argument("--steps", type=int, nargs=2, default=(50, 200), metavar=("MIN", "MAX"))
+    ap.add_argument("--quantum", type=int, default=16)
+    ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp32")
+    ap.add_argument("--budget-gb", type=float, default=150.0)
+    ap.add_argument("--seed", type=int, default=2024)
+    a = ap.parse_args(argv)
+    prec = N.FP32 if a.precision == "fp32" else N.FP64
+    reqs = poisson_requests(a.requests, rate=a.rate, steps=tuple(a.steps), seed=a.seed)
+    srv = Server(budget_bytes=int(a.budget_gb * 1e9), quantum=a.quantum, autotune=True)
+    st = replay(srv, reqs, prec)
+    srv.close()
+    st.pop("ids")
+    st.update(requests=a.requests, rate=a.rate, steps=list(a.steps), quantum=a.quantum, precision=a.precision,
+              demand_cell_steps=sum(r.cfg.cells * r.nsteps for r in reqs))
+    print(json.dumps(st))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
