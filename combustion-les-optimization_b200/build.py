@@ -98,11 +98,11 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
     for src in c:
         name = os.path.splitext(os.path.basename(src))[0]
         obj = os.path.join(bdir, name + ".o")
-        _run(["gcc", "-c", src, "-o", obj, "-O2", "-ffp-contract=off", "-fPIC", "-std=c11", "-Wall",
+        _run(["gcc", "-c", src, "-o", obj, "-O2", "-ffp-contract=off", "-fPIC", "-std=c11", "-Wall", "-pthread",
               "-I", INC, "-I", os.path.join(HERE, "host")], verbose)
         objs.append(obj)
     tmp = lib_path + ".tmp"
-    _run([nvcc, "-shared", "-o", tmp] + objs + ARCH + ["-Xcompiler", "-fPIC", "-lcudart", "-lm",
+    _run([nvcc, "-shared", "-o", tmp] + objs + ARCH + ["-Xcompiler", "-fPIC", "-lcudart", "-lm", "-lpthread",
                                                           "-L", _cuda_lib_dir(nvcc)], verbose)
     os.replace(tmp, lib_path)
     return lib_path

@@ -164,16 +164,16 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 EncodeTiledFn encode_tiled() {
-    static EncodeTiledFn fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
-        tried = true;
+    // looked up once; the initialisation of a function-local static is thread-safe, so
+    // contexts may be created from several host threads
+    static const EncodeTiledFn fn = []() -> EncodeTiledFn {
         void* p = nullptr;
         cudaDriverEntryPointQueryResult q;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            fn = (EncodeTiledFn)p;
-    }
+            return (EncodeTiledFn)p;
+        return nullptr;
+    }();
     return fn;
 }
 
@@ -253,13 +253,9 @@ namespace {
 std::vector<unsigned int> jump_table(int rows) {
     std::vector<unsigned int> J((size_t)rows * 31, 0u);
     auto row = [&](int t) -> const unsigned int* { return &J[(size_t)t * 31]; };
-    static unsigned int unit[31][31];
-    static bool init = false;
-    if (!init) {
-        for (int a = 0; a < 31; a++)
-            for (int b = 0; b < 31; b++) unit[a][b] = (a == b) ? 1u : 0u;
-        init = true;
-    }
+    unsigned int unit[31][31];
+    for (int a = 0; a < 31; a++)
+        for (int b = 0; b < 31; b++) unit[a][b] = (a == b) ? 1u : 0u;
     for (int t = 0; t < rows; t++) {
         const unsigned int* a = (t - 31 < 0) ? unit[t] : row(t - 31);         // x[t-31]
         const unsigned int* b = (t - 3 < 0) ? unit[t + 28] : row(t - 3);     // x[t-3]
@@ -943,6 +939,11 @@ int lesgpu_sync(lesgpu_ctx* ctx) {
     if (!ctx) return LESGPU_EINVAL;
     CK(cudaStreamSynchronize(ctx->d.stream));
     return LESGPU_OK;
+}
+
+int lesgpu_bind_device(int device) {
+    if (device < 0) return LESGPU_EINVAL;
+    return cudaSetDevice(device) == cudaSuccess ? LESGPU_OK : LESGPU_ECUDA;
 }
 
 // ---------------------------------------------------------------- tiles and autotuning

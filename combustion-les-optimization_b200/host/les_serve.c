@@ -4,20 +4,26 @@
  * No counterpart in the reference, which runs one solve per process.  Requests (a config,
  * a step count, optional output files) are submitted at any time.  Each scheduling round
  * (les_serve_step):
- *   1. admits queued requests in arrival order while a slot is free and the request's
+ *   1. starts the requests whose set-up has finished (their first quantum is queued) and
+ *      retires those whose tear-down has finished;
+ *   2. admits queued requests in arrival order while a slot is free and the request's
  *      device memory fits the remaining HBM budget (a request that can never fit is refused
- *      at submission);
- *   2. queues up to `quantum` device-loop steps of every active request, each on its own
- *      stream as a replayed CUDA graph, so the solves overlap on the device;
- *   3. collects every active request's step history (probe / monitor rows) and retires the
- *      requests that have finished: the final state is copied to the host when results are
- *      kept, the solver is destroyed and its memory returns to the budget at once.
- * Requests that arrive while others run join at the next round (continuous batching).  A
- * request's result does not depend on what else is running: every solver has its own
- * state, rand() stream and tiles, and the device loop's results do not depend on how its
- * steps are chunked.
+ *      at submission); their set-up (solver, initial state, uploads, tiles, device-loop
+ *      session) runs on the server's worker threads while the device steps the others;
+ *   3. collects every running request's quantum in turn (its probe / monitor rows) and
+ *      queues that request's next quantum at once, each request on its own stream as a
+ *      replayed CUDA graph, so the device always holds the other requests' work while the
+ *      host handles one; a finished request goes to a worker, which closes its session,
+ *      copies the final state to the host when results are kept and frees its device
+ *      memory, after which its budget returns.
+ * Requests that arrive while others run join as soon as they are set up (continuous
+ * batching).  A request's result does not depend on what else is running: every solver has
+ * its own state, rand() stream and tiles (one autotuning per grid shape, shared), and the
+ * device loop's results do not depend on how its steps are chunked.
  */
-#define _POSIX_C_SOURCE 199309L
+#define _POSIX_C_SOURCE 200809L
+#include <errno.h>
+#include <pthread.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -25,11 +31,21 @@
 
 #include "les_serve.h"
 
+/* Where a request is in its life; phases PREP and FIN belong to a set-up worker. */
+enum {
+    PH_NONE = 0,      /* queued, or retired: holds no budget */
+    PH_PREP = 1,      /* budget reserved, handed to a worker for set-up */
+    PH_READY = 2,     /* set-up done (job_rc) */
+    PH_RUN = 3,       /* stepping on the device */
+    PH_FIN = 4,       /* handed to a worker for loop end, result copy and release */
+    PH_FINISHED = 5   /* that done (job_rc, t_done) */
+};
+
 typedef struct serve_req {
     long long id;
     lesgpu_config cfg;
     int nsteps, done_steps;
-    int state;
+    int state;                    /* LES_REQ_* as the caller sees it */
     int err;
     double t_submit, t_admit, t_done;
     size_t bytes;
@@ -37,27 +53,41 @@ typedef struct serve_req {
     double* result;               /* 11 fields x cells, host, when results are kept */
     char out_dir[1024];
     int out_flags;
+    int phase;                    /* PH_*; changed under the server mutex */
+    int job_rc;
+    int inflight;                 /* steps queued on the device and not yet collected */
+    size_t dev_bytes;             /* device bytes of the solver when it started */
+    struct serve_req* next_job;
 } serve_req;
 
 typedef struct tile_entry {
     int nx, ny, nz, precision;
     int tiles[5];
     int staged;                   /* scalar pass through the staged (TMA) kernel */
+    int ready;                    /* 0 being tuned, 1 filled, -1 tuning failed */
 } tile_entry;
 
 struct les_serve {
     les_serve_options opt;
-    size_t in_use;
+    size_t in_use;                /* budget held by requests in phases PREP..FINISHED */
     serve_req** reqs;             /* every request ever submitted, index = id */
     long long n, cap;
     long long head;               /* first request still queued or active */
-    int n_active;
+    int n_slots;                  /* requests holding budget */
+    int n_active;                 /* requests in state LES_REQ_ACTIVE */
     long long n_done, n_failed, n_cancelled;
     double cell_steps;
     double t_first_admit, t_last_done;
     tile_entry tiles[64];
     int n_tiles;
     char err[256];
+    /* set-up / tear-down workers and their job queue */
+    pthread_mutex_t mu;
+    pthread_cond_t cv_job, cv_done;
+    pthread_t* th;
+    int n_th;
+    int stop;
+    serve_req *jq_head, *jq_tail;
 };
 
 static double now_s(void) {
@@ -94,16 +124,174 @@ void les_serve_default_options(les_serve_options* o) {
     o->autotune = 0;
     o->backfill = 0;
     o->device = 0;
+    o->prep_threads = 4;
 }
+
+/* ------------------------------------------------------------------ worker jobs */
+
+static const tile_entry* find_tiles(les_serve* s, const lesgpu_config* c) {
+    for (int q = 0; q < s->n_tiles; q++) {
+        const tile_entry* t = &s->tiles[q];
+        if (t->nx == c->nx && t->ny == c->ny && t->nz == c->nz && t->precision == c->precision) return t;
+    }
+    return NULL;
+}
+
+/* One autotuning per grid shape and precision; later requests of that shape (also those set
+   up meanwhile by other workers, which wait for it) get the same tiles and scalar-pass form,
+   so a result does not depend on arrival order. */
+static int tiles_for(les_serve* s, serve_req* q, lesgpu_ctx* ctx) {
+    pthread_mutex_lock(&s->mu);
+    const tile_entry* t = find_tiles(s, &q->cfg);
+    while (t && t->ready == 0) {
+        pthread_cond_wait(&s->cv_done, &s->mu);
+        t = find_tiles(s, &q->cfg);
+    }
+    if (t && t->ready == 1) {
+        tile_entry c = *t;
+        pthread_mutex_unlock(&s->mu);
+        int rc = lesgpu_set_tiles(ctx, c.tiles);
+        if (rc == LESGPU_OK) rc = lesgpu_set_scalar_staging(ctx, c.staged);
+        return rc;
+    }
+    tile_entry* e = NULL;
+    if (!t && s->n_tiles < 64) {
+        e = &s->tiles[s->n_tiles++];
+        e->nx = q->cfg.nx; e->ny = q->cfg.ny; e->nz = q->cfg.nz; e->precision = q->cfg.precision;
+        e->ready = 0;
+    }
+    pthread_mutex_unlock(&s->mu);
+    int tl[5];
+    int rc = lesgpu_autotune(ctx, 3, tl, NULL);
+    if (e) {
+        pthread_mutex_lock(&s->mu);
+        if (rc == LESGPU_OK) {
+            memcpy(e->tiles, tl, sizeof(tl));
+            e->staged = lesgpu_get_scalar_staging(ctx);
+            e->ready = 1;
+        } else {
+            e->ready = -1;
+        }
+        pthread_cond_broadcast(&s->cv_done);
+        pthread_mutex_unlock(&s->mu);
+    }
+    return rc;
+}
+
+/* Set-up of an admitted request: solver (initial state, device arena), tiles, output
+   files, device-loop session. */
+static int job_prepare(les_serve* s, serve_req* q) {
+    les_solver* sol = NULL;
+    int rc = les_solver_create(&q->cfg, s->opt.chem_path, s->opt.tran_path, 0, &sol);
+    if (rc) return rc;
+    if (s->opt.autotune) rc = tiles_for(s, q, les_solver_ctx(sol));
+    if (rc == LESGPU_OK && q->out_dir[0]) rc = les_solver_set_outputs(sol, q->out_dir, q->out_flags);
+    if (rc == LESGPU_OK) rc = les_solver_loop_begin(sol, s->opt.quantum_steps);
+    if (rc) {
+        les_solver_destroy(sol);
+        return rc;
+    }
+    q->sol = sol;
+    return LESGPU_OK;
+}
+
+/* End of a finished request: close the loop session (files flushed), copy the final state
+   to the host when results are kept, release the solver and its device memory. */
+static int job_finish(les_serve* s, serve_req* q) {
+    int rc = les_solver_loop_end(q->sol);
+    if (rc == LESGPU_OK && s->opt.keep_results) {
+        const size_t n = (size_t)q->cfg.nx * q->cfg.ny * q->cfg.nz;
+        q->result = (double*)malloc(LESGPU_NSTATE * n * sizeof(double));
+        if (!q->result) {
+            rc = LESGPU_ENOMEM;
+        } else {
+            double* f[LESGPU_NSTATE];
+            for (int k = 0; k < LESGPU_NSTATE; k++) f[k] = q->result + (size_t)k * n;
+            rc = lesgpu_download_state(les_solver_ctx(q->sol), f, LESGPU_NSTATE);
+        }
+    }
+    les_solver_destroy(q->sol);
+    q->sol = NULL;
+    return rc;
+}
+
+static void run_job(les_serve* s, serve_req* q, int phase) {
+    int rc = (phase == PH_PREP) ? job_prepare(s, q) : job_finish(s, q);
+    pthread_mutex_lock(&s->mu);
+    q->job_rc = rc;
+    if (phase == PH_FIN) q->t_done = now_s();
+    q->phase = (phase == PH_PREP) ? PH_READY : PH_FINISHED;
+    pthread_cond_broadcast(&s->cv_done);
+    pthread_mutex_unlock(&s->mu);
+}
+
+static void* worker_main(void* arg) {
+    les_serve* s = (les_serve*)arg;
+    /* CUDA's current device is per host thread */
+    lesgpu_bind_device(s->opt.device);
+    pthread_mutex_lock(&s->mu);
+    for (;;) {
+        while (!s->stop && !s->jq_head) pthread_cond_wait(&s->cv_job, &s->mu);
+        if (!s->jq_head) break;                    /* stopping with the queue drained */
+        serve_req* q = s->jq_head;
+        s->jq_head = q->next_job;
+        if (!s->jq_head) s->jq_tail = NULL;
+        q->next_job = NULL;
+        const int phase = q->phase;
+        pthread_mutex_unlock(&s->mu);
+        run_job(s, q, phase);
+        pthread_mutex_lock(&s->mu);
+    }
+    pthread_mutex_unlock(&s->mu);
+    return NULL;
+}
+
+/* Move q into PREP or FIN and have it done: by a worker, or here when the server has none. */
+static void hand_out(les_serve* s, serve_req* q, int phase) {
+    pthread_mutex_lock(&s->mu);
+    q->phase = phase;
+    if (s->n_th > 0) {
+        q->next_job = NULL;
+        if (s->jq_tail) s->jq_tail->next_job = q;
+        else s->jq_head = q;
+        s->jq_tail = q;
+        pthread_cond_signal(&s->cv_job);
+        pthread_mutex_unlock(&s->mu);
+        return;
+    }
+    pthread_mutex_unlock(&s->mu);
+    run_job(s, q, phase);
+}
+
+/* ------------------------------------------------------------------ server */
 
 int les_serve_create(const les_serve_options* opt, les_serve** out) {
     if (!opt || !out || opt->max_slots < 1 || opt->quantum_steps < 1 || opt->budget_bytes == 0) return LESGPU_EINVAL;
     if (!opt->chem_path[0] || !opt->tran_path[0]) return LESGPU_EINVAL;
+    if (opt->prep_threads < 0 || opt->prep_threads > 64) return LESGPU_EINVAL;
     *out = NULL;
     les_serve* s = (les_serve*)calloc(1, sizeof(les_serve));
     if (!s) return LESGPU_ENOMEM;
     s->opt = *opt;
     s->t_first_admit = -1.0;
+    pthread_mutex_init(&s->mu, NULL);
+    pthread_cond_init(&s->cv_job, NULL);
+    pthread_cond_init(&s->cv_done, NULL);
+    if (opt->prep_threads > 0) {
+        s->th = (pthread_t*)calloc((size_t)opt->prep_threads, sizeof(pthread_t));
+        if (!s->th) {
+            les_serve_destroy(s);
+            return LESGPU_ENOMEM;
+        }
+        for (int t = 0; t < opt->prep_threads; t++) {
+            if (pthread_create(&s->th[t], NULL, worker_main, s) != 0) break;
+            s->n_th++;
+        }
+        if (s->n_th == 0) {
+            les_serve_destroy(s);
+            return LESGPU_ENOMEM;
+        }
+    }
     *out = s;
     return LESGPU_OK;
 }
@@ -135,6 +323,7 @@ int les_serve_submit(les_serve* s, const lesgpu_config* cfg, int nsteps, const c
     q->cfg = *cfg;
     q->nsteps = nsteps;
     q->state = LES_REQ_QUEUED;
+    q->phase = PH_NONE;
     q->t_submit = now_s();
     q->bytes = need;
     if (out_dir) snprintf(q->out_dir, sizeof(q->out_dir), "%s", out_dir);
@@ -144,21 +333,27 @@ int les_serve_submit(les_serve* s, const lesgpu_config* cfg, int nsteps, const c
     return LESGPU_OK;
 }
 
+/* Final bookkeeping of a request no worker holds: its solver (if any) is destroyed and its
+   budget returned. */
 static void retire(les_serve* s, serve_req* q, int state, int err) {
     if (q->sol) {
         les_solver_destroy(q->sol);
         q->sol = NULL;
     }
-    if (q->state == LES_REQ_ACTIVE) {
+    pthread_mutex_lock(&s->mu);
+    if (q->phase != PH_NONE) {
         s->in_use -= q->bytes;
-        s->n_active--;
+        s->n_slots--;
     }
+    q->phase = PH_NONE;
+    pthread_mutex_unlock(&s->mu);
+    if (q->state == LES_REQ_ACTIVE) s->n_active--;
     q->state = state;
     q->err = err;
-    q->t_done = now_s();
+    if (state != LES_REQ_DONE) q->t_done = now_s();
     if (state == LES_REQ_DONE) {
         s->n_done++;
-        s->t_last_done = q->t_done;
+        if (q->t_done > s->t_last_done) s->t_last_done = q->t_done;
     } else if (state == LES_REQ_CANCELLED) {
         s->n_cancelled++;
     } else {
@@ -166,142 +361,170 @@ static void retire(les_serve* s, serve_req* q, int state, int err) {
     }
 }
 
+static int phase_of(les_serve* s, serve_req* q) {
+    pthread_mutex_lock(&s->mu);
+    int p = q->phase;
+    pthread_mutex_unlock(&s->mu);
+    return p;
+}
+
+/* Wait until no worker holds q. */
+static void wait_idle(les_serve* s, serve_req* q) {
+    pthread_mutex_lock(&s->mu);
+    while (q->phase == PH_PREP || q->phase == PH_FIN) pthread_cond_wait(&s->cv_done, &s->mu);
+    pthread_mutex_unlock(&s->mu);
+}
+
 int les_serve_cancel(les_serve* s, long long id) {
     serve_req* q = find(s, id);
     if (!q) return LESGPU_EINVAL;
     if (q->state != LES_REQ_QUEUED && q->state != LES_REQ_ACTIVE) return LESGPU_ESTATE;
-    /* between rounds no step of an active request is in flight (collect waited for it) */
+    wait_idle(s, q);
+    const int ph = phase_of(s, q);
+    if (ph == PH_FINISHED) return serr(s, LESGPU_ESTATE, "request has already finished");
+    if (ph == PH_RUN && q->inflight > 0) {
+        /* let the steps already queued end before the solver is released */
+        (void)les_solver_loop_collect(q->sol, q->inflight);
+        q->inflight = 0;
+    }
     retire(s, q, LES_REQ_CANCELLED, 0);
     return LESGPU_OK;
 }
 
-static const tile_entry* cached_tiles(les_serve* s, const lesgpu_config* c) {
-    for (int q = 0; q < s->n_tiles; q++) {
-        const tile_entry* t = &s->tiles[q];
-        if (t->nx == c->nx && t->ny == c->ny && t->nz == c->nz && t->precision == c->precision) return t;
+/* Queue the next quantum of a running request. */
+static void launch(les_serve* s, serve_req* q) {
+    int n = les_solver_next_chunk(q->sol, q->nsteps - q->done_steps);
+    int rc = (n > 0) ? lesgpu_run(les_solver_ctx(q->sol), n) : LESGPU_ESTATE;
+    if (rc) {
+        retire(s, q, LES_REQ_FAILED, rc);
+        return;
     }
-    return NULL;
+    q->inflight = n;
 }
 
-static int admit(les_serve* s, serve_req* q) {
-    int rc = les_solver_create(&q->cfg, s->opt.chem_path, s->opt.tran_path, 0, &q->sol);
-    if (rc) return rc;
-    lesgpu_ctx* ctx = les_solver_ctx(q->sol);
-    if (s->opt.autotune) {
-        /* one autotuning per grid shape and precision; later requests of that shape get the
-           same tiles and scalar-pass form, so their results do not depend on arrival order */
-        const tile_entry* t = cached_tiles(s, &q->cfg);
-        if (t) {
-            rc = lesgpu_set_tiles(ctx, t->tiles);
-            if (rc == LESGPU_OK) rc = lesgpu_set_scalar_staging(ctx, t->staged);
-        } else {
-            int tl[5];
-            rc = lesgpu_autotune(ctx, 3, tl, NULL);
-            if (rc == LESGPU_OK && s->n_tiles < 64) {
-                tile_entry* e = &s->tiles[s->n_tiles++];
-                e->nx = q->cfg.nx; e->ny = q->cfg.ny; e->nz = q->cfg.nz; e->precision = q->cfg.precision;
-                memcpy(e->tiles, tl, sizeof(tl));
-                e->staged = lesgpu_get_scalar_staging(ctx);
+/* Requests whose worker job ended: set-up done -> running (first quantum queued at once),
+   tear-down done -> done. */
+static void harvest(les_serve* s) {
+    for (long long i = s->head; i < s->n; i++) {
+        serve_req* q = s->reqs[i];
+        if (q->state != LES_REQ_QUEUED && q->state != LES_REQ_ACTIVE) continue;
+        const int ph = phase_of(s, q);
+        if (ph == PH_READY) {
+            if (q->job_rc) {
+                retire(s, q, LES_REQ_FAILED, q->job_rc);
+                continue;
             }
+            pthread_mutex_lock(&s->mu);
+            q->phase = PH_RUN;
+            pthread_mutex_unlock(&s->mu);
+            q->state = LES_REQ_ACTIVE;
+            q->dev_bytes = lesgpu_device_bytes(les_solver_ctx(q->sol));
+            s->n_active++;
+            launch(s, q);
+        } else if (ph == PH_FINISHED) {
+            retire(s, q, q->job_rc ? LES_REQ_FAILED : LES_REQ_DONE, q->job_rc);
         }
     }
-    if (rc == LESGPU_OK && q->out_dir[0]) rc = les_solver_set_outputs(q->sol, q->out_dir, q->out_flags);
-    if (rc == LESGPU_OK) rc = les_solver_loop_begin(q->sol, s->opt.quantum_steps);
-    if (rc) {
-        les_solver_destroy(q->sol);
-        q->sol = NULL;
-        return rc;
-    }
-    q->state = LES_REQ_ACTIVE;
-    q->t_admit = now_s();
-    s->in_use += q->bytes;
-    s->n_active++;
-    if (s->t_first_admit < 0) s->t_first_admit = q->t_admit;
-    return LESGPU_OK;
 }
 
-static int finish(les_serve* s, serve_req* q) {
-    int rc = les_solver_loop_end(q->sol);
-    if (rc == LESGPU_OK && s->opt.keep_results) {
-        const size_t n = (size_t)q->cfg.nx * q->cfg.ny * q->cfg.nz;
-        q->result = (double*)malloc(LESGPU_NSTATE * n * sizeof(double));
-        if (!q->result) return LESGPU_ENOMEM;
-        double* f[LESGPU_NSTATE];
-        for (int k = 0; k < LESGPU_NSTATE; k++) f[k] = q->result + (size_t)k * n;
-        rc = lesgpu_download_state(les_solver_ctx(q->sol), f, LESGPU_NSTATE);
-    }
-    return rc;
-}
-
-static void admit_queued(les_serve* s) {
-    for (long long i = s->head; i < s->n && s->n_active < s->opt.max_slots; i++) {
+/* Reserve budget and a slot for queued requests in arrival order and hand them to the
+   set-up workers.  Returns how many were handed out. */
+static int admit_queued(les_serve* s) {
+    int k = 0;
+    for (long long i = s->head; i < s->n && s->n_slots < s->opt.max_slots; i++) {
         serve_req* q = s->reqs[i];
-        if (q->state != LES_REQ_QUEUED) continue;
+        if (q->state != LES_REQ_QUEUED || q->phase != PH_NONE) continue;
         if (s->in_use + q->bytes > s->opt.budget_bytes) {
             if (s->opt.backfill) continue;
             break;
         }
-        int rc = admit(s, q);
-        if (rc == LESGPU_ENOMEM && s->n_active > 0) break;   /* the device is fuller than budgeted: wait */
-        if (rc) retire(s, q, LES_REQ_FAILED, rc);
+        pthread_mutex_lock(&s->mu);
+        s->in_use += q->bytes;
+        s->n_slots++;
+        pthread_mutex_unlock(&s->mu);
+        q->t_admit = now_s();
+        if (s->t_first_admit < 0) s->t_first_admit = q->t_admit;
+        hand_out(s, q, PH_PREP);
+        k++;
     }
+    return k;
+}
+
+/* Wait for the next worker job to end, or until no job is pending. */
+static void wait_any_job(les_serve* s) {
+    pthread_mutex_lock(&s->mu);
+    for (;;) {
+        int busy = 0, ready = 0;
+        for (long long i = s->head; i < s->n; i++) {
+            const int p = s->reqs[i]->phase;
+            if (p == PH_PREP || p == PH_FIN) busy = 1;
+            if (p == PH_READY || p == PH_FINISHED) ready = 1;
+        }
+        if (ready || !busy) break;
+        pthread_cond_wait(&s->cv_done, &s->mu);
+    }
+    pthread_mutex_unlock(&s->mu);
+}
+
+static int count_running(les_serve* s) {
+    int r = 0;
+    for (long long i = s->head; i < s->n; i++) {
+        serve_req* q = s->reqs[i];
+        if (q->state == LES_REQ_ACTIVE && phase_of(s, q) == PH_RUN) r++;
+    }
+    return r;
 }
 
 int les_serve_step(les_serve* s) {
     if (!s) return LESGPU_EINVAL;
+    /* the workers create the contexts; this thread drives them on the server's device */
+    if (lesgpu_bind_device(s->opt.device) != LESGPU_OK) return serr(s, LESGPU_ECUDA, "cannot select the device");
     while (s->head < s->n && s->reqs[s->head]->state != LES_REQ_QUEUED && s->reqs[s->head]->state != LES_REQ_ACTIVE)
         s->head++;
-    /* with nothing running there is nothing to overlap: admit first */
-    const int admit_early = (s->n_active == 0);
-    if (admit_early) admit_queued(s);
-    /* 1. queue one quantum of every active request (asynchronous, one stream each) */
-    int* qn = NULL;
-    serve_req** act = NULL;
-    int na = 0;
-    const int cap_a = s->n_active;
-    if (cap_a > 0) {
-        qn = (int*)malloc((size_t)cap_a * sizeof(int));
-        act = (serve_req**)malloc((size_t)cap_a * sizeof(serve_req*));
-        if (!qn || !act) {
-            free(qn);
-            free(act);
-            return serr(s, LESGPU_ENOMEM, "round tables");
+    /* 1. results of set-up / tear-down jobs; newly running requests get their first quantum */
+    harvest(s);
+    /* 2. admission, in arrival order; set-up runs on the workers while the device steps */
+    admit_queued(s);
+    if (count_running(s) == 0) {
+        /* nothing on the device to overlap with: wait for every set-up in progress */
+        pthread_mutex_lock(&s->mu);
+        for (;;) {
+            int busy = 0;
+            for (long long i = s->head; i < s->n; i++)
+                if (s->reqs[i]->phase == PH_PREP) busy = 1;
+            if (!busy) break;
+            pthread_cond_wait(&s->cv_done, &s->mu);
         }
-        for (long long i = s->head; i < s->n && na < cap_a; i++) {
-            serve_req* q = s->reqs[i];
-            if (q->state != LES_REQ_ACTIVE) continue;
-            int left = q->nsteps - q->done_steps;
-            int n = les_solver_next_chunk(q->sol, left);
-            int rc = (n > 0) ? lesgpu_run(les_solver_ctx(q->sol), n) : LESGPU_ESTATE;
-            if (rc) {
-                retire(s, q, LES_REQ_FAILED, rc);
-                continue;
-            }
-            act[na] = q;
-            qn[na] = n;
-            na++;
-        }
+        pthread_mutex_unlock(&s->mu);
+        harvest(s);
     }
-    /* 2. admission, in arrival order, while the quanta just queued run on the device (the
-     *    host-side set-up of a new request overlaps them); new requests join next round */
-    if (!admit_early) admit_queued(s);
-    /* 3. collect histories and retire finished requests */
-    for (int a = 0; a < na; a++) {
-        serve_req* q = act[a];
-        int rc = les_solver_loop_collect(q->sol, qn[a]);
+    /* 3. collect every running request's quantum in turn; the next quantum of a request is
+     *    queued as soon as its last one is collected, so the device keeps the other
+     *    requests' work while the host handles one */
+    for (long long i = s->head; i < s->n; i++) {
+        serve_req* q = s->reqs[i];
+        if (q->state != LES_REQ_ACTIVE || phase_of(s, q) != PH_RUN) continue;
+        if (q->inflight == 0) {
+            launch(s, q);
+            if (q->state != LES_REQ_ACTIVE) continue;
+        }
+        const int n = q->inflight;
+        int rc = les_solver_loop_collect(q->sol, n);
+        q->inflight = 0;
         if (rc) {
             retire(s, q, LES_REQ_FAILED, rc);
             continue;
         }
-        q->done_steps += qn[a];
-        s->cell_steps += (double)qn[a] * (double)q->cfg.nx * q->cfg.ny * q->cfg.nz;
-        if (q->done_steps >= q->nsteps) {
-            rc = finish(s, q);
-            retire(s, q, rc ? LES_REQ_FAILED : LES_REQ_DONE, rc);
-        }
+        q->done_steps += n;
+        s->cell_steps += (double)n * (double)q->cfg.nx * q->cfg.ny * q->cfg.nz;
+        if (q->done_steps >= q->nsteps) hand_out(s, q, PH_FIN);
+        else launch(s, q);
     }
-    free(qn);
-    free(act);
+    /* 4. with nothing left on the device, wait for a worker instead of returning at once */
+    if (count_running(s) == 0) {
+        wait_any_job(s);
+        harvest(s);
+    }
     long long pending = 0;
     for (long long i = s->head; i < s->n; i++)
         if (s->reqs[i]->state == LES_REQ_QUEUED || s->reqs[i]->state == LES_REQ_ACTIVE) pending++;
@@ -316,7 +539,7 @@ int les_serve_info(les_serve* s, long long id, les_serve_request_info* info) {
     info->steps_done = q->done_steps;
     info->nsteps = q->nsteps;
     info->bytes = q->bytes;
-    info->device_bytes = q->sol ? lesgpu_device_bytes(les_solver_ctx(q->sol)) : 0;
+    info->device_bytes = (q->state == LES_REQ_ACTIVE) ? q->dev_bytes : 0;
     info->t_submit = q->t_submit;
     info->t_admit = q->t_admit;
     info->t_done = q->t_done;
@@ -365,7 +588,9 @@ int les_serve_stats(les_serve* s, les_serve_summary* st) {
     st->failed = s->n_failed;
     st->cancelled = s->n_cancelled;
     st->active = s->n_active;
+    pthread_mutex_lock(&s->mu);
     st->bytes_in_use = s->in_use;
+    pthread_mutex_unlock(&s->mu);
     st->cell_steps = s->cell_steps;
     for (long long i = 0; i < s->n; i++)
         if (s->reqs[i]->state == LES_REQ_QUEUED) st->queued++;
@@ -388,6 +613,13 @@ const char* les_serve_last_error(const les_serve* s) { return s ? s->err : "null
 
 void les_serve_destroy(les_serve* s) {
     if (!s) return;
+    /* the workers end the jobs they hold or have queued, then exit */
+    pthread_mutex_lock(&s->mu);
+    s->stop = 1;
+    pthread_cond_broadcast(&s->cv_job);
+    pthread_mutex_unlock(&s->mu);
+    for (int t = 0; t < s->n_th; t++) pthread_join(s->th[t], NULL);
+    free(s->th);
     for (long long i = 0; i < s->n; i++) {
         serve_req* q = s->reqs[i];
         if (q->sol) les_solver_destroy(q->sol);
@@ -395,5 +627,8 @@ void les_serve_destroy(les_serve* s) {
         free(q);
     }
     free(s->reqs);
+    pthread_cond_destroy(&s->cv_job);
+    pthread_cond_destroy(&s->cv_done);
+    pthread_mutex_destroy(&s->mu);
     free(s);
 }

@@ -30,7 +30,7 @@ STATE_NAMES = {QUEUED: "queued", ACTIVE: "active", DONE: "done", CANCELLED: "can
 class ServeOptions(C.Structure):
     _fields_ = [("budget_bytes", C.c_size_t), ("max_slots", C.c_int), ("quantum_steps", C.c_int),
                 ("keep_results", C.c_int), ("autotune", C.c_int), ("backfill", C.c_int), ("device", C.c_int),
-                ("chem_path", C.c_char * 1024), ("tran_path", C.c_char * 1024)]
+                ("chem_path", C.c_char * 1024), ("tran_path", C.c_char * 1024), ("prep_threads", C.c_int)]
 
 
 class RequestInfo(C.Structure):
@@ -77,13 +77,15 @@ def request_bytes(cfg: SolverConfig, precision: int = N.FP32, quantum: int = 16)
 class Server:
     def __init__(self, budget_bytes: int = 150 * 10**9, max_slots: int = 64, quantum: int = 16,
                  keep_results: bool = True, autotune: bool = False, backfill: bool = False, device: int = 0,
-                 chem: str = N.CHEM_BIN, tran: str = N.TRAN_BIN):
+                 chem: str = N.CHEM_BIN, tran: str = N.TRAN_BIN, prep_threads: Optional[int] = None):
         L = _lib()
         o = ServeOptions()
         L.les_serve_default_options(C.byref(o))
         o.budget_bytes, o.max_slots, o.quantum_steps = int(budget_bytes), max_slots, quantum
         o.keep_results, o.autotune, o.backfill, o.device = int(keep_results), int(autotune), int(backfill), device
         o.chem_path, o.tran_path = chem.encode(), tran.encode()
+        if prep_threads is not None:
+            o.prep_threads = prep_threads
         h = C.c_void_p()
         rc = L.les_serve_create(C.byref(o), C.byref(h))
         if rc:

@@ -269,6 +269,12 @@ int lesgpu_get_scalar_staging(const lesgpu_ctx* ctx);
 /* Block until all work queued on the context's stream has finished. */
 int lesgpu_sync(lesgpu_ctx* ctx);
 
+/* No counterpart in the reference (one host thread).  Make `device` the calling host
+ * thread's current CUDA device.  lesgpu_create selects the configured device for the thread
+ * that calls it; the other calls use the calling thread's current device, so a thread that
+ * drives contexts created by another thread calls this first. */
+int lesgpu_bind_device(int device);
+
 /* Bytes of device memory the context holds (for admission by memory budget). */
 size_t lesgpu_device_bytes(const lesgpu_ctx* ctx);
 size_t lesgpu_bytes_for_grid(int nx, int ny, int nz, int precision);

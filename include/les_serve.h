@@ -5,17 +5,23 @@
  * No counterpart in the reference, which runs one solve per process (main(),
  * les_combustion_solver.c:4016-4632).  Each request is one les_solver (les_solver.h) with
  * its own grid, model constants, seed, rand() stream and output files; its results are the
- * same as running it alone with les_solver_run_device.  One host thread drives a server.
+ * same as running it alone with les_solver_run_device.  One host thread calls a server;
+ * the server keeps prep_threads worker threads of its own for the per-request set-up and
+ * tear-down (solver creation with its initial state and uploads, the final state's copy to
+ * the host, releasing device memory), so that host work overlaps the device's.
  *
  *   les_serve_submit   queue a request (refused at once if it can never fit the budget);
  *   les_serve_step     one scheduling round: admit queued requests in arrival order while a
- *                      slot is free and their memory fits, queue up to quantum_steps steps
- *                      of every active request (one stream and graph each, overlapping on
- *                      the device), collect their step histories, retire finished ones
- *                      (final state copied to the host when results are kept, device
- *                      memory returned at once).  Returns the number of requests still
- *                      queued or active (>= 0) or a negative LESGPU_E* code;
- *   les_serve_cancel   drop a queued or active request between rounds;
+ *                      slot is free and their memory fits (their set-up goes to the
+ *                      workers; with nothing running the round waits for it), start
+ *                      requests whose set-up is done, and collect the step history of every
+ *                      running request in turn, queueing its next quantum_steps steps (one
+ *                      stream and graph per request, overlapping on the device) as soon as
+ *                      the last ones are collected; finished requests go to the workers and
+ *                      are retired when their final state is on the host and their device
+ *                      memory returned.  Returns the number of requests still queued or
+ *                      active (>= 0) or a negative LESGPU_E* code;
+ *   les_serve_cancel   drop a queued or active request (waits for its steps in flight);
  *   les_serve_info / les_serve_result / les_serve_release / les_serve_stats.
  * Latency is completion time minus submission time (CLOCK_MONOTONIC); p50/p99 use linear
  * interpolation between order statistics.
@@ -43,12 +49,15 @@ typedef struct les_serve_options {
     int device;
     char chem_path[1024];
     char tran_path[1024];
+    int prep_threads;         /* host threads that set up and tear down requests (0: the
+                                 thread calling les_serve_step does it) */
 } les_serve_options;
 
 typedef struct les_serve_request_info {
     int state, error, steps_done, nsteps;
     size_t bytes;             /* budgeted bytes */
-    size_t device_bytes;      /* bytes the solver holds (active requests) */
+    size_t device_bytes;      /* device bytes of the request's solver, from its start until
+                                 the request is retired (0 otherwise) */
     double t_submit, t_admit, t_done, latency_s;
 } les_serve_request_info;
 

@@ -1,7 +1,8 @@
 """Serving loop on the GPU: a request's result is the same alone and in a mix of other
 requests arriving while it runs (bit-identical: each request has its own state, rand()
-stream and tiles, and the device loop does not depend on chunking), admission never
-exceeds the HBM budget, and cancellation frees the request's memory."""
+stream and tiles, and the device loop does not depend on chunking), whether requests are set
+up by the stepping thread or by the server's workers; admission never exceeds the HBM
+budget, and cancellation frees the request's memory."""
 import numpy as np
 import pytest
 
@@ -31,14 +32,15 @@ def test_result_same_alone_and_in_the_mix(N, S, prec):
     from lesgpu.config import preset
     P = N.FP32 if prec == "fp32" else N.FP64
     target = preset("small", seed=91, cs_unburned=0.12, relax=3000.0)
-    alone = S.Server(quantum=7)
+    # alone: set-up on the stepping thread; in the mix: on the server's worker threads
+    alone = S.Server(quantum=7, prep_threads=0)
     rid = alone.submit(target, 23, P)
     alone.drain()
     assert alone.info(rid)["state_name"] == "done"
     r_alone = alone.result(rid)
     alone.close()
 
-    mix = S.Server(quantum=5, max_slots=3)
+    mix = S.Server(quantum=5, max_slots=3, prep_threads=3)
     others = [mix.submit(preset("tiny", seed=5), 40, P), mix.submit(preset("c1", seed=6, accel_strength=1.0), 12, P)]
     mix.step()
     mix.step()
