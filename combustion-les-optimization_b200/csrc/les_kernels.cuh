@@ -99,23 +99,24 @@ struct MinBlocks<float> {
 
 // ---------------------------------------------------------------------------- helpers
 
-// Scalar-pass prefetch of its streaming operands: 0 off, 1 into L2, 2 into L1.  Measured at
-// 256x128x128 on B200: FP64 3.18 -> 3.07 ms per step (L1 and L2 alike); FP32 1.73 -> 2.01 ms
-// (the addresses cost registers at 6 blocks per SM), so FP32 leaves it off.
-#ifndef LES_SCALAR_PREFETCH_F64
-#define LES_SCALAR_PREFETCH_F64 1
+// The scalar pass reads Phi_n, the RK running sum, the flow pass's right-hand sides and the
+// diffusivities once per stage and writes the running sum back for the next stage only:
+// these go through ld.global.cs / st.global.cs (evict first), so they do not push the
+// stencil fields' halo planes out of L2.  Measured at 256x128x128 on B200: DRAM traffic of
+// the FP64 scalar pass 414-494 B/cell per launch (plain loads 479-531; with an L2 prefetch
+// of these operands 530-622 at 3 % less time); FP32 scalar pass 1.73 -> 1.66 ms per step.
+#ifndef LES_SCALAR_STREAM
+#define LES_SCALAR_STREAM 1
 #endif
-#ifndef LES_SCALAR_PREFETCH_F32
-#define LES_SCALAR_PREFETCH_F32 0
-#endif
-template <typename R>
-struct ScalarPrefetch {
-    static constexpr int level = std::is_same<R, float>::value ? LES_SCALAR_PREFETCH_F32 : LES_SCALAR_PREFETCH_F64;
-};
-template <int Level>
-__device__ __forceinline__ void prefetch_line(const void* p) {
-    if constexpr (Level == 1) asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
-    else if constexpr (Level == 2) asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+template <typename T>
+__device__ __forceinline__ T ld_stream(const T* p) {
+    if constexpr (LES_SCALAR_STREAM != 0) return __ldcs(p);
+    else return *p;
+}
+template <typename T>
+__device__ __forceinline__ void st_stream(T* p, T v) {
+    if constexpr (LES_SCALAR_STREAM != 0) __stcs(p, v);
+    else *p = v;
 }
 
 template <typename R>
@@ -913,23 +914,6 @@ __device__ __forceinline__ void rhs_scalar_cell(const Consts& C, const uint8_t* 
         return;
     }
 
-    if constexpr (ScalarPrefetch<R>::level != 0) {
-        // The RK bookkeeping at the end reads Phi_n, the running sum and the flow pass's
-        // right-hand sides; none depends on the stencil work, so their lines are requested
-        // now and are on chip by the time they are read.
-        constexpr int L = ScalarPrefetch<R>::level;
-#pragma unroll
-        for (int q = 0; q < NSTATE; q++) prefetch_line<L>(S0.p[q] + id);
-        if (stage > 0) {
-#pragma unroll
-            for (int q = 0; q < NACC; q++) prefetch_line<L>(acc.p[q] + id);
-        }
-#pragma unroll
-        for (int q = 0; q < 4; q++) prefetch_line<L>(kf.p[q] + id);
-#pragma unroll
-        for (int s = 0; s < NSP; s++) prefetch_line<L>(P.D[s] + id);
-        prefetch_line<L>(P.aT + id);
-    }
     const R u0 = F.p[0][id], v0 = F.p[1][id], w0 = F.p[2][id];
     const bool band2 = (i < 2 || i >= nx - 2 || j < 2 || j >= ny - 2 || k < 2 || k >= nz - 2);
     R kv[NACC];
@@ -942,7 +926,7 @@ __device__ __forceinline__ void rhs_scalar_cell(const Consts& C, const uint8_t* 
     for (int s = 0; s < NSP; s++) {
         const auto qY = src.y(s);
         R conv = conv_muscl<R>(C, qY, band2, u0, v0, w0);
-        R mol = P.D[s][id] * lap3<R>(C, qY);
+        R mol = ld_stream(P.D[s] + id) * lap3<R>(C, qY);
         R sgs = sgs_div<R>(C, qY, gs);
         R tgt;
         if (s == C3H8) tgt = (R)K.inletYk[C3H8] * (R(1.0) - g);
@@ -956,17 +940,17 @@ __device__ __forceinline__ void rhs_scalar_cell(const Consts& C, const uint8_t* 
     {
         const auto qT = src.t();
         R conv = conv_muscl<R>(C, qT, band2, u0, v0, w0);
-        R mol = P.aT[id] * lap3<R>(C, qT);
+        R mol = ld_stream(P.aT + id) * lap3<R>(C, qT);
         const SgsFaces<R> gt = sgs_faces<R>(src.nu(), K.d_prt2);
         R sgs = sgs_div<R>(C, qT, gt);
         R Tt = (R)K.t_in + g * (R)K.t_burnt_span;
         R nud = relax * (Tt - qT(0, 0, 0));
         kv[3] = -conv + mol + sgs + nud;
     }
-    kv[0] = kf.p[0][id];
-    kv[1] = kf.p[1][id];
-    kv[2] = kf.p[2][id];
-    kv[4] = kf.p[3][id];
+    kv[0] = ld_stream(kf.p[0] + id);
+    kv[1] = ld_stream(kf.p[1] + id);
+    kv[2] = ld_stream(kf.p[2] + id);
+    kv[4] = ld_stream(kf.p[3] + id);
     if (kd.p[0]) {
         kd.p[3][id] = kv[3];
 #pragma unroll
@@ -980,24 +964,24 @@ __device__ __forceinline__ void rhs_scalar_cell(const Consts& C, const uint8_t* 
     R incr[NACC];
     if (stage == 0) {
 #pragma unroll
-        for (int q = 0; q < NACC; q++) { incr[q] = kv[q]; acc.p[q][id] = kv[q]; }
+        for (int q = 0; q < NACC; q++) { incr[q] = kv[q]; st_stream(acc.p[q] + id, kv[q]); }
     } else if (stage < 3) {
 #pragma unroll
-        for (int q = 0; q < NACC; q++) { incr[q] = kv[q]; acc.p[q][id] = acc.p[q][id] + R(2.0) * kv[q]; }
+        for (int q = 0; q < NACC; q++) { incr[q] = kv[q]; st_stream(acc.p[q] + id, ld_stream(acc.p[q] + id) + R(2.0) * kv[q]); }
     } else {
 #pragma unroll
-        for (int q = 0; q < NACC; q++) incr[q] = acc.p[q][id] + kv[q];
+        for (int q = 0; q < NACC; q++) incr[q] = ld_stream(acc.p[q] + id) + kv[q];
     }
     // The update itself runs in the state's type: in the FP32 form the right-hand sides are
     // FP32 and Phi_n, the stage update and the final combine FP64, so increments far below
     // the state's FP32 ulp are not rounded away step after step.
     const RS cdt = fin ? (RS)(dt / 6.0) : (RS)((stage == 2 ? 1.0 : 0.5) * dt);
-    const RS rho_n = S0.p[5][id];
-    RS Tn = S0.p[3][id] + cdt * (RS)incr[3];
-    RS Gn = S0.p[4][id] + cdt * (RS)incr[4];
+    const RS rho_n = ld_stream(S0.p[5] + id);
+    RS Tn = ld_stream(S0.p[3] + id) + cdt * (RS)incr[3];
+    RS Gn = ld_stream(S0.p[4] + id) + cdt * (RS)incr[4];
     RS Y[NSP];
 #pragma unroll
-    for (int s = 0; s < NSP; s++) Y[s] = S0.p[6 + s][id] + cdt * (RS)incr[5 + s];
+    for (int s = 0; s < NSP; s++) Y[s] = ld_stream(S0.p[6 + s] + id) + cdt * (RS)incr[5 + s];
     Tn = fmax(RS(200.0), fmin(RS(3000.0), Tn));
     Gn = fmax(RS(0.0), fmin(RS(1.0), Gn));
     RS sy = RS(0);
@@ -1014,7 +998,7 @@ __device__ __forceinline__ void rhs_scalar_cell(const Consts& C, const uint8_t* 
     RS vel[3];
 #pragma unroll
     for (int q = 0; q < 3; q++) {
-        RS m = rho_n * S0.p[q][id] + cdt * (RS)incr[q];   // rhou = rho*u after the BC (:3146)
+        RS m = rho_n * ld_stream(S0.p[q] + id) + cdt * (RS)incr[q];   // rhou = rho*u after the BC (:3146)
         vel[q] = (rn > RS(SMALL)) ? sdiv<R>(m, rn) : RS(0);
     }
     if (fin) {

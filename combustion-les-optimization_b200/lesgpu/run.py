@@ -1,6 +1,6 @@
 """Run a named case for a few steps and report per-kernel-class device times.
 
-    python -m lesgpu.run --workload c2 --precision fp64 --steps 4 [--tiles auto|default]
+    python -m lesgpu.run --workload c2 --precision fp64 --steps 4 [--tiles auto|default|f,s,fl,sc,e]
                          [--loop host|device] [--kernel-times] [--outputs DIR]
 
 The case starts from the reference's initial state (les_solver_create).  With
@@ -25,7 +25,8 @@ def main(argv=None) -> int:
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--warmup", type=int, default=2)
-    ap.add_argument("--tiles", choices=["auto", "default"], default="default")
+    ap.add_argument("--tiles", default="default",
+                    help="auto, default, or five tile-shape indices (filter,strain,flow,scalar,eos), e.g. 0,1,2,5,0")
     ap.add_argument("--loop", choices=["host", "device"], default="host")
     ap.add_argument("--kernel-times", action="store_true")
     ap.add_argument("--outputs", default=None)
@@ -37,6 +38,9 @@ def main(argv=None) -> int:
     if a.tiles == "auto":
         tiles, ms = s.ctx.autotune(3)
         out["tiles"] = tiles
+    elif a.tiles != "default":
+        s.ctx.set_tiles([int(t) for t in a.tiles.split(",")])
+        out["tiles"] = s.ctx.get_tiles()
     if a.outputs:
         s.set_outputs(a.outputs, N.LES_OUT_PROBES | N.LES_OUT_MONITOR)
     run = (lambda n: s.run_device(n, chunk=max(n, 1))) if a.loop == "device" else s.step
