@@ -46,7 +46,24 @@ int les_ensemble_create(const lesgpu_config* cfgs, int n, const char* chem_path,
     e->n = n;
     for (int q = 0; q < n; q++) {
         int rc = les_solver_create(&cfgs[q], chem_path, tran_path, 0, &e->members[q]);
-        if (rc == LESGPU_OK && autotune) rc = lesgpu_autotune(les_solver_ctx(e->members[q]), 3, NULL, NULL);
+        if (rc == LESGPU_OK && autotune) {
+            /* tiles are tuned on the first member of each grid shape and precision and reused
+               by the others, so members of one shape run the same kernels */
+            int p = 0;
+            while (p < q && !(cfgs[p].nx == cfgs[q].nx && cfgs[p].ny == cfgs[q].ny && cfgs[p].nz == cfgs[q].nz &&
+                              cfgs[p].precision == cfgs[q].precision))
+                p++;
+            lesgpu_ctx* c = les_solver_ctx(e->members[q]);
+            if (p < q) {
+                int tl[5];
+                lesgpu_ctx* src = les_solver_ctx(e->members[p]);
+                rc = lesgpu_get_tiles(src, tl);
+                if (rc == LESGPU_OK) rc = lesgpu_set_tiles(c, tl);
+                if (rc == LESGPU_OK) rc = lesgpu_set_scalar_staging(c, lesgpu_get_scalar_staging(src));
+            } else {
+                rc = lesgpu_autotune(c, 3, NULL, NULL);
+            }
+        }
         if (rc) {
             les_ensemble_destroy(e);
             return rc;

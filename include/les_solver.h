@@ -123,8 +123,9 @@ unsigned long long les_solver_rng_draws(const les_solver* s);
 /* Ensembles (no reference counterpart as an API: the reference's Bayesian optimiser runs
  * one LES per parameter proposal, bayesian_optimizer.py:568-673).  n solvers with their own
  * configs (grids, model constants, seeds) on one device, all advanced by one multi-stream
- * graph per step (lesgpu_group_*).  autotune != 0 picks each member's tiles at creation
- * (lesgpu_autotune).  les_ensemble_run advances every member by nsteps in chunks of
+ * graph per step (lesgpu_group_*).  autotune != 0 tunes the tiles at creation
+ * (lesgpu_autotune, once per grid shape and precision; the other members of that shape get
+ * the same tiles).  les_ensemble_run advances every member by nsteps in chunks of
  * `chunk` steps (<= 0: 64), writing each member's enabled outputs as les_solver_run_device
  * does; each member's results equal running it alone with the same tiles. */
 typedef struct les_ensemble les_ensemble;
