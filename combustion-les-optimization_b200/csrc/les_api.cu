@@ -265,12 +265,24 @@ std::vector<unsigned int> jump_table(int rows) {
     return J;
 }
 
+// Device buffers of a context come from the device's stream-ordered pool, allocated and freed
+// on the context's stream.  cudaFree waits for the whole device, so a serving loop that creates
+// and retires solves while others step would stall every stream at each retirement.  A buffer
+// is used on another stream (or by a synchronous copy) only after the context's stream has
+// been synchronised once since its allocation.
+template <typename T>
+cudaError_t dalloc(DevCtx& d, T** p, size_t bytes) {
+    return cudaMallocAsync((void**)p, bytes, d.stream);
+}
+inline void dfree(DevCtx& d, void* p) {
+    if (p) cudaFreeAsync(p, d.stream);
+}
+
 void free_loop(DevCtx& d) {
     if (d.graph) { cudaGraphExecDestroy(d.graph); d.graph = nullptr; }
     d.graph_ok = false;
     void* bufs[] = {d.J, d.dL, d.loop_st, d.hist_probe, d.hist_dt, d.hist_umax, d.hist_mon};
-    for (void* b : bufs)
-        if (b) cudaFree(b);
+    for (void* b : bufs) dfree(d, b);
     d.J = nullptr; d.dL = nullptr; d.loop_st = nullptr;
     d.hist_probe = d.hist_dt = d.hist_umax = d.hist_mon = nullptr;
     d.loop_ready = false;
@@ -281,16 +293,16 @@ int alloc_history(lesgpu_ctx* ctx, const int* st, int n, int kline, int cap) {
     if (d.graph) { cudaGraphExecDestroy(d.graph); d.graph = nullptr; }
     d.graph_ok = false;
     void* bufs[] = {d.loop_st, d.hist_probe, d.hist_dt, d.hist_umax, d.hist_mon};
-    for (void* b : bufs)
-        if (b) cudaFree(b);
+    for (void* b : bufs) dfree(d, b);
     d.loop_st = nullptr; d.hist_probe = d.hist_dt = d.hist_umax = d.hist_mon = nullptr;
     d.loop_nst = n; d.loop_kline = kline; d.loop_cap = cap;
-    CK(cudaMalloc(&d.loop_st, (n > 0 ? n : 1) * sizeof(int)));
+    CK(dalloc(d, &d.loop_st, (n > 0 ? n : 1) * sizeof(int)));
+    CK(dalloc(d, &d.hist_probe, (size_t)cap * (n > 0 ? n : 1) * d.ny * 6 * sizeof(double)));
+    CK(dalloc(d, &d.hist_dt, (size_t)cap * sizeof(double)));
+    CK(dalloc(d, &d.hist_umax, (size_t)cap * sizeof(double)));
+    CK(dalloc(d, &d.hist_mon, (size_t)cap * 6 * sizeof(double)));
+    CK(cudaStreamSynchronize(d.stream));
     if (n > 0) CK(cudaMemcpy(d.loop_st, st, n * sizeof(int), cudaMemcpyHostToDevice));
-    CK(cudaMalloc(&d.hist_probe, (size_t)cap * (n > 0 ? n : 1) * d.ny * 6 * sizeof(double)));
-    CK(cudaMalloc(&d.hist_dt, (size_t)cap * sizeof(double)));
-    CK(cudaMalloc(&d.hist_umax, (size_t)cap * sizeof(double)));
-    CK(cudaMalloc(&d.hist_mon, (size_t)cap * 6 * sizeof(double)));
     return LESGPU_OK;
 }
 
@@ -398,8 +410,15 @@ int lesgpu_create(const lesgpu_config* cfg, const lesgpu_species* sp, lesgpu_ctx
     const size_t fb8 = ((d.n * 8 + 255) / 256) * 256;
     const size_t nf = fields_for_precision();
     d.arena_bytes = kStateFields * fb8 + (nf - kStateFields) * fb;
-    e = cudaMalloc(&d.arena, d.arena_bytes);
-    if (e != cudaSuccess) { ctx->d.err = "device arena allocation failed"; lesgpu_destroy(ctx); return LESGPU_ENOMEM; }
+    e = dalloc(d, &d.arena_raw, d.arena_bytes + 256);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        d.arena_raw = nullptr;
+        ctx->d.err = "device arena allocation failed";
+        lesgpu_destroy(ctx);
+        return LESGPU_ENOMEM;
+    }
+    d.arena = (void*)(((uintptr_t)d.arena_raw + 255) & ~(uintptr_t)255);
     cudaMemsetAsync(d.arena, 0, d.arena_bytes, d.stream);
     char* p = (char*)d.arena;
     auto take = [&]() { void* r = p; p += fb; return r; };
@@ -416,27 +435,25 @@ int lesgpu_create(const lesgpu_config* cfg, const lesgpu_species* sp, lesgpu_ctx
     size_t nb = les::max_cell_blocks(d.nx, d.ny, d.nz);
     d.part_len = 6 * (nb > (size_t)les::MON_BLOCKS ? nb : (size_t)les::MON_BLOCKS) + 64;
     size_t planes = (size_t)d.ny * d.nz;
-    bool ok = cudaMalloc(&d.attr, d.n) == cudaSuccess &&
-              cudaMalloc(&d.dC, sizeof(les::Consts)) == cudaSuccess &&
-              cudaMalloc(&d.dS, sizeof(les::Scalars)) == cudaSuccess &&
-              cudaMalloc(&d.part, d.part_len * sizeof(double)) == cudaSuccess &&
-              cudaMalloc(&d.plane, 3 * planes * sizeof(double)) == cudaSuccess &&
-              cudaMalloc(&d.noise, 3 * planes * sizeof(double)) == cudaSuccess &&
-              cudaMalloc(&d.inlet_list, planes * sizeof(int)) == cudaSuccess &&
-              cudaMalloc(&d.inlet_pos, planes * sizeof(int)) == cudaSuccess &&
-              cudaMalloc(&d.flag, sizeof(int)) == cudaSuccess;
-    if (!ok) { ctx->d.err = "device allocation failed"; lesgpu_destroy(ctx); return LESGPU_ENOMEM; }
+    bool ok = dalloc(d, &d.attr, d.n) == cudaSuccess &&
+              dalloc(d, &d.dC, sizeof(les::Consts)) == cudaSuccess &&
+              dalloc(d, &d.dS, sizeof(les::Scalars)) == cudaSuccess &&
+              dalloc(d, &d.part, d.part_len * sizeof(double)) == cudaSuccess &&
+              dalloc(d, &d.plane, 3 * planes * sizeof(double)) == cudaSuccess &&
+              dalloc(d, &d.noise, 3 * planes * sizeof(double)) == cudaSuccess &&
+              dalloc(d, &d.inlet_list, planes * sizeof(int)) == cudaSuccess &&
+              dalloc(d, &d.inlet_pos, planes * sizeof(int)) == cudaSuccess &&
+              dalloc(d, &d.flag, sizeof(int)) == cudaSuccess;
+    if (!ok) { cudaGetLastError(); ctx->d.err = "device allocation failed"; lesgpu_destroy(ctx); return LESGPU_ENOMEM; }
     d.nv_cap = cfg->num_vortices > 0 ? cfg->num_vortices : 1;
-    if (cudaMalloc(&d.vort, (size_t)d.nv_cap * 7 * sizeof(double)) != cudaSuccess) {
+    if (dalloc(d, &d.vort, (size_t)d.nv_cap * 7 * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        d.vort = nullptr;
         ctx->d.err = "vortex buffer allocation failed";
         lesgpu_destroy(ctx);
         return LESGPU_ENOMEM;
     }
-    d.h_pinned_len = d.n * 8;
-    if (cudaMallocHost(&d.h_pinned, d.h_pinned_len) != cudaSuccess) {
-        d.h_pinned = nullptr;
-        d.h_pinned_len = 0;
-    }
+    // the pinned staging buffer of the host-driven inflow is allocated on first use
     static_assert(sizeof(les::TmaMapsStorage) == sizeof(d.tma_maps), "tensor map storage");
     if (make_tma_maps(d)) {
         cudaError_t pe = (d.precision == LESGPU_FP64) ? les::prepare_tma_f64() : les::prepare_tma_f32();
@@ -461,12 +478,12 @@ void lesgpu_destroy(lesgpu_ctx* ctx) {
     if (!ctx) return;
     DevCtx& d = ctx->d;
     if (d.stream) cudaStreamSynchronize(d.stream);
-    void* bufs[] = {d.arena, d.attr, d.dC, d.dS, d.part, d.plane, d.noise, d.vort, d.inlet_list, d.inlet_pos,
+    if (d.side) cudaStreamSynchronize(d.side);
+    // every buffer was allocated on d.stream, which exists whenever one of them does
+    void* bufs[] = {d.arena_raw, d.attr, d.dC, d.dS, d.part, d.plane, d.noise, d.vort, d.inlet_list, d.inlet_pos,
                     d.probe_st, d.probe_out, d.flag, d.dbg_cp, d.dbg_lam, d.dbg_alpha, d.avg, d.grad_g};
-    for (void* b : bufs)
-        if (b) cudaFree(b);
-    for (int q = 0; q < les::NACC; q++)
-        if (d.kd[q]) cudaFree(d.kd[q]);
+    for (void* b : bufs) dfree(d, b);
+    for (int q = 0; q < les::NACC; q++) dfree(d, d.kd[q]);
     if (d.h_pinned) cudaFreeHost(d.h_pinned);
     for (cudaEvent_t e : d.ev_pool) cudaEventDestroy(e);
     for (int q = 0; q < 16; q++)
@@ -583,10 +600,10 @@ static int ensure_debug(lesgpu_ctx* ctx) {
     DevCtx& d = ctx->d;
     if (d.dbg_cp) return LESGPU_OK;
     size_t bytes = d.n * d.esz;
-    CK(cudaMalloc(&d.dbg_cp, bytes));
-    CK(cudaMalloc(&d.dbg_lam, bytes));
-    CK(cudaMalloc(&d.dbg_alpha, bytes));
-    for (int q = 0; q < les::NACC; q++) CK(cudaMalloc(&d.kd[q], bytes));
+    CK(dalloc(d, &d.dbg_cp, bytes));
+    CK(dalloc(d, &d.dbg_lam, bytes));
+    CK(dalloc(d, &d.dbg_alpha, bytes));
+    for (int q = 0; q < les::NACC; q++) CK(dalloc(d, &d.kd[q], bytes));
     CK(cudaMemsetAsync(d.dbg_cp, 0, bytes, d.stream));
     CK(cudaMemsetAsync(d.dbg_lam, 0, bytes, d.stream));
     CK(cudaMemsetAsync(d.dbg_alpha, 0, bytes, d.stream));
@@ -655,8 +672,8 @@ int lesgpu_set_inflow(lesgpu_ctx* ctx, const double* vortices, int nv, const dou
     if (nv > d.nv_cap) {
         double* nb = nullptr;
         CK(cudaStreamSynchronize(d.stream));
-        CK(cudaMalloc(&nb, (size_t)nv * 7 * sizeof(double)));
-        cudaFree(d.vort);
+        CK(dalloc(d, &nb, (size_t)nv * 7 * sizeof(double)));
+        dfree(d, d.vort);
         d.vort = nb;
         d.nv_cap = nv;
     }
@@ -664,7 +681,15 @@ int lesgpu_set_inflow(lesgpu_ctx* ctx, const double* vortices, int nv, const dou
     if (nv > 0) CK(cudaMemcpyAsync(d.vort, vortices, (size_t)nv * 7 * sizeof(double), cudaMemcpyHostToDevice, d.stream));
     if (d.n_inlet > 0) {
         if (!noise) return LESGPU_EINVAL;
-        if (d.h_pinned == nullptr) return fail(ctx, LESGPU_ENOMEM, "pinned staging buffer unavailable");
+        if (d.h_pinned == nullptr) {
+            d.h_pinned_len = 3 * (size_t)d.ny * d.nz * sizeof(double);
+            if (cudaMallocHost(&d.h_pinned, d.h_pinned_len) != cudaSuccess) {
+                cudaGetLastError();
+                d.h_pinned = nullptr;
+                d.h_pinned_len = 0;
+                return fail(ctx, LESGPU_ENOMEM, "pinned staging buffer unavailable");
+            }
+        }
         // pack r1, r2, r3 of the inlet cells (the only cells the inflow condition reads);
         // the pinned buffer is reused, so wait for the previous upload to finish first
         CK(cudaStreamSynchronize(d.stream));
@@ -703,22 +728,23 @@ int lesgpu_loop_begin(lesgpu_ctx* ctx, const unsigned int rng_window[31], const 
     CK(cudaStreamSynchronize(d.stream));
     free_loop(d);
     if (nv > d.nv_cap) {
-        cudaFree(d.vort);
+        dfree(d, d.vort);
         d.vort = nullptr;
-        CK(cudaMalloc(&d.vort, (size_t)nv * 7 * sizeof(double)));
+        CK(dalloc(d, &d.vort, (size_t)nv * 7 * sizeof(double)));
         d.nv_cap = nv;
     }
     d.nv = nv;
-    if (nv > 0) CK(cudaMemcpy(d.vort, vortices, (size_t)nv * 7 * sizeof(double), cudaMemcpyHostToDevice));
     // at most 6 draws per vortex and 3 per inlet cell in one step
     d.jrows = 6 * nv + 3 * d.n_inlet;
     if (d.jrows < 31) d.jrows = 31;
     std::vector<unsigned int> J = jump_table(d.jrows);
-    CK(cudaMalloc(&d.J, J.size() * sizeof(unsigned int)));
+    CK(dalloc(d, &d.J, J.size() * sizeof(unsigned int)));
+    CK(dalloc(d, &d.dL, sizeof(les::LoopState)));
+    CK(cudaStreamSynchronize(d.stream));
+    if (nv > 0) CK(cudaMemcpy(d.vort, vortices, (size_t)nv * 7 * sizeof(double), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d.J, J.data(), J.size() * sizeof(unsigned int), cudaMemcpyHostToDevice));
     les::LoopState ls{};
     for (int j = 0; j < 31; j++) ls.win[j] = rng_window[j];
-    CK(cudaMalloc(&d.dL, sizeof(les::LoopState)));
     CK(cudaMemcpy(d.dL, &ls, sizeof(ls), cudaMemcpyHostToDevice));
     const lesgpu_config& g = ctx->cfg;
     d.lp_lbox = g.length_scale; d.lp_ly = g.ly; d.lp_lz = g.lz; d.lp_uin = g.inlet_velocity;
@@ -851,12 +877,12 @@ int lesgpu_probe_lines(lesgpu_ctx* ctx, const int* i_stations, int n, int k_line
         if (i_stations[q] < 0 || i_stations[q] >= d.nx) return fail(ctx, LESGPU_EINVAL, "station out of range");
     if (n > d.probe_cap) {
         CK(cudaStreamSynchronize(d.stream));
-        if (d.probe_st) cudaFree(d.probe_st);
-        if (d.probe_out) cudaFree(d.probe_out);
+        dfree(d, d.probe_st);
+        dfree(d, d.probe_out);
         d.probe_st = nullptr;
         d.probe_out = nullptr;
-        CK(cudaMalloc(&d.probe_st, n * sizeof(int)));
-        CK(cudaMalloc(&d.probe_out, (size_t)n * d.ny * 6 * sizeof(double)));
+        CK(dalloc(d, &d.probe_st, n * sizeof(int)));
+        CK(dalloc(d, &d.probe_out, (size_t)n * d.ny * 6 * sizeof(double)));
         d.probe_cap = n;
     }
     CK(cudaMemcpyAsync(d.probe_st, i_stations, n * sizeof(int), cudaMemcpyHostToDevice, d.stream));
@@ -1061,11 +1087,12 @@ int lesgpu_keep_grad_g(lesgpu_ctx* ctx, int enable) {
     CK(cudaStreamSynchronize(d.stream));
     if (enable && !d.grad_g) {
         const size_t bytes = d.n * d.esz;
-        CK(cudaMalloc(&d.grad_g, bytes));
-        CK(cudaMemset(d.grad_g, 0, bytes));   // non-fluid cells stay 0, as in the reference (:2820)
+        CK(dalloc(d, &d.grad_g, bytes));
+        CK(cudaMemsetAsync(d.grad_g, 0, bytes, d.stream));   // non-fluid cells stay 0, as in the reference (:2820)
+        CK(cudaStreamSynchronize(d.stream));
         d.total_bytes += bytes;
     } else if (!enable && d.grad_g) {
-        cudaFree(d.grad_g);
+        dfree(d, d.grad_g);
         d.grad_g = nullptr;
         d.total_bytes -= d.n * d.esz;
     }
@@ -1081,7 +1108,7 @@ int lesgpu_avg_begin(lesgpu_ctx* ctx, int start_step) {
     CK(cudaStreamSynchronize(d.stream));
     const size_t bytes = (size_t)les::NAVG * d.n * sizeof(double);
     if (!d.avg) {
-        CK(cudaMalloc(&d.avg, bytes));
+        CK(dalloc(d, &d.avg, bytes));
         d.total_bytes += bytes;
     }
     CK(cudaMemsetAsync(d.avg, 0, bytes, d.stream));
@@ -1097,7 +1124,7 @@ int lesgpu_avg_end(lesgpu_ctx* ctx) {
     DevCtx& d = ctx->d;
     CK(cudaStreamSynchronize(d.stream));
     if (d.avg) {
-        cudaFree(d.avg);
+        dfree(d, d.avg);
         d.avg = nullptr;
         d.total_bytes -= (size_t)les::NAVG * d.n * sizeof(double);
     }

@@ -79,7 +79,8 @@ struct DevCtx {
     double* probe_out = nullptr;
     int probe_cap = 0;
     int* flag = nullptr;
-    void* arena = nullptr;              // one allocation backing all fields
+    void* arena = nullptr;              // one allocation backing all fields (256-byte aligned)
+    void* arena_raw = nullptr;          // the pool allocation it starts in
     size_t arena_bytes = 0;
     size_t total_bytes = 0;
     cudaStream_t stream = nullptr;

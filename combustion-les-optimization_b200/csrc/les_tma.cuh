@@ -61,9 +61,13 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
+// One step of the ring: the six field planes at i-plane z and, when with_nu, the nu_t plane
+// z - 1.  step_bytes counts all seven; without nu_t the barrier expects nu_bytes fewer.
 __device__ __forceinline__ void tma_issue_step(const TmaMaps& M, uint32_t bar, uint32_t fdst0, uint32_t ndst,
-                                               int fbytes_slot, int step_bytes, int x, int y, int z) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(step_bytes) : "memory");
+                                               int fbytes_slot, int step_bytes, int nu_bytes, bool with_nu, int x,
+                                               int y, int z) {
+    const int bytes = with_nu ? step_bytes : step_bytes - nu_bytes;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 #pragma unroll
     for (int f = 0; f < TMA_NF; f++) {
         const uint64_t map = reinterpret_cast<uint64_t>(&M.f[f]);
@@ -73,6 +77,7 @@ __device__ __forceinline__ void tma_issue_step(const TmaMaps& M, uint32_t bar, u
             "l"(map), "r"(x), "r"(y), "r"(z), "r"(bar)
             : "memory");
     }
+    if (!with_nu) return;
     const uint64_t nmap = reinterpret_cast<uint64_t>(&M.nut);
     asm volatile(
         "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
@@ -124,14 +129,18 @@ __global__ void __launch_bounds__(TMA_TK* TMA_TJ, (sizeof(R) == 8) ? 2 : 3)
     __syncthreads();
     const uint32_t fdst = smem_u32(fring);
     const uint32_t ndst = smem_u32(nbase);
-    // ring slot of field plane at step r: r % RING (RING planes apart per field f: f * RING + slot)
+    // ring slot of field plane at step r: r % RING (RING planes apart per field f: f * RING + slot).
+    // Step r also brings nu_t plane i0 - 3 + r into slot r % NRING.  The prologue issues RING
+    // steps at once, so steps 0 and 1 would share nu_t slots with steps 3 and 4 while both
+    // copies are in flight (their completion order is not defined); their planes i0 - 3 and
+    // i0 - 2 are never read, so those two steps bring no nu_t.
     int issued = 0;   // steps issued (thread 0)
     auto issue = [&](int r) {
         issued = r + 1;
         const int slot = r % TMA_RING, nslot = r % TMA_NRING;
         tma_issue_step(M, smem_u32(&bars[slot]), fdst + (uint32_t)(slot * G::FBYTES),
-                       ndst + (uint32_t)(nslot * G::NSTRIDE), TMA_RING * G::FBYTES, G::STEP_BYTES, x, y,
-                       i0 - 2 + r);
+                       ndst + (uint32_t)(nslot * G::NSTRIDE), TMA_RING * G::FBYTES, G::STEP_BYTES, G::NBYTES,
+                       r >= 2, x, y, i0 - 2 + r);
     };
     if (tid == 0) {
         const int pro = nsteps < TMA_RING ? nsteps : TMA_RING;

@@ -118,7 +118,10 @@ void les_serve_default_options(les_serve_options* o) {
     if (!o) return;
     memset(o, 0, sizeof(*o));
     o->budget_bytes = (size_t)150 * 1000 * 1000 * 1000;
-    o->max_slots = 64;
+    /* 16 requests on the device at once keep it busy; more only share L2 and SM time among
+       more solves (measured on the mixed 100-request stream: 16 slots 7.8e8 cell-steps/s,
+       p50 12 s; 64 slots 6.8e8, p50 21 s) */
+    o->max_slots = 16;
     o->quantum_steps = 16;
     o->keep_results = 1;
     o->autotune = 0;

@@ -75,7 +75,7 @@ def request_bytes(cfg: SolverConfig, precision: int = N.FP32, quantum: int = 16)
 
 
 class Server:
-    def __init__(self, budget_bytes: int = 150 * 10**9, max_slots: int = 64, quantum: int = 16,
+    def __init__(self, budget_bytes: int = 150 * 10**9, max_slots: int = 16, quantum: int = 16,
                  keep_results: bool = True, autotune: bool = False, backfill: bool = False, device: int = 0,
                  chem: str = N.CHEM_BIN, tran: str = N.TRAN_BIN, prep_threads: Optional[int] = None):
         L = _lib()
@@ -217,14 +217,18 @@ def main(argv=None) -> int:
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp32")
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--prep-threads", type=int, default=None, help="set-up / tear-down worker threads")
+    ap.add_argument("--max-slots", type=int, default=16, help="at most this many requests on the device at once")
     a = ap.parse_args(argv)
     prec = N.FP32 if a.precision == "fp32" else N.FP64
     reqs = poisson_requests(a.requests, rate=a.rate, steps=tuple(a.steps), seed=a.seed)
-    srv = Server(budget_bytes=int(a.budget_gb * 1e9), quantum=a.quantum, autotune=True)
+    srv = Server(budget_bytes=int(a.budget_gb * 1e9), max_slots=a.max_slots, quantum=a.quantum, autotune=True,
+                 prep_threads=a.prep_threads)
     st = replay(srv, reqs, prec)
     srv.close()
     st.pop("ids")
     st.update(requests=a.requests, rate=a.rate, steps=list(a.steps), quantum=a.quantum, precision=a.precision,
+              prep_threads=a.prep_threads, max_slots=a.max_slots,
               demand_cell_steps=sum(r.cfg.cells * r.nsteps for r in reqs))
     print(json.dumps(st))
     return 0
