@@ -336,6 +336,7 @@ def run_ours(args):
     for k, v in st.items():
         pinned[k].numpy()[...] = v
     host_state = {k: t.numpy() for k, t in pinned.items()}
+    pinned_out = {k: torch.empty(v.shape, dtype=torch.float64, pin_memory=True).numpy() for k, v in st.items()}
     tmpd = tempfile.mkdtemp(prefix="lesbench_")
     sol.set_outputs(tmpd, N.LES_OUT_PROBES | N.LES_OUT_MONITOR)
     sol.loop_begin(chunk=args.steps)
@@ -344,7 +345,7 @@ def run_ours(args):
     ctx.mark(2)
     ctx.upload_state(host_state)
     sol.loop_run(args.steps)
-    out = ctx.download_state()
+    out = ctx.download_state(out=pinned_out)
     ctx.mark(3)
     sol.loop_end()
     e2e_ms = _max_over_ranks(ctx.elapsed_ms(2, 3), world)

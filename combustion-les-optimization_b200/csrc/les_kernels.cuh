@@ -396,6 +396,9 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::filter)
     if (last) {
         __threadfence();
         double s = 0.0, mn = 0.0, ma = 0.0;
+        // unrolled so that the partials' loads are in flight together; each thread still adds
+        // its entries in ascending order, so the sum is unchanged
+#pragma unroll 8
         for (unsigned q = tid; q < nblk; q += NT) {
             s += __ldcg(&part[q]);
             if (want_max) { mn = fmax(mn, __ldcg(&part[nblk + q])); ma = fmax(ma, __ldcg(&part[2 * nblk + q])); }
@@ -1189,6 +1192,7 @@ __global__ void __launch_bounds__(NT) k_bc_eos(LES_KERNEL_CONSTS, const uint8_t*
     if (last) {
         __threadfence();
         double m = 0.0;
+#pragma unroll 8
         for (unsigned q = tid; q < nblk; q += NT) m = fmax(m, __ldcg(&part[q]));
         m = block_max<NT>(m, sh, tid);
         if (tid == 0) {
@@ -1231,6 +1235,7 @@ __global__ void __launch_bounds__(NT) k_umax(LES_KERNEL_CONSTS, const uint8_t* _
     if (last) {
         __threadfence();
         double m = 0.0;
+#pragma unroll 8
         for (unsigned q = tid; q < nblk; q += NT) m = fmax(m, __ldcg(&part[q]));
         m = block_max<NT>(m, sh, tid);
         if (tid == 0) {
@@ -1275,6 +1280,7 @@ __global__ void __launch_bounds__(NT) k_monitor(LES_KERNEL_CONSTS, F11<R> S, dou
     if (last) {
         __threadfence();
         double acc[6] = {0.0, 1.0e9, -1.0e9, 1.0e9, -1.0e9, 1.0e9};
+#pragma unroll 4
         for (unsigned q = tid; q < nblk; q += NT) {
             acc[0] += __ldcg(&part[q]);
             acc[1] = fmin(acc[1], __ldcg(&part[nblk + q]));
@@ -1383,6 +1389,7 @@ __global__ void __launch_bounds__(NT) k_loop_monitor(LES_KERNEL_CONSTS, F11<R> S
     if (last) {
         __threadfence();
         double acc[6] = {0.0, 1.0e9, -1.0e9, 1.0e9, -1.0e9, 1.0e9};
+#pragma unroll 4
         for (unsigned q = tid; q < nblk; q += NT) {
             acc[0] += __ldcg(&part[q]);
             acc[1] = fmin(acc[1], __ldcg(&part[nblk + q]));

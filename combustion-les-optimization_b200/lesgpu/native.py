@@ -279,8 +279,16 @@ class Context:
             assert a.shape == self.shape
         self._check(lib().lesgpu_upload_state(self._h, _ptrs(arrs), len(arrs)), "upload_state")
 
-    def download_state(self) -> Dict[str, np.ndarray]:
-        arrs = [np.empty(self.shape, dtype=np.float64) for _ in STATE_NAMES]
+    def download_state(self, out: Optional[Dict[str, np.ndarray]] = None) -> Dict[str, np.ndarray]:
+        """The state Phi_n as float64 host arrays; ``out`` (C-contiguous float64 arrays of the
+        grid's shape, e.g. views of pinned buffers) receives it in place."""
+        if out is None:
+            arrs = [np.empty(self.shape, dtype=np.float64) for _ in STATE_NAMES]
+        else:
+            arrs = [out[k] for k in STATE_NAMES]
+            for a in arrs:
+                if a.dtype != np.float64 or a.shape != self.shape or not a.flags.c_contiguous or not a.flags.writeable:
+                    raise ValueError("download_state: out arrays must be writeable C-contiguous float64 of the grid shape")
         self._check(lib().lesgpu_download_state(self._h, _ptrs(arrs), len(arrs)), "download_state")
         return dict(zip(STATE_NAMES, arrs))
 
