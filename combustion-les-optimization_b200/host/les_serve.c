@@ -57,6 +57,8 @@ typedef struct serve_req {
     int job_rc;
     int inflight;                 /* steps queued on the device and not yet collected */
     size_t dev_bytes;             /* device bytes of the solver when it started */
+    long long retry_after;        /* set-up ran out of device memory: wait until more than this
+                                     many requests have ended */
     struct serve_req* next_job;
 } serve_req;
 
@@ -327,6 +329,7 @@ int les_serve_submit(les_serve* s, const lesgpu_config* cfg, int nsteps, const c
     q->nsteps = nsteps;
     q->state = LES_REQ_QUEUED;
     q->phase = PH_NONE;
+    q->retry_after = -1;
     q->t_submit = now_s();
     q->bytes = need;
     if (out_dir) snprintf(q->out_dir, sizeof(q->out_dir), "%s", out_dir);
@@ -413,6 +416,17 @@ static void harvest(les_serve* s) {
         if (q->state != LES_REQ_QUEUED && q->state != LES_REQ_ACTIVE) continue;
         const int ph = phase_of(s, q);
         if (ph == PH_READY) {
+            if (q->job_rc == LESGPU_ENOMEM && s->n_active > 0) {
+                /* the device is fuller than budgeted (memory of running requests, or freed
+                   memory not yet returned): queue it again until another request ends */
+                pthread_mutex_lock(&s->mu);
+                s->in_use -= q->bytes;
+                s->n_slots--;
+                q->phase = PH_NONE;
+                pthread_mutex_unlock(&s->mu);
+                q->retry_after = s->n_done + s->n_failed + s->n_cancelled;
+                continue;
+            }
             if (q->job_rc) {
                 retire(s, q, LES_REQ_FAILED, q->job_rc);
                 continue;
@@ -436,7 +450,11 @@ static int admit_queued(les_serve* s) {
     int k = 0;
     for (long long i = s->head; i < s->n && s->n_slots < s->opt.max_slots; i++) {
         serve_req* q = s->reqs[i];
-        if (q->state != LES_REQ_QUEUED || q->phase != PH_NONE) continue;
+        if (q->state != LES_REQ_QUEUED || phase_of(s, q) != PH_NONE) continue;
+        if (q->retry_after >= 0 && s->n_done + s->n_failed + s->n_cancelled <= q->retry_after) {
+            if (s->opt.backfill) continue;
+            break;
+        }
         if (s->in_use + q->bytes > s->opt.budget_bytes) {
             if (s->opt.backfill) continue;
             break;
