@@ -3,7 +3,7 @@ reference's own outputs (tests/golden).
 
 Tolerances (plain FP64 form), relative L2 per state field ||gpu - ref|| / ||ref||:
   * RHS intermediates of one calculate_RHS evaluation: 1e-12
-  * whole state after 1 step: 1e-10; after 10 steps: 1e-8
+  * whole state after 1 step: 1e-10; after 10 steps: 1e-8 (the parity tolerances the drop-in is held to)
   * dt: identical (it is a max-reduction of identical fields and a host formula)
   * SEM inflow face: bit-identical (the plane is summed in the reference's order)
 """
