@@ -45,3 +45,10 @@ def test_missing_library_fails_loudly(tmp_path, monkeypatch):
         assert "build.py" in str(e)
     else:
         raise AssertionError("expected FileNotFoundError")
+
+
+def test_bind_device_rejects_a_negative_device(lesgpu_native):
+    lib = ctypes.CDLL(lesgpu_native.LIB_PATH)
+    lib.lesgpu_bind_device.argtypes = [ctypes.c_int]
+    lib.lesgpu_bind_device.restype = ctypes.c_int
+    assert lib.lesgpu_bind_device(-1) == -1          # LESGPU_EINVAL, no CUDA call made
