@@ -416,9 +416,10 @@ static void harvest(les_serve* s) {
         if (q->state != LES_REQ_QUEUED && q->state != LES_REQ_ACTIVE) continue;
         const int ph = phase_of(s, q);
         if (ph == PH_READY) {
-            if (q->job_rc == LESGPU_ENOMEM && s->n_active > 0) {
-                /* the device is fuller than budgeted (memory of running requests, or freed
-                   memory not yet returned): queue it again until another request ends */
+            if (q->job_rc == LESGPU_ENOMEM && s->n_slots > 1) {
+                /* the device is fuller than budgeted while other requests hold memory (set-ups
+                   in progress, running or finishing solves): queue it again until another
+                   request ends */
                 pthread_mutex_lock(&s->mu);
                 s->in_use -= q->bytes;
                 s->n_slots--;
@@ -451,7 +452,7 @@ static int admit_queued(les_serve* s) {
     for (long long i = s->head; i < s->n && s->n_slots < s->opt.max_slots; i++) {
         serve_req* q = s->reqs[i];
         if (q->state != LES_REQ_QUEUED || phase_of(s, q) != PH_NONE) continue;
-        if (q->retry_after >= 0 && s->n_done + s->n_failed + s->n_cancelled <= q->retry_after) {
+        if (q->retry_after >= 0 && s->n_done + s->n_failed + s->n_cancelled <= q->retry_after && s->n_slots > 0) {
             if (s->opt.backfill) continue;
             break;
         }
