@@ -8,10 +8,13 @@ and the final state fields.
 
 The flow is chaotic: any perturbation, even at rounding level, grows until the two
 trajectories decorrelate, after which their statistics differ by sampling noise alone.  A
-further FP64 runs from an initial temperature field scaled by (1 + eps) separate that floor
-from the precision error: eps = 1e-15 (rounding level in FP64) and eps = 1e-7 (rounding
-level in FP32, applied once).  Their profile and state differences against the first FP64
-run are reported beside the FP32 ones (``profiles_floor_<eps>``).
+further FP64 runs from an initial field scaled by (1 + eps) separate that floor from the
+precision error: eps = 1e-15 (rounding level in FP64) and eps = 1e-7 (rounding level in FP32,
+applied once).  Their profile and state differences against the first FP64 run are reported
+beside the FP32 ones (``profiles_floor_<eps>``).  The scaled field is T by default; T and Y
+are nudged towards their targets, so a T perturbation reaches the velocity only through the
+density, while ``--floor-field u`` perturbs the velocity itself and so measures how fast the
+flow amplifies a rounding-size difference.
 """
 from __future__ import annotations
 
@@ -43,11 +46,11 @@ def _pool(directory: str) -> Dict[str, np.ndarray]:
 
 
 def run_form(cfg: SolverConfig, precision: int, steps: int, directory: str, chunk: int = 64, device: int = 0,
-             perturb: float = 0.0):
+             perturb: float = 0.0, field: str = "T"):
     s = N.Solver(cfg, precision=precision, device=device)
     if perturb:
         st = s.state()
-        st["T"] = st["T"] * (1.0 + perturb)
+        st[field] = st[field] * (1.0 + perturb)
         s.ctx.upload_state(st)
     s.set_outputs(directory, N.LES_OUT_PROBES | N.LES_OUT_MONITOR)
     t = time.perf_counter()
@@ -68,7 +71,7 @@ def _state_err(a, b):
 
 
 def compare(cfg: SolverConfig, steps: int, workdir: Optional[str] = None, chunk: int = 64,
-            floor=(1e-15, 1e-7)) -> dict:
+            floor=(1e-15, 1e-7), floor_field: str = "T") -> dict:
     workdir = workdir or tempfile.mkdtemp(prefix="lesprec_")
     dirs = {k: os.path.join(workdir, k) for k in ("fp64", "fp32")}
     for d in dirs.values():
@@ -82,7 +85,7 @@ def compare(cfg: SolverConfig, steps: int, workdir: Optional[str] = None, chunk:
     for eps in (floor or ()):
         d = os.path.join(workdir, f"fp64_eps{eps:g}")
         os.makedirs(d, exist_ok=True)
-        salt, walt = run_form(cfg, N.FP64, steps, d, chunk, perturb=eps)
+        salt, walt = run_form(cfg, N.FP64, steps, d, chunk, perturb=eps, field=floor_field)
         ralt = _pool(d)
         out["wall_s"][f"fp64_eps{eps:g}"] = walt
         out[f"profiles_floor_{eps:g}"] = stats.compare_profiles(ralt, r64)
@@ -98,8 +101,10 @@ def main(argv=None) -> int:
     ap.add_argument("--chunk", type=int, default=64)
     ap.add_argument("--workdir", default=None)
     ap.add_argument("--no-floor", action="store_true")
+    ap.add_argument("--floor-field", choices=["T", "u"], default="T", help="field the floor runs scale by 1 + eps")
     a = ap.parse_args(argv)
-    print(json.dumps(compare(preset(a.workload), a.steps, a.workdir, a.chunk, floor=() if a.no_floor else (1e-15, 1e-7))))
+    print(json.dumps(compare(preset(a.workload), a.steps, a.workdir, a.chunk, floor=() if a.no_floor else (1e-15, 1e-7),
+                             floor_field=a.floor_field)))
     return 0
 
 
