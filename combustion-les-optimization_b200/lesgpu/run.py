@@ -29,6 +29,7 @@ def main(argv=None) -> int:
                     help="auto, default, or five tile-shape indices (filter,strain,flow,scalar,eos), e.g. 0,1,2,5,0")
     ap.add_argument("--loop", choices=["host", "device"], default="host")
     ap.add_argument("--kernel-times", action="store_true")
+    ap.add_argument("--staged", action="store_true", help="scalar pass through the TMA-staged kernel")
     ap.add_argument("--outputs", default=None)
     a = ap.parse_args(argv)
     prec = N.FP32 if a.precision == "fp32" else N.FP64
@@ -41,6 +42,9 @@ def main(argv=None) -> int:
     elif a.tiles != "default":
         s.ctx.set_tiles([int(t) for t in a.tiles.split(",")])
         out["tiles"] = s.ctx.get_tiles()
+    if a.staged:
+        s.ctx.set_scalar_staging(True)
+        out["staged"] = True
     if a.outputs:
         s.set_outputs(a.outputs, N.LES_OUT_PROBES | N.LES_OUT_MONITOR)
     run = (lambda n: s.run_device(n, chunk=max(n, 1))) if a.loop == "device" else s.step
