@@ -64,8 +64,9 @@ struct KFlow {               // momentum and G right-hand sides handed from C1 t
 // Minimum resident blocks per SM requested from the register allocator (filter / flow /
 // scalar).  These kernels are latency-bound; swept on B200 at 256x128x128: FP64 5/4/4 (the
 // scalar pass at 3 blocks 3.41 ms, at 4 3.17 ms; the filter at 4 3.14 ms, at 5 3.02 ms; the
-// flow pass at 5 slower), FP32 8/8/8/6 for filter/strain/flow/scalar (the scalar pass at 4
-// blocks 2.01 ms, at 5 1.84 ms, at 6 1.76 ms).
+// flow pass at 5 slower), FP32 8/8/6/6 for filter/strain/flow/scalar (the scalar pass at 4
+// blocks 2.01 ms, at 5 1.84 ms, at 6 1.76 ms; the flow pass at 8 0.616 ms, at 7 0.616, at 6
+// 0.597).
 #ifndef LES_MINB_FILTER
 #define LES_MINB_FILTER 5
 #endif
@@ -82,7 +83,7 @@ struct KFlow {               // momentum and G right-hand sides handed from C1 t
 #define LES_MINB_STRAIN_F32 8
 #endif
 #ifndef LES_MINB_FLOW_F32
-#define LES_MINB_FLOW_F32 8
+#define LES_MINB_FLOW_F32 6
 #endif
 #ifndef LES_MINB_SCALAR_F32
 #define LES_MINB_SCALAR_F32 6
