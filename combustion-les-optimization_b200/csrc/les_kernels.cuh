@@ -70,6 +70,9 @@ struct KFlow {               // momentum and G right-hand sides handed from C1 t
 #ifndef LES_MINB_FILTER
 #define LES_MINB_FILTER 5
 #endif
+#ifndef LES_MINB_STRAIN
+#define LES_MINB_STRAIN 3
+#endif
 #ifndef LES_MINB_FLOW
 #define LES_MINB_FLOW 4
 #endif
@@ -90,7 +93,8 @@ struct KFlow {               // momentum and G right-hand sides handed from C1 t
 #endif
 template <typename R>
 struct MinBlocks {
-    static constexpr int filter = LES_MINB_FILTER, strain = 3, flow = LES_MINB_FLOW, scalar = LES_MINB_SCALAR;
+    static constexpr int filter = LES_MINB_FILTER, strain = LES_MINB_STRAIN, flow = LES_MINB_FLOW,
+                         scalar = LES_MINB_SCALAR;
 };
 template <>
 struct MinBlocks<float> {
