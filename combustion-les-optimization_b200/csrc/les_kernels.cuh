@@ -281,7 +281,11 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
     // Hirschfelder-Curtiss (:1716-1749): sx_a = sum over b != a (ascending b) of X_b / D_ab.
     // With a symmetric fit table each D_ab is evaluated once per unordered pair and both
     // sums take their term from it; the rows are visited in ascending order, so each sx_a
-    // still receives its terms in ascending b.  The quotient uses one reciprocal per pair.
+    // still receives its terms in ascending b.  1 / D_ab is taken directly as
+    // exp(-P_ab(ln T)) * 1e4 (D_ab = exp(P_ab) * 1e-4), one exponential and no division: the
+    // terms X_b / D_ab differ from the reference's quotients by at most ~2 ulp (the FP64
+    // property pass 2.82 -> 2.53 ms per 256x128x128 step); the skip rule D_ab > 1e-12 reads
+    // 1 / D_ab < 1e12.
     R sxa[NSP];
 #pragma unroll
     for (int a = 0; a < NSP; a++) sxa[a] = R(0);
@@ -291,11 +295,13 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
 #pragma unroll
             for (int b = a + 1; b < NSP; b++) {
                 if (!(X[a] > R(1e-12) || X[b] > R(1e-12))) continue;
-                const R v = fit_prop<R>(K.dco[a][b], C.dco_zero[a][b], L, L2, L3) * R(1e-4);
-                if (!(v > R(1e-12))) continue;
-                const R y = qdiv(R(1.0), v);
-                if (X[b] > R(1e-12)) sxa[a] += mdiv(X[b], v, y);
-                if (X[a] > R(1e-12)) sxa[b] += mdiv(X[a], v, y);
+                if (C.dco_zero[a][b]) continue;          // D_ab = 0 fails D_ab > 1e-12
+                const auto& co = K.dco[a][b];
+                const R lp = (R)co[0] + (R)co[1] * L + (R)co[2] * L2 + (R)co[3] * L3;
+                const R y = qexp(-lp) * R(1e4);
+                if (!(y < R(1e12))) continue;
+                if (X[b] > R(1e-12)) sxa[a] += X[b] * y;
+                if (X[a] > R(1e-12)) sxa[b] += X[a] * y;
             }
     } else {
 #pragma unroll
