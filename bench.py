@@ -63,6 +63,12 @@ def kernel_bytes_per_cell(cls: str, e: int) -> float:
     }[cls]
 
 
+# The CPU reference is timed on the same bounded sample in both places it is reported (the
+# cpu_baseline leg of this arm and the --impl reference arm): the first REF_SAMPLE_STEPS
+# steps of the workload, the first of them untimed (page faults), wall time per step.
+REF_SAMPLE_STEPS = 21
+REF_SAMPLE_BUDGET_S = 150.0
+
 # Whole step, FP64: per RK stage read the stage state (11 fields), Phi_n (10) and the RK
 # accumulator (10), write the accumulator (10) and the next stage state (11): 52 field
 # accesses x 4 stages x 8 B = 1664 B per cell-step (832 B with 4-byte fields).
@@ -244,8 +250,7 @@ def run_reference_arm(args):
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    steps = max(2, args.warmup + args.steps)
-    r = cpu_reference_rate(args.workload, min(steps, 40), budget_s=150.0, threads=threads)
+    r = cpu_reference_rate(args.workload, REF_SAMPLE_STEPS, budget_s=REF_SAMPLE_BUDGET_S, threads=threads)
     if r is None:
         print(json.dumps({"impl": "reference", "unavailable": "compiled reference produced no timed steps"}))
         return 0
@@ -255,7 +260,10 @@ def run_reference_arm(args):
     line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world,
             "steps": n, "warmup": 1, "ms_per_step": cfg.cells / rate * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOADS.get(args.workload, args.workload), "grid": [cfg.nx, cfg.ny, cfg.nz]},
+            "config": {"workload": WORKLOADS.get(args.workload, args.workload), "grid": [cfg.nx, cfg.ny, cfg.nz],
+                       "cells": cfg.cells, "precision": "fp64", "parallelism": f"OpenMP x{cores} host threads",
+                       "l2": "host caches (the reference's 174 FP64 grids stay in host memory)",
+                       "tiles": None},
             "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -374,7 +382,8 @@ def run_ours(args):
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            r = cpu_reference_rate(args.workload, 4, budget_s=60.0, threads=os.cpu_count() or 1)
+            r = cpu_reference_rate(args.workload, REF_SAMPLE_STEPS, budget_s=REF_SAMPLE_BUDGET_S,
+                                   threads=os.cpu_count() or 1)
             if r is not None:
                 rate, n, cores, kind, sample = r
                 cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}

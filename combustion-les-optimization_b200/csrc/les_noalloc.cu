@@ -8,12 +8,20 @@
 // caller owns the field arrays and a 6-double output buffer on the device and must not see
 // the library allocate anything behind its back.
 //
-// Scratch lives in one file-scope __device__ array, so every GPU that loads the library
-// holds LES_NOALLOC_SCRATCH_BYTES of it until the process exits.  The array is shared by
+// Scratch lives in one file-scope __device__ array of kScratchDoubles doubles (3 MiB, for
+// LESGPU_NOALLOC_MAX_CELLS cells), so every GPU that loads the library holds it until the
+// process exits.  The array is shared by
 // all calls on a device and keeps the previous call's contents; the completion counter at
 // its start is cleared on every call, and the per-block partials are rewritten before they
 // are read.  Calls whose work overlaps on the GPU (different streams, or different threads
-// on one device) race on the array and must be serialised by the caller.
+// on one device) race on the array and must be serialised by the caller.  The scratch address
+// is the current device's, so the stream and the buffers must belong to the current device;
+// a mismatch is refused (LESGPU_EINVAL) rather than launched on another device's memory.
+//
+// Reductions: the minima and maxima start from the monitor's own +-1e9 sentinels (as
+// write_monitor_log does, les_combustion_solver.c:3880-3897), so a field entirely beyond
+// them reports the sentinel; fmin/fmax skip NaN operands, where the reference's comparisons
+// would keep the first value -- the reference's NaN guard is check_for_nan, not the monitor.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -112,10 +120,27 @@ extern "C" int lesgpu_monitor_noalloc(const double* rho, const double* T, const 
                                       double dx, double dy, double dz, double* out, void* stream) {
     if (!rho || !T || !G || !Y0 || !out || n == 0) return LESGPU_EINVAL;
     if (n > (size_t)LESGPU_NOALLOC_MAX_CELLS) return LESGPU_EINVAL;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return LESGPU_ECUDA;
+    // the output must be device memory of the current device, and so must the stream's device
+    cudaPointerAttributes pa;
+    if (cudaPointerGetAttributes(&pa, out) != cudaSuccess) {
+        cudaGetLastError();
+        return LESGPU_EINVAL;
+    }
+    if ((pa.type != cudaMemoryTypeDevice && pa.type != cudaMemoryTypeManaged) || pa.device != dev) return LESGPU_EINVAL;
+    if (st) {
+        int sdev = -1;
+        if (cudaStreamGetDevice(st, &sdev) != cudaSuccess) {
+            cudaGetLastError();
+            return LESGPU_EINVAL;
+        }
+        if (sdev != dev) return LESGPU_EINVAL;
+    }
     double* scratch = nullptr;
     int rc = scratch_for_current_device(&scratch);
     if (rc != LESGPU_OK) return rc;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     // the completion counter must start at zero on every call
     if (cudaMemsetAsync(scratch, 0, 256, st) != cudaSuccess) return LESGPU_ECUDA;
     const unsigned nb = (unsigned)((n + kThreads - 1) / kThreads);

@@ -134,9 +134,9 @@ void les_serve_default_options(les_serve_options* o) {
 
 /* ------------------------------------------------------------------ worker jobs */
 
-static const tile_entry* find_tiles(les_serve* s, const lesgpu_config* c) {
+static tile_entry* find_tiles(les_serve* s, const lesgpu_config* c) {
     for (int q = 0; q < s->n_tiles; q++) {
-        const tile_entry* t = &s->tiles[q];
+        tile_entry* t = &s->tiles[q];
         if (t->nx == c->nx && t->ny == c->ny && t->nz == c->nz && t->precision == c->precision) return t;
     }
     return NULL;
@@ -144,10 +144,13 @@ static const tile_entry* find_tiles(les_serve* s, const lesgpu_config* c) {
 
 /* One autotuning per grid shape and precision; later requests of that shape (also those set
    up meanwhile by other workers, which wait for it) get the same tiles and scalar-pass form,
-   so a result does not depend on arrival order. */
+   so a result does not depend on arrival order.  An entry is 0 while its autotune runs, 1
+   once published, -1 after a failed autotune: the next request of that shape (a woken waiter
+   or a later arrival) claims it and tunes again, so a failure is never cached and every
+   request of the shape still ends up with the one published result. */
 static int tiles_for(les_serve* s, serve_req* q, lesgpu_ctx* ctx) {
     pthread_mutex_lock(&s->mu);
-    const tile_entry* t = find_tiles(s, &q->cfg);
+    tile_entry* t = find_tiles(s, &q->cfg);
     while (t && t->ready == 0) {
         pthread_cond_wait(&s->cv_done, &s->mu);
         t = find_tiles(s, &q->cfg);
@@ -160,7 +163,10 @@ static int tiles_for(les_serve* s, serve_req* q, lesgpu_ctx* ctx) {
         return rc;
     }
     tile_entry* e = NULL;
-    if (!t && s->n_tiles < 64) {
+    if (t) {
+        e = t;                     /* the last autotune of this shape failed: retry here */
+        e->ready = 0;
+    } else if (s->n_tiles < 64) {
         e = &s->tiles[s->n_tiles++];
         e->nx = q->cfg.nx; e->ny = q->cfg.ny; e->nz = q->cfg.nz; e->precision = q->cfg.precision;
         e->ready = 0;

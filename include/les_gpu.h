@@ -185,7 +185,8 @@ int lesgpu_monitor(lesgpu_ctx* ctx, double out[6]);
  * until exit, so n is limited to LESGPU_NOALLOC_MAX_CELLS; larger n returns LESGPU_EINVAL.
  * The first call on a device looks up that array's device address and should come before
  * any stream capture.  All calls share the array: calls that overlap on the GPU race and
- * must be serialised by the caller. */
+ * must be serialised by the caller.  `stream` and every buffer must belong to the current
+ * device (the scratch address is the current device's); otherwise LESGPU_EINVAL. */
 #define LESGPU_NOALLOC_MAX_CELLS 16777216
 int lesgpu_monitor_noalloc(const double* rho, const double* T, const double* G, const double* Y0, size_t n,
                            double dx, double dy, double dz, double* out, void* stream);
@@ -261,8 +262,9 @@ int lesgpu_get_tiles(const lesgpu_ctx* ctx, int tiles[5]);
 int lesgpu_autotune(lesgpu_ctx* ctx, int reps, int tiles_out[5], double* ms_out);
 /* The scalar pass with its stencil fields staged in shared memory by tensor copies
  * (cp.async.bulk.tensor, a (32 x 8) tile marching through i-planes; the same arithmetic, so
- * the same bits).  Available when a grid row (NZ values) is a multiple of 16 bytes;
- * lesgpu_autotune switches it on when it times faster than the best plain tile. */
+ * the same bits).  Available when a grid row (NZ values) is a multiple of 16 bytes.  Off
+ * by default and left alone by lesgpu_autotune: on B200 it is slower than the plain pass
+ * (two resident blocks of 112.5 KB shared memory per SM instead of four). */
 int lesgpu_set_scalar_staging(lesgpu_ctx* ctx, int enable);
 int lesgpu_get_scalar_staging(const lesgpu_ctx* ctx);
 

@@ -17,10 +17,20 @@ This recipe compiles ``les_combustion_solver.c`` from the reference tree into
   ``checkpoint.bin`` field order plus ``nu_t``/``S_mag`` and prints the per-step wall
   time (``omp_get_wtime``), and a hook after the stage-1 ``calculate_RHS`` (``:4429``)
   that dumps the RHS intermediates for per-kernel checks,
-* ``output_vtk`` returns immediately when ``LES_REF_NOVTK`` is set (timing runs).
+* ``output_vtk`` returns immediately when ``LES_REF_NOVTK`` is set (timing runs),
+* the inflow loop of ``apply_boundary_conditions`` (``:2978``), which draws three
+  ``rand()`` values per inlet cell inside ``#pragma omp parallel for``, runs on one thread
+  when ``LES_REF_SERIAL_BC=1``: the draws then come in the serial (j, k) order whatever
+  ``OMP_NUM_THREADS`` is, so a multi-threaded run is comparable with the GPU solver (with
+  several threads the draw order depends on the OpenMP schedule and glibc's lock).  Every
+  other loop keeps its threads; only the order of the OpenMP sums (``<rho_f>``, ``:2538``)
+  still depends on the thread count, at rounding level,
+* with ``LES_REF_DUMP_FIRST=1`` the state after the first step is dumped as well as every
+  ``LES_REF_DUMP_EVERY``-th.
 
 Nothing else in the solver is touched.  The reference tree is only read; all outputs go
-under ``oracle/_ref/``.  Usage::
+under ``oracle/_ref/``.  The reference checkout is ``$LES_REFERENCE_DIR``, else a
+``reference`` directory beside this repository.  Usage::
 
     python oracle/build_ref.py [--ref /path/to/reference] [--config NAME ...]
 """
@@ -35,7 +45,19 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_ROOT = os.path.join(HERE, "_ref")
-DEFAULT_REF = "/root/reference"
+
+
+def default_ref() -> str:
+    """The reference checkout: ``$LES_REFERENCE_DIR``, else ``../reference`` beside the repository."""
+    env = os.environ.get("LES_REFERENCE_DIR")
+    if env:
+        return env
+    return os.path.normpath(os.path.join(os.path.dirname(HERE), "..", "reference"))
+
+
+def ref_present(ref_dir: str = None) -> bool:
+    return os.path.exists(os.path.join(ref_dir or default_ref(), "les_combustion_solver.c"))
+
 
 # Grid configurations that the oracle binary is compiled for.  Grid sizes and the SEM
 # vortex count are array dimensions in the reference, so each needs its own binary.
@@ -65,6 +87,7 @@ double les_ref_accel_strength = 2.0361, les_ref_accel_width = 0.1126, les_ref_ac
 double les_ref_relax = 5000.0;
 unsigned int les_ref_seed = 1234u;
 int les_ref_start = 0, les_ref_steps = 10, les_ref_dump_every = 0, les_ref_novtk = 0, les_ref_rhs_dump_step = -1;
+int les_ref_serial_bc = 0, les_ref_dump_first = 0;
 double les_ref_t0 = 0.0, les_ref_tprev = 0.0;
 static double les_ref_envd(const char* n, double d) { const char* s = getenv(n); return s ? strtod(s, NULL) : d; }
 static int les_ref_envi(const char* n, int d) { const char* s = getenv(n); return s ? atoi(s) : d; }
@@ -82,6 +105,8 @@ void les_ref_init(void) {
     les_ref_dump_every = les_ref_envi("LES_REF_DUMP_EVERY", 0);
     les_ref_novtk = les_ref_envi("LES_REF_NOVTK", 0);
     les_ref_rhs_dump_step = les_ref_envi("LES_REF_RHS_DUMP_STEP", -1);
+    les_ref_serial_bc = les_ref_envi("LES_REF_SERIAL_BC", 0);
+    les_ref_dump_first = les_ref_envi("LES_REF_DUMP_FIRST", 0);
 }
 '''
 
@@ -92,7 +117,7 @@ void les_ref_after_step(int t, double dt) {
     fprintf(stderr, "LESREF_STEP %d %.17g %.9f\n", t, dt, now - les_ref_tprev);
     les_ref_tprev = now;
     int n = t + 1 - les_ref_start;
-    if (les_ref_dump_every > 0 && n % les_ref_dump_every == 0) {
+    if ((les_ref_dump_every > 0 && n % les_ref_dump_every == 0) || (les_ref_dump_first && n == 1)) {
         char p[64]; sprintf(p, "state_%06d.bin", n);
         FILE* f = fopen(p, "wb");
         if (!f) return;
@@ -175,6 +200,10 @@ def patch_source(src: str, cfg: dict) -> str:
              "calculate_RHS(t_loop, u, v, w, T, G, Yk, rho, k1_rhou, k1_rhov, k1_rhow, k1_T, k1_G, k1_Yk);"
              " les_ref_after_rhs1(t_loop);")
     s = _sub(s, r"^void output_vtk\(int t\) \{", "void output_vtk(int t) { if (les_ref_novtk) return;")
+    s, n = re.subn(r"(\(i=0, i=NX-1\) ---[^\n]*\n[^\n]*\n[ \t]*)#pragma omp parallel for(\r?\n)",
+                   lambda m: m.group(1) + "#pragma omp parallel for if(!les_ref_serial_bc)" + m.group(2), s)
+    if n != 1:
+        raise RuntimeError(f"inflow-loop pragma patch matched {n} times (expected exactly 1)")
     s = _sub(s, r"^int main\(int argc, char \*argv\[\]\) \{", MAIN_HOOKS + "\nint main(int argc, char *argv[]) {")
     return s
 
@@ -206,7 +235,7 @@ def build(ref_dir: str, names, quiet: bool = False) -> None:
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("--ref", default=os.environ.get("LES_REFERENCE_DIR", DEFAULT_REF))
+    ap.add_argument("--ref", default=default_ref())
     ap.add_argument("--config", action="append", choices=sorted(CONFIGS))
     args = ap.parse_args(argv)
     build(args.ref, args.config or sorted(CONFIGS))

@@ -224,7 +224,9 @@ def run_reference(name: str, steps: int, seed: int = 1234, start: int = 0, dump_
     ncell = shape[0] * shape[1] * shape[2]
     dumps = {}
     if dump_every > 0:
-        for n in range(dump_every, steps + 1, dump_every):
+        wanted = sorted(set(range(dump_every, steps + 1, dump_every))
+                        | ({1} if os.path.exists(os.path.join(work, "state_000001.bin")) else set()))
+        for n in wanted:
             path = os.path.join(work, f"state_{n:06d}.bin")
             with open(path, "rb") as f:
                 raw = f.read()

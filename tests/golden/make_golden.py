@@ -37,7 +37,7 @@ FIELDS = build_ref.STATE_FIELDS
 
 def make(name: str, spec: dict) -> str:
     if not oracle.ref_available(spec["config"]):
-        build_ref.build(os.environ.get("LES_REFERENCE_DIR", build_ref.DEFAULT_REF), [spec["config"]])
+        build_ref.build(build_ref.default_ref(), [spec["config"]])
     dumps, meta = oracle.run_reference(spec["config"], spec["steps"], seed=spec["seed"], start=spec["start"],
                                        dump_every=1)
     out = {"steps": np.array(spec["keep"]), "dt": np.array([dumps[n]["dt"] for n in range(1, spec["steps"] + 1)]),

@@ -26,7 +26,10 @@ import types
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(HERE)), "oracle"))
+import build_ref  # noqa: E402
+
+REF = sys.argv[1] if len(sys.argv) > 1 else build_ref.default_ref()
 
 
 class Recorder:

@@ -24,6 +24,13 @@ static pthread_mutex_t g_mu = PTHREAD_MUTEX_INITIALIZER;
 static size_t g_used, g_peak, g_limit = (size_t)-1;
 static long long g_creates, g_enomem, g_tunes, g_live, g_max_live, g_collect_errors;
 static double g_setup_s = 0.002, g_step_ns_per_cell = 1.0;
+static int g_fail_tunes;            /* the next g_fail_tunes autotunes report LESGPU_ECUDA */
+
+void fake_fail_tunes(int n) {
+    pthread_mutex_lock(&g_mu);
+    g_fail_tunes = n;
+    pthread_mutex_unlock(&g_mu);
+}
 
 static void nap(double s) {
     if (s <= 0) return;
@@ -41,6 +48,7 @@ void fake_configure(size_t limit, double setup_s, double step_ns_per_cell) {
     g_step_ns_per_cell = step_ns_per_cell;
     g_used = g_peak = 0;
     g_creates = g_enomem = g_tunes = g_live = g_max_live = g_collect_errors = 0;
+    g_fail_tunes = 0;
     pthread_mutex_unlock(&g_mu);
 }
 
@@ -149,7 +157,10 @@ int lesgpu_autotune(lesgpu_ctx* ctx, int reps, int tiles_out[5], double* ms_out)
     nap(g_setup_s);
     pthread_mutex_lock(&g_mu);
     g_tunes++;
+    const int fail = g_fail_tunes > 0;
+    if (fail) g_fail_tunes--;
     pthread_mutex_unlock(&g_mu);
+    if (fail) return LESGPU_ECUDA;
     for (int q = 0; q < 5; q++) s->tiles[q] = s->cfg.nx % 8;
     if (tiles_out) memcpy(tiles_out, s->tiles, sizeof(s->tiles));
     return LESGPU_OK;

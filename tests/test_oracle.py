@@ -96,10 +96,11 @@ def test_oracle_varied_constants_live(oracle_mod):
 def test_build_recipe_patches_exactly_once():
     """Every textual patch of the reference build recipe matches exactly one site."""
     import build_ref
-    src_path = os.path.join(build_ref.DEFAULT_REF, "les_combustion_solver.c")
+    src_path = os.path.join(build_ref.default_ref(), "les_combustion_solver.c")
     if not os.path.exists(src_path):
         pytest.skip("reference source not present")
     with open(src_path, encoding="utf-8") as f:
         src = f.read()
     patched = build_ref.patch_source(src, build_ref.CONFIGS["tiny"])
     assert "#define NX 24" in patched and "les_ref_after_step(t_loop, DT_sim)" in patched
+    assert "#pragma omp parallel for if(!les_ref_serial_bc)" in patched

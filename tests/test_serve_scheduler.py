@@ -47,6 +47,7 @@ def fake(tmp_path_factory, lesgpu_native):
     L.les_serve_destroy.argtypes = [vp]
     L.fake_configure.argtypes = [C.c_size_t, C.c_double, C.c_double]
     L.fake_stats.argtypes = [C.POINTER(C.c_longlong)]
+    L.fake_fail_tunes.argtypes = [C.c_int]
     return L, S, lesgpu_native
 
 
@@ -150,6 +151,31 @@ def test_budget_slots_and_steps_with_worker_threads(fake):
         r = srv.result(rid)
         for k in range(11):
             assert np.all(r[k] == c.seed * 1000 + n + k + 1e6 * (c.nx % 8)), (rid, k)
+    srv.close()
+
+
+@pytest.mark.parametrize("threads", [0, 3])
+def test_failed_autotune_is_retried_not_cached(fake, threads):
+    """The first autotune of a shape fails: that request fails, the next request of the same
+    shape tunes again, and every later one gets the published tiles (no request runs its own
+    tuning or keeps the failure)."""
+    L, S, N = fake
+    L.fake_configure(0, 0.002, 100.0)
+    L.fake_fail_tunes(1)
+    srv = Server(fake, 10 ** 12, slots=4, quantum=3, threads=threads)
+    reqs = [(_cfg(N, 12, 6, 4, 300 + q), 4 + q) for q in range(8)]
+    ids = [srv.submit(c, n) for c, n in reqs]
+    _drain(srv)
+    st = srv.stats()
+    fs = srv.fake_stats()
+    assert st["failed"] == 1 and st["done"] == 7, st
+    assert fs["tunes"] == 2 and fs["live"] == 0, fs
+    failed = [r for r in ids if srv.info(r)["error"] != 0]
+    assert len(failed) == 1
+    for rid, (c, n) in zip(ids, reqs):
+        if rid in failed:
+            continue
+        assert srv.result(rid)[0][0] == c.seed * 1000 + n + 1e6 * (c.nx % 8)
     srv.close()
 
 
