@@ -3,6 +3,8 @@
 
 * ``csrc/les_f64.cu``  -- plain FP64 form, compiled with ``-fmad=false`` (no FMA
   contraction, matching the reference's x86-64 arithmetic operation for operation);
+* ``csrc/les_f64_aux.cu`` -- SEM plane, device-loop dt / rand() draws, division self-check
+  (``-fmad=false``: bit-identical to the host);
 * ``csrc/les_f32.cu``  -- FP32-bulk precision form, FMA contraction on;
 * ``csrc/les_api.cu``  -- the C ABI of ``include/les_gpu.h``;
 * ``host/*.c``         -- the C host side (solver loop, glibc-compatible rand(), SEM vortex
@@ -25,6 +27,10 @@ INC = os.path.join(ROOT, "include")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "liblesgpu.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# Units compiled without FMA contraction: the FP64 stage kernels (the reference's operation
+# order, one rounding per operation) and the shared SEM / device-loop code, whose results
+# must equal the host's bit for bit.
+FMAD_OFF = {"les_f64", "les_f64_aux"}
 
 
 def _nvcc() -> str:
@@ -88,7 +94,8 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
         obj = os.path.join(bdir, name + ".o")
         flags = [nvcc, "-c", src, "-o", obj, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                  "-I", INC, "-I", os.path.join(HERE, "csrc")] + ARCH + [f"-D{d}" for d in defines]
-        flags += ["-fmad=false"] if name.endswith("_f64") else ["-fmad=true"]
+        fmad_off = FMAD_OFF - ({"les_f64"} if "LES_F64_CONTRACT" in defines else set())
+        flags += ["-fmad=false"] if name in fmad_off else ["-fmad=true"]
         if ptxas_verbose:
             flags += ["-Xptxas", "-v"]
         r = _run(flags, verbose)

@@ -500,6 +500,8 @@ const char* lesgpu_last_error(const lesgpu_ctx* ctx) { return ctx ? ctx->d.err.c
 
 size_t lesgpu_device_bytes(const lesgpu_ctx* ctx) { return ctx ? ctx->d.total_bytes : 0; }
 
+static void drop_graph(DevCtx& d);
+
 int lesgpu_upload_attribute(lesgpu_ctx* ctx, const int* attr) {
     if (!ctx || !attr) return LESGPU_EINVAL;
     DevCtx& d = ctx->d;
@@ -534,6 +536,8 @@ int lesgpu_upload_attribute(lesgpu_ctx* ctx, const int* attr) {
     CK(cudaMemcpyAsync(d.dC, &d.hC, sizeof(les::Consts), cudaMemcpyHostToDevice, d.stream));
     CK(cudaStreamSynchronize(d.stream));
     d.have_attr = true;
+    // a captured step holds the constants (total volume, inlet count) by value
+    drop_graph(d);
     return LESGPU_OK;
 }
 
@@ -662,6 +666,18 @@ int lesgpu_dt_inputs(lesgpu_ctx* ctx, double* umax, double* numax, double* alpha
     *umax = h.umax > 1e-10 ? h.umax : ctx->cfg.inlet_velocity;   // :1484
     *numax = h.numax;
     *alphamax = h.alphamax;
+    return LESGPU_OK;
+}
+
+int lesgpu_set_dt_inputs(lesgpu_ctx* ctx, double numax, double alphamax) {
+    if (!ctx || !(numax >= 0.0) || !(alphamax >= 0.0)) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    if (!d.have_state) return fail(ctx, LESGPU_ESTATE, "no state uploaded");
+    CK(cudaMemcpyAsync((char*)d.dS + offsetof(les::Scalars, numax), &numax, sizeof(double), cudaMemcpyHostToDevice,
+                       d.stream));
+    CK(cudaMemcpyAsync((char*)d.dS + offsetof(les::Scalars, alphamax), &alphamax, sizeof(double),
+                       cudaMemcpyHostToDevice, d.stream));
+    CK(cudaStreamSynchronize(d.stream));
     return LESGPU_OK;
 }
 

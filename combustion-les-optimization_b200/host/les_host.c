@@ -779,6 +779,120 @@ int les_solver_load_checkpoint(les_solver* s, const char* path, int* t_out) {
     return LESGPU_OK;
 }
 
+/* ------------------------------------------------------------------ end of run and resume */
+
+#define LES_RESUME_MAGIC 0x5253454cu   /* "LESR" */
+
+/* les_resume.bin: magic, nv, t_loop, the rand() state, the nu/alpha maxima, nv x 7 vortices. */
+static int write_resume_sidecar(les_solver* s, const char* path) {
+    double umax = 0.0, numax = 0.0, amax = 0.0;
+    int rc = lesgpu_dt_inputs(s->ctx, &umax, &numax, &amax);
+    if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
+    FILE* fp = fopen(path, "wb");
+    if (!fp) return serr(s, LESGPU_EIO, "cannot open les_resume.bin for writing");
+    const unsigned int magic = LES_RESUME_MAGIC;
+    const int nv = s->cfg.num_vortices, t = s->t_loop;
+    const size_t nvd = (size_t)(nv > 0 ? nv : 0) * 7;
+    int ok = fwrite(&magic, sizeof magic, 1, fp) == 1 && fwrite(&nv, sizeof nv, 1, fp) == 1 &&
+             fwrite(&t, sizeof t, 1, fp) == 1 && fwrite(&s->rng, sizeof s->rng, 1, fp) == 1 &&
+             fwrite(&numax, sizeof numax, 1, fp) == 1 && fwrite(&amax, sizeof amax, 1, fp) == 1 &&
+             (nvd == 0 || fwrite(s->vort, sizeof(double), nvd, fp) == nvd);
+    fclose(fp);
+    return ok ? LESGPU_OK : serr(s, LESGPU_EIO, "short les_resume.bin write");
+}
+
+int les_solver_finish(les_solver* s, const char* dir, int mode) {
+    if (!s || !dir || (mode != LES_RESUME_REFERENCE && mode != LES_RESUME_FIXED)) return LESGPU_EINVAL;
+    if (s->loop_on) return serr(s, LESGPU_ESTATE, "end the device loop first");
+    int rc = les_solver_flush(s);
+    if (rc) return rc;
+    char path[1200];
+    /* save_quick_checkpoint(0) (:4623) -- or the step reached */
+    join_path(path, sizeof(path), dir, "checkpoint.bin");
+    rc = les_solver_save_checkpoint(s, path, mode == LES_RESUME_FIXED ? s->t_loop : 0);
+    if (rc) return rc;
+    if (s->avg_on) {                                   /* save_statistics_backup (:4624) */
+        join_path(path, sizeof(path), dir, "stats_backup.bin");
+        rc = les_solver_save_stats(s, path);
+        if (rc) return rc;
+    }
+    join_path(path, sizeof(path), dir, "les_resume.bin");
+    if (mode == LES_RESUME_FIXED) return write_resume_sidecar(s, path);
+    remove(path);                 /* no stale sidecar beside a reference-mode checkpoint */
+    return LESGPU_OK;
+}
+
+int les_solver_resume(les_solver* s, const char* dir, int mode, int* t_out) {
+    if (!s || !dir || (mode != LES_RESUME_REFERENCE && mode != LES_RESUME_FIXED)) return LESGPU_EINVAL;
+    if (s->loop_on) return serr(s, LESGPU_ESTATE, "end the device loop first");
+    char path[1200], line[256];
+    /* restart detection (:4150-4181): "BINARY" then the step on the next line */
+    join_path(path, sizeof(path), dir, "restart_info.txt");
+    FILE* fi = fopen(path, "r");
+    if (!fi) return serr(s, LESGPU_EIO, "no restart_info.txt");
+    int step = 0, binary = 0;
+    if (fgets(line, sizeof line, fi) && strncmp(line, "BINARY", 6) == 0 && fgets(line, sizeof line, fi) &&
+        sscanf(line, "%d", &step) == 1)
+        binary = 1;
+    fclose(fi);
+    if (!binary) return serr(s, LESGPU_EIO, "restart_info.txt does not name a binary checkpoint");
+    /* fixed mode: read the sidecar first, so a bad one leaves the solver untouched */
+    les_rng rng;
+    double numax = 0.0, amax = 0.0;
+    double* vort = NULL;
+    const int nv = s->cfg.num_vortices;
+    const size_t nvd = (size_t)(nv > 0 ? nv : 0) * 7;
+    if (mode == LES_RESUME_FIXED) {
+        join_path(path, sizeof(path), dir, "les_resume.bin");
+        FILE* fp = fopen(path, "rb");
+        if (!fp) return serr(s, LESGPU_EIO, "les_resume.bin missing: the checkpoint was not written by a fixed finish");
+        unsigned int magic = 0;
+        int fnv = -1, ft = 0;
+        vort = (double*)malloc(nvd ? nvd * sizeof(double) : sizeof(double));
+        int ok = vort && fread(&magic, sizeof magic, 1, fp) == 1 && magic == LES_RESUME_MAGIC &&
+                 fread(&fnv, sizeof fnv, 1, fp) == 1 && fnv == nv && fread(&ft, sizeof ft, 1, fp) == 1 &&
+                 fread(&rng, sizeof rng, 1, fp) == 1 && fread(&numax, sizeof numax, 1, fp) == 1 &&
+                 fread(&amax, sizeof amax, 1, fp) == 1 && (nvd == 0 || fread(vort, sizeof(double), nvd, fp) == nvd);
+        fclose(fp);
+        if (!ok) { free(vort); return serr(s, LESGPU_EIO, "les_resume.bin does not match this solver"); }
+    }
+    /* load_quick_checkpoint (:3701-3726); the run continues from the step stored in it (:4189) */
+    join_path(path, sizeof(path), dir, "checkpoint.bin");
+    int t = 0;
+    int rc = les_solver_load_checkpoint(s, path, &t);
+    if (rc) { free(vort); return rc; }
+    if (s->avg_on) {                                   /* load_statistics_backup (:4190) */
+        join_path(path, sizeof(path), dir, "stats_backup.bin");
+        FILE* fs = fopen(path, "rb");
+        if (fs) {
+            fclose(fs);
+            rc = les_solver_load_stats(s, path);
+            if (rc) { free(vort); return rc; }
+        }
+    }
+    if (mode == LES_RESUME_REFERENCE) {
+        /* initialize_vortices (:4193) after the start-up srand(seed) (:4085) */
+        les_rng_seed(&s->rng, s->cfg.seed);
+        les_vortices_init(&s->rng, &s->cfg, s->vort);
+        /* the start-up attribute map (:4123-4136): setting() does not run on a resume, so the
+           j = 0 face keeps code 4 instead of the symmetry code 5 (and no rim code 6) */
+        for (size_t c = 0; c < s->n; c++)
+            if (s->attr[c] == 5 || s->attr[c] == 6) s->attr[c] = 4;
+        rc = lesgpu_upload_attribute(s->ctx, s->attr);
+        if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
+        /* the nu/alpha maxima stay 0, as the state upload of les_solver_load_checkpoint left them */
+    } else {
+        s->rng = rng;
+        if (nvd) memcpy(s->vort, vort, nvd * sizeof(double));
+        free(vort);
+        rc = lesgpu_set_dt_inputs(s->ctx, numax, amax);
+        if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
+    }
+    s->t_loop = t;
+    if (t_out) *t_out = t;
+    return LESGPU_OK;
+}
+
 /* ------------------------------------------------------------------ time averages */
 
 int les_solver_set_averaging(les_solver* s, int start_step) {

@@ -37,6 +37,11 @@ AVG_NAMES = ["u", "v", "w", "uu", "vv", "ww", "uv", "uw", "vw", "G"]
 STRESS_NAMES = ["uu", "vv", "ww", "uv", "uw", "vw", "G_mean"]
 
 
+# les_solver_finish / les_solver_resume modes (les_solver.h)
+RESUME_REFERENCE = 0
+RESUME_FIXED = 1
+
+
 class LesgpuError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"{ERRORS.get(code, code)}: {msg}")
@@ -184,6 +189,9 @@ def lib():
         _sig(L, "les_solver_load_checkpoint", C.c_int, [vp, C.c_char_p, C.POINTER(C.c_int)])
         _sig(L, "les_solver_vortices", C.c_int, [vp, dp])
         _sig(L, "les_solver_rng_draws", C.c_ulonglong, [vp])
+        _sig(L, "les_solver_finish", C.c_int, [vp, C.c_char_p, C.c_int])
+        _sig(L, "les_solver_resume", C.c_int, [vp, C.c_char_p, C.c_int, C.POINTER(C.c_int)])
+        _sig(L, "lesgpu_set_dt_inputs", C.c_int, [vp, C.c_double, C.c_double])
         _lib = L
     return _lib
 
@@ -457,6 +465,18 @@ class Solver:
 
     def loop_begin(self, chunk: int = 64):
         self._check(lib().les_solver_loop_begin(self._h, chunk), "loop_begin")
+
+    def finish(self, directory: str, mode: int = 0):
+        """End-of-run writes (checkpoint.bin, restart_info.txt, ...); mode RESUME_REFERENCE
+        saves step 0 as the reference does, RESUME_FIXED the step reached plus les_resume.bin."""
+        self._check(lib().les_solver_finish(self._h, directory.encode(), mode), "finish")
+
+    def resume(self, directory: str, mode: int = 0) -> int:
+        """The reference's auto-resume from `directory` (RESUME_REFERENCE keeps its defects,
+        RESUME_FIXED continues the run exactly); returns the step the run continues from."""
+        t = C.c_int(0)
+        self._check(lib().les_solver_resume(self._h, directory.encode(), mode, C.byref(t)), "resume")
+        return t.value
 
     def set_averaging(self, start_step: int):
         """Sum the time averages from t_loop >= start_step on (< 0: off)."""

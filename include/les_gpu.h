@@ -117,6 +117,12 @@ int lesgpu_get_field(lesgpu_ctx* ctx, int field_id, double* out);
  * RHS evaluation (0 before the first step). */
 int lesgpu_dt_inputs(lesgpu_ctx* ctx, double* umax, double* numax, double* alphamax);
 
+/* No counterpart in the reference (its nu/alpha arrays are never saved): sets the nu and
+ * alpha maxima that the next dt reads, as lesgpu_dt_inputs returned them before a
+ * checkpoint, so a run resumed from that checkpoint takes the same dt as the uninterrupted
+ * one.  Call after lesgpu_upload_state, which resets them to 0. */
+int lesgpu_set_dt_inputs(lesgpu_ctx* ctx, double numax, double alphamax);
+
 /* SEM inflow for the next step (:943-1075 and the white noise of :2987-2997).
  * vortices: nv x {x, y, z, radius, strength_u, strength_v, strength_w} after the host's
  *           update_vortices (:900-939) for this step's dt;

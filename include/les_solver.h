@@ -101,6 +101,32 @@ int les_solver_attribute(const les_solver* s, int* out);
 int les_solver_save_checkpoint(les_solver* s, const char* path, int t);
 int les_solver_load_checkpoint(les_solver* s, const char* path, int* t_out);
 
+/* End of a run (:4604-4623) and the reference's auto-resume from restart_info.txt +
+ * checkpoint.bin (:4138-4193), with the reference's resume defects kept or fixed:
+ *
+ * LES_RESUME_REFERENCE -- what the reference does, defects included:
+ *   - les_solver_finish writes checkpoint.bin and restart_info.txt with step 0 whatever step
+ *     was reached (save_quick_checkpoint(0), :4623), so the resumed run starts its step count
+ *     (and the t_loop >= 500 switch to the WENO5 flame-front gradient) again at 0;
+ *   - les_solver_resume re-seeds rand() with the configured seed and redraws the SEM
+ *     vortices (initialize_vortices after the load, :4193) instead of continuing the stream;
+ *   - it installs the start-up attribute map (:4123-4136), because a resume never runs
+ *     setting(): the j = 0 face is a wall/free face (code 4), not the symmetry plane (code 5);
+ *   - the nu/alpha maxima of the first dt after the resume are 0 (not restored, :4401-4408).
+ * LES_RESUME_FIXED -- les_solver_finish writes the step reached and, beside checkpoint.bin,
+ *   les_resume.bin (the SEM vortices, the rand() state and the nu/alpha maxima);
+ *   les_solver_resume restores all of it and keeps setting()'s attribute map, so the resumed
+ *   run continues the uninterrupted one exactly.
+ *
+ * finish also writes what les_solver_flush writes and stats_backup.bin when time averages
+ * are on (:4611-4625).  resume reads `dir`/restart_info.txt ("BINARY\n<step>\n"),
+ * checkpoint.bin (the step the run continues from is the one stored in it, as :4189 takes)
+ * and, with averages on, stats_backup.bin; t_out receives that step. */
+#define LES_RESUME_REFERENCE 0
+#define LES_RESUME_FIXED 1
+int les_solver_finish(les_solver* s, const char* dir, int mode);
+int les_solver_resume(les_solver* s, const char* dir, int mode, int* t_out);
+
 /* Time averages (update_time_averages, :3166-3191) summed on the device from the step whose
  * t_loop reaches start_step (the reference's start_avg_step); start_step < 0 turns them off.
  * save/load: stats_backup.bin (:3736-3778); reynolds_stresses: the seven fields of

@@ -191,8 +191,14 @@ def ref_available(name: str) -> bool:
 
 def run_reference(name: str, steps: int, seed: int = 1234, start: int = 0, dump_every: int = 1,
                   rhs_dump_step: int = -1, threads: int = 1, env_extra: Optional[Dict] = None,
-                  keep_dir: Optional[str] = None, novtk: bool = True, timeout: float = 3600.0):
+                  keep_dir: Optional[str] = None, novtk: bool = True, timeout: float = 3600.0,
+                  binary: Optional[str] = None, resume: bool = False):
     """Run the compiled reference for ``steps`` steps in a scratch directory.
+
+    ``binary`` runs another build of the same grid instead (the reference with the GPU
+    drop-in spliced into its loop, tests/dropin/build_dropin.py); it reads the same
+    environment and writes the same files.  ``resume`` keeps an existing restart_info.txt in
+    ``keep_dir``, so the reference auto-resumes from the checkpoint there (:4150-4193).
 
     Returns ``(dumps, meta)``: ``dumps[n]`` is the state after ``n`` steps (dict of
     arrays + 'dt'), ``meta`` holds the per-step wall times, probe CSV texts and the monitor
@@ -200,7 +206,7 @@ def run_reference(name: str, steps: int, seed: int = 1234, start: int = 0, dump_
     """
     from build_ref import CONFIGS, STATE_FIELDS, RHS1_FIELDS  # noqa: local module
     cfg = CONFIGS[name]
-    exe = os.path.join(REF_ROOT, name, "les_ref")
+    exe = binary or os.path.join(REF_ROOT, name, "les_ref")
     if not os.path.exists(exe):
         raise FileNotFoundError(exe)
     work = keep_dir or tempfile.mkdtemp(prefix=f"lesref_{name}_")
@@ -208,7 +214,7 @@ def run_reference(name: str, steps: int, seed: int = 1234, start: int = 0, dump_
     for fn in ("chem.bin", "tran.bin"):
         shutil.copyfile(os.path.join(REF_ROOT, name, fn), os.path.join(work, fn))
     rinfo = os.path.join(work, "restart_info.txt")
-    if os.path.exists(rinfo):
+    if os.path.exists(rinfo) and not resume:
         os.remove(rinfo)          # the reference auto-resumes when this file exists
     env = dict(os.environ)
     env.update({"OMP_NUM_THREADS": str(threads), "LES_REF_STEPS": str(steps),

@@ -23,6 +23,8 @@ import os
 import numpy as np
 import pytest
 
+from refcompare import compare_probes, read_probe_texts, rel
+
 pytestmark = pytest.mark.gpu
 
 STATE = ["u", "v", "w", "T", "G", "rho", "Y0", "Y1", "Y2", "Y3", "Y4"]
@@ -30,39 +32,6 @@ EXTRA = ["nu_t", "S_mag"]
 TOL_1 = 1e-10
 TOL_10 = 1e-8
 TOL_DT = 1e-13
-
-
-def rel(a, b):
-    nb = np.linalg.norm(b)
-    return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
-
-
-def _parse_probe(text):
-    rows = [ln.split(",") for ln in text.splitlines()[1:] if ln.strip()]
-    return np.array([[float(x) for x in r] for r in rows]).reshape(-1, 11)
-
-
-def _compare_probes(gpu_dir, ref_probes):
-    worst = 0.0
-    for n in range(7):
-        path = os.path.join(gpu_dir, f"probe_data_flame_region_loc{n}.csv")
-        ref_txt = ref_probes.get(n)
-        if ref_txt is None:
-            assert not os.path.exists(path), f"station {n}: GPU wrote rows the reference did not"
-            continue
-        with open(path) as f:
-            gpu_txt = f.read()
-        a, b = _parse_probe(gpu_txt), _parse_probe(ref_txt)
-        assert a.shape == b.shape, f"station {n}: {a.shape[0]} rows against the reference's {b.shape[0]}"
-        # timestep, x, y_flame, y, y_rel, u, v, w, G at %.6f: one unit of the 6th decimal
-        d_fixed = np.abs(a[:, :9] - b[:, :9]).max(initial=0.0)
-        assert d_fixed <= 1.01e-6, f"station {n}: fixed-point columns differ by {d_fixed:.3e}"
-        # nu_t, |S| at %.6e: one unit of the 7th significant digit
-        scale = np.maximum(np.abs(b[:, 9:]), 1e-300)
-        d_exp = (np.abs(a[:, 9:] - b[:, 9:]) / scale).max(initial=0.0)
-        assert d_exp <= 1.01e-6, f"station {n}: nu_t/S_mag differ by {d_exp:.3e} relative"
-        worst = max(worst, d_fixed)
-    return worst
 
 
 def _run_case(N, oracle_mod, grid, steps, keep, tmp_path):
@@ -101,7 +70,7 @@ def _run_case(N, oracle_mod, grid, steps, keep, tmp_path):
         print(f"[{grid}] step {n}: worst rel L2 {errs[k]:.3e} ({k}); "
               + ", ".join(f"{f} {errs[f]:.1e}" for f in STATE + EXTRA))
         assert errs[k] <= tol, f"{grid} step {n}: {k} rel L2 {errs[k]:.3e} > {tol}"
-    pw = _compare_probes(str(gdir), meta["probes"])
+    pw = compare_probes(read_probe_texts(str(gdir)), meta["probes"])
     print(f"[{grid}] probe rows after {steps} steps: identical row sets, max |diff| {pw:.2e}")
 
 

@@ -1,6 +1,9 @@
 """The C examples of the integration notes compile against include/*.h (syntax and types;
-gcc -fsyntax-only, no GPU).  The first example uses the reference's own globals and is
-skipped; the others are wrapped in a function with the few names they take as given."""
+gcc -fsyntax-only, no GPU).  The first example is written against the reference's own
+globals: it is spliced into the reference source by tests/dropin/build_dropin.py and
+compiled there (below, when the reference source is present; tests/test_gpu_dropin.py runs
+the result on a GPU).  The others are wrapped in a function with the few names they take as
+given."""
 import os
 import re
 import shutil
@@ -42,3 +45,24 @@ def test_examples_compile(tmp_path):
                             "-Wno-unused-but-set-variable", "-I", os.path.join(ROOT, "include"), str(src)],
                            capture_output=True, text=True)
         assert r.returncode == 0, f"example {n}:\n{r.stderr}"
+
+
+def test_first_example_compiles_inside_the_reference(tmp_path):
+    """The drop-in block of the first example, spliced into the reference's own source, is
+    valid C against les_gpu.h (every patch site matched exactly once)."""
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "tests", "dropin"))
+    import build_dropin
+    ref = build_dropin.build_ref.default_ref()
+    src_path = os.path.join(ref, "les_combustion_solver.c")
+    if not os.path.exists(src_path) or shutil.which("gcc") is None:
+        pytest.skip("reference source or gcc not present")
+    with open(src_path, encoding="utf-8") as f:
+        patched = build_dropin.patch_dropin(f.read(), build_dropin.build_ref.CONFIGS["c1"])
+    assert "gpu_step(t_loop, &DT_sim, &max_velocity)" in patched
+    assert "calculate_RHS(t_loop, u_temp" not in patched.split("for (int t_loop")[1].split("lesgpu_destroy")[0]
+    src = tmp_path / "dropin.c"
+    src.write_text(patched)
+    r = subprocess.run(["gcc", "-fsyntax-only", "-fopenmp", "-w", "-I", os.path.join(ROOT, "include"), str(src)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
