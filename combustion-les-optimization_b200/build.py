@@ -30,7 +30,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # Units compiled without FMA contraction: the FP64 stage kernels (the reference's operation
 # order, one rounding per operation) and the shared SEM / device-loop code, whose results
 # must equal the host's bit for bit.
-FMAD_OFF = {"les_f64", "les_f64_aux"}
+FMAD_OFF = {"les_f64", "les_f64_aux", "les_pstat"}
 
 
 def _nvcc() -> str:

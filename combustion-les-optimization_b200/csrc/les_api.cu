@@ -481,7 +481,8 @@ void lesgpu_destroy(lesgpu_ctx* ctx) {
     if (d.side) cudaStreamSynchronize(d.side);
     // every buffer was allocated on d.stream, which exists whenever one of them does
     void* bufs[] = {d.arena_raw, d.attr, d.dC, d.dS, d.part, d.plane, d.noise, d.vort, d.inlet_list, d.inlet_pos,
-                    d.probe_st, d.probe_out, d.flag, d.dbg_cp, d.dbg_lam, d.dbg_alpha, d.avg, d.grad_g};
+                    d.probe_st, d.probe_out, d.flag, d.dbg_cp, d.dbg_lam, d.dbg_alpha, d.avg, d.grad_g,
+                    d.ps_edges, d.ps_sums, d.ps_yflame, d.ps_rowbin};
     for (void* b : bufs) dfree(d, b);
     for (int q = 0; q < les::NACC; q++) dfree(d, d.kd[q]);
     if (d.h_pinned) cudaFreeHost(d.h_pinned);
@@ -1097,6 +1098,94 @@ int lesgpu_keep_grad_g(lesgpu_ctx* ctx, int enable) {
         d.total_bytes -= d.n * d.esz;
     }
     drop_graph(d);
+    return LESGPU_OK;
+}
+
+// ---------------------------------------------------------------- profile statistics
+
+static void pstat_free(DevCtx& d) {
+    void* bufs[] = {d.ps_edges, d.ps_sums, d.ps_yflame, d.ps_rowbin};
+    for (void* b : bufs) dfree(d, b);
+    d.ps_edges = d.ps_sums = d.ps_yflame = nullptr;
+    d.ps_rowbin = nullptr;
+    d.ps_rows_cap = 0;
+    d.ps_nsums = 0;
+    d.ps_on = false;
+}
+
+static bool increasing(const double* e, int n) {
+    for (int q = 0; q < n; q++)
+        if (!(e[q] < e[q + 1])) return false;
+    return true;
+}
+
+int lesgpu_pstat_begin(lesgpu_ctx* ctx, const double* y_edges_mm, int n_y, const double* g_rc_edges, int n_grc,
+                       const double* g_ho_edges, int n_gho, const double* u_edges, const double* v_edges, int n_pdf) {
+    if (!ctx || !y_edges_mm || !g_rc_edges || !g_ho_edges || !u_edges || !v_edges) return LESGPU_EINVAL;
+    if (n_y < 1 || n_grc < 1 || n_gho < 1 || n_pdf < 1 || n_y > 4096 || n_grc > 4096 || n_gho > 4096 || n_pdf > 4096)
+        return fail(ctx, LESGPU_EINVAL, "bin counts must be in 1..4096");
+    if (!increasing(y_edges_mm, n_y) || !increasing(g_rc_edges, n_grc) || !increasing(g_ho_edges, n_gho) ||
+        !increasing(u_edges, n_pdf) || !increasing(v_edges, n_pdf))
+        return fail(ctx, LESGPU_EINVAL, "bin edges must increase");
+    DevCtx& d = ctx->d;
+    CK(cudaStreamSynchronize(d.stream));
+    pstat_free(d);
+    std::vector<double> e;
+    e.insert(e.end(), y_edges_mm, y_edges_mm + n_y + 1);
+    e.insert(e.end(), g_rc_edges, g_rc_edges + n_grc + 1);
+    e.insert(e.end(), g_ho_edges, g_ho_edges + n_gho + 1);
+    e.insert(e.end(), u_edges, u_edges + n_pdf + 1);
+    e.insert(e.end(), v_edges, v_edges + n_pdf + 1);
+    d.ps_ny = n_y; d.ps_ngrc = n_grc; d.ps_ngho = n_gho; d.ps_npdf = n_pdf;
+    d.ps_nsums = 4 + 9 * (size_t)n_y + 7 * (size_t)n_grc + 4 * (size_t)n_gho + 4 * (size_t)n_pdf;
+    CK(dalloc(d, &d.ps_edges, e.size() * sizeof(double)));
+    CK(dalloc(d, &d.ps_sums, d.ps_nsums * sizeof(double)));
+    CK(cudaMemcpyAsync(d.ps_edges, e.data(), e.size() * sizeof(double), cudaMemcpyHostToDevice, d.stream));
+    CK(cudaMemsetAsync(d.ps_sums, 0, d.ps_nsums * sizeof(double), d.stream));
+    CK(cudaStreamSynchronize(d.stream));
+    d.ps_on = true;
+    return LESGPU_OK;
+}
+
+int lesgpu_pstat_accumulate(lesgpu_ctx* ctx, int nsteps, int n_lines) {
+    if (!ctx || nsteps < 0 || n_lines < 0) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    if (!d.ps_on) return fail(ctx, LESGPU_ESTATE, "lesgpu_pstat_begin first");
+    if (!d.loop_ready || !d.hist_probe) return fail(ctx, LESGPU_ESTATE, "no device-loop history");
+    if (nsteps > d.loop_cap || n_lines > d.loop_nst)
+        return fail(ctx, LESGPU_EINVAL, "more steps or lines than the history holds");
+    if (nsteps == 0 || n_lines == 0) return LESGPU_OK;
+    const size_t rows = (size_t)d.loop_cap * d.loop_nst * d.ny;
+    if (rows > d.ps_rows_cap) {          // scratch sized for the whole history once
+        dfree(d, d.ps_yflame);
+        dfree(d, d.ps_rowbin);
+        d.ps_yflame = nullptr;
+        d.ps_rowbin = nullptr;
+        CK(dalloc(d, &d.ps_yflame, (size_t)d.loop_cap * d.loop_nst * sizeof(double)));
+        CK(dalloc(d, &d.ps_rowbin, rows * 5 * sizeof(int)));
+        d.ps_rows_cap = rows;
+    }
+    cudaError_t e = les::pstat_accumulate(d, nsteps, n_lines);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "pstat_accumulate");
+    return LESGPU_OK;
+}
+
+size_t lesgpu_pstat_size(const lesgpu_ctx* ctx) { return (ctx && ctx->d.ps_on) ? ctx->d.ps_nsums : 0; }
+
+int lesgpu_pstat_read(lesgpu_ctx* ctx, double* out) {
+    if (!ctx || !out) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    if (!d.ps_on) return fail(ctx, LESGPU_ESTATE, "lesgpu_pstat_begin first");
+    CK(cudaStreamSynchronize(d.stream));
+    CK(cudaMemcpy(out, d.ps_sums, d.ps_nsums * sizeof(double), cudaMemcpyDeviceToHost));
+    return LESGPU_OK;
+}
+
+int lesgpu_pstat_end(lesgpu_ctx* ctx) {
+    if (!ctx) return LESGPU_EINVAL;
+    DevCtx& d = ctx->d;
+    CK(cudaStreamSynchronize(d.stream));
+    pstat_free(d);
     return LESGPU_OK;
 }
 

@@ -112,6 +112,16 @@ struct DevCtx {
     // time averages (lesgpu_avg_*): NAVG running sums, FP64, in one allocation
     double* avg = nullptr;
     int avg_start = 0;
+    // profile statistics of the probe rows (lesgpu_pstat_*, les_pstat.cu): bin edges, the
+    // running moment sums, and per-row scratch for one history chunk
+    bool ps_on = false;
+    int ps_ny = 0, ps_ngrc = 0, ps_ngho = 0, ps_npdf = 0;   // bins of each kind
+    double* ps_edges = nullptr;         // y (mm), G right-closed, G half-open, u, v edges
+    double* ps_sums = nullptr;          // moment sums (lesgpu_pstat_read layout)
+    size_t ps_nsums = 0;
+    double* ps_yflame = nullptr;        // y_flame per history line (cap x lines)
+    int* ps_rowbin = nullptr;           // 5 bin indices per row (cap x lines x NY)
+    size_t ps_rows_cap = 0;
     // kernel timing: event pairs recorded around each kernel class during a step
     bool timing = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -127,6 +137,10 @@ struct DevCtx {
 struct TmaMapsStorage {
     unsigned char b[7 * 128];
 };
+
+// Profile statistics (les_pstat.cu): accumulate the rows of the last nsteps history slots
+// (the first m lines, the probe stations) into ps_sums, on the context's stream.
+cudaError_t pstat_accumulate(DevCtx& c, int nsteps, int m);
 
 // Kernel-timing helpers (les_api.cu): tmark_begin returns a pair slot or -1.
 int tmark_begin(DevCtx& c, int cls);

@@ -80,6 +80,8 @@ struct les_solver {
     double* pt_buf[4];    /* PT_MAX x {u, v, w, G} */
     /* time averages (lesgpu_avg_*) */
     int avg_on, avg_start;
+    /* profile statistics on the device (lesgpu_pstat_*) */
+    int ps_on;
     /* device-loop session (les_solver_loop_*) */
     int loop_on, l_chunk, l_m, l_lines;
     int l_st[LES_MAX_LINES], l_slot[LES_MAX_LINES];
@@ -643,6 +645,11 @@ int les_solver_loop_collect(les_solver* s, int n) {
     int rc = lesgpu_loop_history(s->ctx, n, s->l_dt, s->l_umax, (want_probes || want_points) ? s->l_probe : NULL,
                                  want_mon ? s->l_mon : NULL);
     if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
+    /* the rows of this chunk into the device statistics, before the next chunk reuses the slots */
+    if (s->ps_on && m > 0) {
+        rc = lesgpu_pstat_accumulate(s->ctx, n, m);
+        if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
+    }
     for (int q = 0; q < n; q++) {
         const int t = s->t_loop + q;
         const double* lines = s->l_probe + (size_t)q * L * s->ny * 6;
@@ -776,6 +783,48 @@ int les_solver_load_checkpoint(les_solver* s, const char* path, int* t_out) {
     free_fields(f);
     if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
     if (t_out) *t_out = t;
+    return LESGPU_OK;
+}
+
+/* ------------------------------------------------------------------ device profile statistics */
+
+int les_solver_pstat_begin(les_solver* s, const double* y_edges_mm, int n_y, const double* g_rc_edges, int n_grc,
+                           const double* g_ho_edges, int n_gho, const double* u_edges, const double* v_edges,
+                           int n_pdf) {
+    if (!s) return LESGPU_EINVAL;
+    if (s->loop_on) return serr(s, LESGPU_ESTATE, "end the device loop before starting the statistics");
+    int rc;
+    if (y_edges_mm && g_rc_edges && g_ho_edges && u_edges && v_edges) {
+        rc = lesgpu_pstat_begin(s->ctx, y_edges_mm, n_y, g_rc_edges, n_grc, g_ho_edges, n_gho, u_edges, v_edges, n_pdf);
+    } else {
+        /* defaults; edges are start + b * step, as numpy's arange and linspace compute them */
+        const double ly_mm = 1000.0 * s->cfg.ly, U = s->cfg.inlet_velocity;
+        const int ny_b = (int)(2.0 * ly_mm / 0.5 + 0.5), ng = 20, np_ = 40;
+        double* e = (double*)malloc((size_t)(ny_b + 1 + 2 * (ng + 1) + 2 * (np_ + 1)) * sizeof(double));
+        if (!e) return serr(s, LESGPU_ENOMEM, "host buffers");
+        double *ey = e, *erc = ey + ny_b + 1, *eho = erc + ng + 1, *eu = eho + ng + 1, *ev = eu + np_ + 1;
+        for (int b = 0; b <= ny_b; b++) ey[b] = -ly_mm + b * 0.5;
+        for (int b = 0; b <= ng; b++) erc[b] = b * 0.05;
+        for (int b = 0; b < ng; b++) eho[b] = b * (1.0 / ng);
+        eho[ng] = 1.0;
+        for (int b = 0; b < np_; b++) { eu[b] = -U + b * (4.0 * U / np_); ev[b] = -2.0 * U + b * (4.0 * U / np_); }
+        eu[np_] = 3.0 * U;
+        ev[np_] = 2.0 * U;
+        rc = lesgpu_pstat_begin(s->ctx, ey, ny_b, erc, ng, eho, ng, eu, ev, np_);
+        free(e);
+    }
+    if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
+    s->ps_on = 1;
+    return LESGPU_OK;
+}
+
+size_t les_solver_pstat_size(const les_solver* s) { return (s && s->ps_on) ? lesgpu_pstat_size(s->ctx) : 0; }
+
+int les_solver_pstat_read(les_solver* s, double* out) {
+    if (!s || !out) return LESGPU_EINVAL;
+    if (!s->ps_on) return serr(s, LESGPU_ESTATE, "les_solver_pstat_begin first");
+    int rc = lesgpu_pstat_read(s->ctx, out);
+    if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
     return LESGPU_OK;
 }
 

@@ -192,6 +192,9 @@ def lib():
         _sig(L, "les_solver_finish", C.c_int, [vp, C.c_char_p, C.c_int])
         _sig(L, "les_solver_resume", C.c_int, [vp, C.c_char_p, C.c_int, C.POINTER(C.c_int)])
         _sig(L, "lesgpu_set_dt_inputs", C.c_int, [vp, C.c_double, C.c_double])
+        _sig(L, "les_solver_pstat_begin", C.c_int, [vp, dp, C.c_int, dp, C.c_int, dp, C.c_int, dp, dp, C.c_int])
+        _sig(L, "les_solver_pstat_size", C.c_size_t, [vp])
+        _sig(L, "les_solver_pstat_read", C.c_int, [vp, dp])
         _lib = L
     return _lib
 
@@ -477,6 +480,30 @@ class Solver:
         t = C.c_int(0)
         self._check(lib().les_solver_resume(self._h, directory.encode(), mode, C.byref(t)), "resume")
         return t.value
+
+    def pstat_begin(self, edges: Optional[Dict[str, np.ndarray]] = None) -> Dict[str, np.ndarray]:
+        """Accumulate the probe-row statistics on the device during device-loop runs; returns
+        the edges in use (stats.default_edges when none are given)."""
+        from . import stats
+        e = edges or stats.default_edges(self.cfg.ly, self.cfg.inlet_velocity)
+        a = {k: np.ascontiguousarray(e[k], dtype=np.float64) for k in ("y_mm", "g_rc", "g_ho", "u", "v")}
+        assert len(a["u"]) == len(a["v"])
+        self._check(lib().les_solver_pstat_begin(self._h, a["y_mm"].ctypes.data, len(a["y_mm"]) - 1,
+                                                 a["g_rc"].ctypes.data, len(a["g_rc"]) - 1, a["g_ho"].ctypes.data,
+                                                 len(a["g_ho"]) - 1, a["u"].ctypes.data, a["v"].ctypes.data,
+                                                 len(a["u"]) - 1), "pstat_begin")
+        self._pstat_edges = a
+        return a
+
+    def pstat_read(self) -> np.ndarray:
+        out = np.empty(lib().les_solver_pstat_size(self._h))
+        self._check(lib().les_solver_pstat_read(self._h, out.ctypes.data), "pstat_read")
+        return out
+
+    def profile_stats(self) -> Dict:
+        """The device-accumulated statistics (stats.from_moments of pstat_read)."""
+        from . import stats
+        return stats.from_moments(self.pstat_read(), self._pstat_edges)
 
     def set_averaging(self, start_step: int):
         """Sum the time averages from t_loop >= start_step on (< 0: off)."""

@@ -20,6 +20,9 @@ form states against the FP64 form:
 
 Rows are read from the CSV files (``read_probe_csv``) or built from the device loop's probe
 history.  All statistics are computed in float64 with numpy.
+
+``from_moments`` turns the moment sums that the solver accumulates on the device
+(``lesgpu_pstat_*``, no probe files) into the same four statistics.
 """
 from __future__ import annotations
 
@@ -189,3 +192,107 @@ def compare_profiles(rows_a: Dict[str, np.ndarray], rows_b: Dict[str, np.ndarray
     for k in pa:
         err[f"pdf.{k}"] = profile_error(pa[k], pb[k])
     return err
+
+
+# ----------------------------------------------------------------- device moment sums
+
+def default_edges(ly: float, inlet_velocity: float) -> Dict[str, np.ndarray]:
+    """The bins les_solver_pstat_begin uses when given no edges (start + b * step)."""
+    ly_mm = 1000.0 * ly
+    ny_b = int(2.0 * ly_mm / 0.5 + 0.5)
+    U = inlet_velocity
+    e = {"y_mm": -ly_mm + np.arange(ny_b + 1) * 0.5,
+         "g_rc": np.arange(21) * 0.05,
+         "g_ho": np.append(np.arange(20) * (1.0 / 20), 1.0),
+         "u": np.append(-U + np.arange(40) * (4.0 * U / 40), 3.0 * U),
+         "v": np.append(-2.0 * U + np.arange(40) * (4.0 * U / 40), 2.0 * U)}
+    return e
+
+
+def moments_size(edges: Dict[str, np.ndarray]) -> int:
+    ny, nrc, nho, npdf = (len(edges[k]) - 1 for k in ("y_mm", "g_rc", "g_ho", "u"))
+    return 4 + 9 * ny + 7 * nrc + 4 * nho + 4 * npdf
+
+
+def from_moments(sums: np.ndarray, edges: Dict[str, np.ndarray]) -> Dict[str, Dict]:
+    """The statistics of ``flame_profile(rows, edges['y_mm'])``, ``stress_vs_g``, ``uv_vs_g``
+    and ``conditional_pdfs(rows, edges['u'], edges['v'])`` from the device moment sums (layout
+    of lesgpu_pstat_read).  Means of squared fluctuations come from the raw moments:
+    <(x - m)^2> = <x^2> - 2 m <x> + m^2."""
+    s = np.asarray(sums, dtype=np.float64)
+    ny, nrc, nho, npdf = (len(edges[k]) - 1 for k in ("y_mm", "g_rc", "g_ho", "u"))
+    if len(s) != moments_size(edges):
+        raise ValueError("moment vector does not match the edges")
+    N, su, sv, sw = s[0:4]
+    out = {}
+    # flame_profile: fluctuations about the global means
+    Y = s[4:4 + 9 * ny].reshape(ny, 9)
+    occ = Y[:, 0] > 0
+    n = Y[occ, 0]
+    mu, mv, mw = (su / N, sv / N, sw / N) if N > 0 else (0.0, 0.0, 0.0)
+    fp = {"bin_center": (0.5 * (edges["y_mm"][:-1] + edges["y_mm"][1:]))[occ],
+          "u": Y[occ, 1] / n, "v": Y[occ, 2] / n, "w": Y[occ, 3] / n, "G": Y[occ, 4] / n,
+          "re_uu": (Y[occ, 5] - 2.0 * mu * Y[occ, 1]) / n + mu * mu,
+          "re_vv": (Y[occ, 6] - 2.0 * mv * Y[occ, 2]) / n + mv * mv,
+          "re_ww": (Y[occ, 7] - 2.0 * mw * Y[occ, 3]) / n + mw * mw,
+          "re_uv": (Y[occ, 8] - mv * Y[occ, 1] - mu * Y[occ, 2]) / n + mu * mv}
+    out["flame_profile"] = fp
+    # stress_vs_g: fluctuations about the per-bin means
+    o = 4 + 9 * ny
+    Rc = s[o:o + 7 * nrc].reshape(nrc, 7)
+    occ = Rc[:, 0] > 0
+    n = Rc[occ, 0]
+    bu, bv, bw = Rc[occ, 1] / n, Rc[occ, 2] / n, Rc[occ, 3] / n
+    out["stress_vs_g"] = {"uu_cond": Rc[occ, 4] / n - bu * bu, "vv_cond": Rc[occ, 5] / n - bv * bv,
+                          "uv_cond": Rc[occ, 6] / n - bu * bv, "u_mean": bu, "v_mean": bv, "w_mean": bw,
+                          "G_center": (0.5 * (edges["g_rc"][:-1] + edges["g_rc"][1:]))[occ]}
+    # uv_vs_g: bins with fewer than 10 rows are NaN
+    o += 7 * nrc
+    Ho = s[o:o + 4 * nho].reshape(nho, 4)
+    stress = np.full(nho, np.nan)
+    ok = Ho[:, 0] >= 10
+    n = Ho[ok, 0]
+    stress[ok] = Ho[ok, 3] / n - (Ho[ok, 1] / n) * (Ho[ok, 2] / n)
+    out["uv_vs_g"] = (0.5 * (edges["g_ho"][:-1] + edges["g_ho"][1:]), stress)
+    # conditional PDFs: density-normalised histograms
+    o += 4 * nho
+    H = s[o:o + 4 * npdf].reshape(4, npdf)
+    pdfs = {}
+    for q, (k, tag) in enumerate((("u", "unburnt"), ("v", "unburnt"), ("u", "burnt"), ("v", "burnt"))):
+        c = H[q]
+        w = np.diff(edges[k])
+        tot = c.sum()
+        pdfs[f"{k}_{tag}"] = c / (tot * w) if tot > 0 else np.zeros(npdf)
+    out["conditional_pdfs"] = pdfs
+    return out
+
+
+def probe_rows(lines: np.ndarray, t0: int, dy: float, x_locations: np.ndarray) -> Dict[str, np.ndarray]:
+    """Rows of record_flame_region_data (les_combustion_solver.c:3419-3466) at full precision,
+    from probe lines shaped (steps, stations, NY, 6) = u, v, w, G, nu_t, S_mag."""
+    cols = {c: [] for c in COLUMNS}
+    steps, nst, ny, _ = lines.shape
+    for q in range(steps):
+        for n in range(nst):
+            G = lines[q, n, :, 3]
+            y_flame = -1.0
+            for j in range(ny - 1):
+                G1, G2 = G[j], G[j + 1]
+                if (G1 - 0.5) * (G2 - 0.5) <= 0.0:
+                    y1, y2 = j * dy, (j + 1) * dy
+                    y_flame = y1 if abs(G2 - G1) < 1e-9 else y1 + (0.5 - G1) / (G2 - G1) * (y2 - y1)
+                    break
+            if not y_flame > 0.0:
+                continue
+            yp = np.arange(ny) * dy
+            yr = yp - y_flame
+            keep = np.abs(yr) <= 1.0
+            k = int(keep.sum())
+            cols["timestep"].append(np.full(k, float(t0 + q)))
+            cols["x_location"].append(np.full(k, x_locations[n]))
+            cols["y_flame"].append(np.full(k, y_flame))
+            cols["y_physical"].append(yp[keep])
+            cols["y_relative"].append(yr[keep])
+            for c, idx in (("u", 0), ("v", 1), ("w", 2), ("G", 3), ("nu_t", 4), ("S_mag", 5)):
+                cols[c].append(lines[q, n, keep, idx])
+    return {c: (np.concatenate(v) if v else np.zeros(0)) for c, v in cols.items()}

@@ -197,6 +197,29 @@ int lesgpu_monitor(lesgpu_ctx* ctx, double out[6]);
 int lesgpu_monitor_noalloc(const double* rho, const double* T, const double* G, const double* Y0, size_t n,
                            double dx, double dy, double dz, double* out, void* stream);
 
+/* Profile statistics of the probe rows on the device -- no counterpart as an API: the
+ * reference appends every probe row to a CSV file each step (record_flame_region_data,
+ * :3403-3471) and its post-processing reads them back (analysis.py:82-154, :215-257,
+ * bayesian_optimizer.py:71-117).  Here the rows stay on the device: after each device-loop
+ * chunk, lesgpu_pstat_accumulate bins the rows of the first n_lines history lines (the probe
+ * stations; y_flame from the lower G = 0.5 crossing, rows with |y_rel| <= 1 m) and adds their
+ * moments to running FP64 sums, deterministically.  Bins (each array holds n + 1 increasing
+ * edges): flame distance y_rel in mm, right-closed (e_b, e_b+1]; G right-closed (the
+ * conditional stresses); G half-open [e_b, e_b+1) (the optimiser's <u'v'>); u and v
+ * histograms [e_b, e_b+1), last bin closed, for G < 0.5 and G >= 0.5.
+ * lesgpu_pstat_read writes lesgpu_pstat_size() doubles:
+ *   N, sum u, sum v, sum w;
+ *   per y bin: n, sum u, v, w, G, uu, vv, ww, uv;
+ *   per right-closed G bin: n, sum u, v, w, uu, vv, uv;
+ *   per half-open G bin: n, sum u, v, uv;
+ *   counts: u unburnt [n_pdf], v unburnt [n_pdf], u burnt [n_pdf], v burnt [n_pdf]. */
+int lesgpu_pstat_begin(lesgpu_ctx* ctx, const double* y_edges_mm, int n_y, const double* g_rc_edges, int n_grc,
+                       const double* g_ho_edges, int n_gho, const double* u_edges, const double* v_edges, int n_pdf);
+int lesgpu_pstat_accumulate(lesgpu_ctx* ctx, int nsteps, int n_lines);
+size_t lesgpu_pstat_size(const lesgpu_ctx* ctx);
+int lesgpu_pstat_read(lesgpu_ctx* ctx, double* out);
+int lesgpu_pstat_end(lesgpu_ctx* ctx);
+
 /* check_for_nan (:1289-1305) without exit(): returns LESGPU_ENONFINITE if any u is not finite. */
 int lesgpu_check_finite(lesgpu_ctx* ctx, int field_id);
 

@@ -127,6 +127,20 @@ int les_solver_load_checkpoint(les_solver* s, const char* path, int* t_out);
 int les_solver_finish(les_solver* s, const char* dir, int mode);
 int les_solver_resume(les_solver* s, const char* dir, int mode, int* t_out);
 
+/* Profile statistics of the probe rows, accumulated on the device during device-loop runs
+ * (lesgpu_pstat_* in les_gpu.h): after les_solver_pstat_begin every chunk of
+ * les_solver_run_device / les_solver_loop_run / les_ensemble_run adds its rows, with or
+ * without probe files; les_solver_pstat_read returns the sums in lesgpu_pstat_read's layout.
+ * NULL edge arrays select the defaults: 0.5 mm flame-distance bins over [-LY, LY] (in mm),
+ * the post-processing's G bins (0, 0.05] .. (0.95, 1.0] and the optimiser's [0, 0.05) ..
+ * [0.95, 1.0), and 40-bin histograms of u over [-U, 3U] and v over [-2U, 2U] for the inlet
+ * velocity U; n_* are then ignored. */
+int les_solver_pstat_begin(les_solver* s, const double* y_edges_mm, int n_y, const double* g_rc_edges, int n_grc,
+                           const double* g_ho_edges, int n_gho, const double* u_edges, const double* v_edges,
+                           int n_pdf);
+size_t les_solver_pstat_size(const les_solver* s);
+int les_solver_pstat_read(les_solver* s, double* out);
+
 /* Time averages (update_time_averages, :3166-3191) summed on the device from the step whose
  * t_loop reaches start_step (the reference's start_avg_step); start_step < 0 turns them off.
  * save/load: stats_backup.bin (:3736-3778); reynolds_stresses: the seven fields of

@@ -168,6 +168,15 @@ int lesgpu_loop_end(lesgpu_ctx* c, unsigned int win[31], double* vort, int* t_lo
     return LESGPU_EINVAL;
 }
 
+int lesgpu_pstat_begin(lesgpu_ctx* c, const double* ye, int ny, const double* grc, int ngrc, const double* gho, int ngho,
+                       const double* ue, const double* ve, int npdf) {
+    (void)c; (void)ye; (void)ny; (void)grc; (void)ngrc; (void)gho; (void)ngho; (void)ue; (void)ve; (void)npdf;
+    return LESGPU_EINVAL;
+}
+int lesgpu_pstat_accumulate(lesgpu_ctx* c, int nsteps, int n_lines) { (void)c; (void)nsteps; (void)n_lines; return LESGPU_EINVAL; }
+size_t lesgpu_pstat_size(const lesgpu_ctx* c) { (void)c; return 0; }
+int lesgpu_pstat_read(lesgpu_ctx* c, double* out) { (void)c; (void)out; return LESGPU_EINVAL; }
+
 /* for the test: the attribute map the "device" holds and how often it was uploaded */
 int fake_attr(const lesgpu_ctx* c, int* out) {
     memcpy(out, c->attr, c->n * sizeof(int));
