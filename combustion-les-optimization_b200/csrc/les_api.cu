@@ -1172,6 +1172,24 @@ int lesgpu_pstat_accumulate(lesgpu_ctx* ctx, int nsteps, int n_lines) {
 
 size_t lesgpu_pstat_size(const lesgpu_ctx* ctx) { return (ctx && ctx->d.ps_on) ? ctx->d.ps_nsums : 0; }
 
+int lesgpu_pstat_layout(const lesgpu_ctx* ctx, int* n_y, int* n_grc, int* n_gho, int* n_pdf, double* edges,
+                        size_t* n_edges) {
+    if (!ctx) return LESGPU_EINVAL;
+    const DevCtx& d = ctx->d;
+    if (!d.ps_on) return LESGPU_ESTATE;
+    if (n_y) *n_y = d.ps_ny;
+    if (n_grc) *n_grc = d.ps_ngrc;
+    if (n_gho) *n_gho = d.ps_ngho;
+    if (n_pdf) *n_pdf = d.ps_npdf;
+    const size_t ne = (size_t)d.ps_ny + d.ps_ngrc + d.ps_ngho + 2 * (size_t)d.ps_npdf + 5;
+    if (n_edges) *n_edges = ne;
+    if (edges) {
+        cudaError_t e = cudaMemcpy(edges, d.ps_edges, ne * sizeof(double), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return LESGPU_ECUDA;
+    }
+    return LESGPU_OK;
+}
+
 int lesgpu_pstat_read(lesgpu_ctx* ctx, double* out) {
     if (!ctx || !out) return LESGPU_EINVAL;
     DevCtx& d = ctx->d;

@@ -11,6 +11,7 @@
 
 #include <errno.h>
 #include <math.h>
+#include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -378,6 +379,10 @@ int les_solver_set_outputs(les_solver* s, const char* dir, int flags) {
     if ((flags & LES_OUT_VTK) != (s->out_flags & LES_OUT_VTK)) {
         int rc = lesgpu_keep_grad_g(s->ctx, (flags & LES_OUT_VTK) ? 1 : 0);
         if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
+    }
+    if ((flags & LES_OUT_PSTAT) && !s->ps_on) {
+        int rc = les_solver_pstat_begin(s, NULL, 0, NULL, 0, NULL, 0, NULL, NULL, 0);
+        if (rc) return rc;
     }
     s->out_flags = flags;
     if (!dir) return LESGPU_OK;
@@ -820,6 +825,27 @@ int les_solver_pstat_begin(les_solver* s, const double* y_edges_mm, int n_y, con
 
 size_t les_solver_pstat_size(const les_solver* s) { return (s && s->ps_on) ? lesgpu_pstat_size(s->ctx) : 0; }
 
+int les_solver_pstat_write(les_solver* s, const char* path) {
+    if (!s || !path) return LESGPU_EINVAL;
+    if (!s->ps_on) return serr(s, LESGPU_ESTATE, "les_solver_pstat_begin first");
+    int32_t hdr[5] = {0x53505350, 0, 0, 0, 0};
+    size_t ne = 0;
+    int rc = lesgpu_pstat_layout(s->ctx, &hdr[1], &hdr[2], &hdr[3], &hdr[4], NULL, &ne);
+    if (rc) return serr(s, rc, lesgpu_last_error(s->ctx));
+    const size_t ns = lesgpu_pstat_size(s->ctx);
+    double* buf = (double*)malloc((ne + ns) * sizeof(double));
+    if (!buf) return serr(s, LESGPU_ENOMEM, "host buffers");
+    rc = lesgpu_pstat_layout(s->ctx, NULL, NULL, NULL, NULL, buf, &ne);
+    if (rc == LESGPU_OK) rc = lesgpu_pstat_read(s->ctx, buf + ne);
+    if (rc) { free(buf); return serr(s, rc, lesgpu_last_error(s->ctx)); }
+    FILE* fp = fopen(path, "wb");
+    if (!fp) { free(buf); return serr(s, LESGPU_EIO, "cannot open profile_stats.bin for writing"); }
+    const int ok = fwrite(hdr, sizeof hdr, 1, fp) == 1 && fwrite(buf, sizeof(double), ne + ns, fp) == ne + ns;
+    fclose(fp);
+    free(buf);
+    return ok ? LESGPU_OK : serr(s, LESGPU_EIO, "short profile_stats.bin write");
+}
+
 int les_solver_pstat_read(les_solver* s, double* out) {
     if (!s || !out) return LESGPU_EINVAL;
     if (!s->ps_on) return serr(s, LESGPU_ESTATE, "les_solver_pstat_begin first");
@@ -1054,6 +1080,11 @@ int les_solver_flush(les_solver* s) {
     if (s->loop_on) return serr(s, LESGPU_ESTATE, "end the device loop first");
     int rc = write_vtk_step(s, s->t_loop);
     flush_points(s);
+    if (rc == LESGPU_OK && s->ps_on && (s->out_flags & LES_OUT_PSTAT) && s->out_dir[0]) {
+        char path[1200];
+        join_path(path, sizeof(path), s->out_dir, "profile_stats.bin");
+        rc = les_solver_pstat_write(s, path);
+    }
     return rc;
 }
 

@@ -206,10 +206,12 @@ static int job_prepare(les_serve* s, serve_req* q) {
     return LESGPU_OK;
 }
 
-/* End of a finished request: close the loop session (files flushed), copy the final state
-   to the host when results are kept, release the solver and its device memory. */
+/* End of a finished request: close the loop session (files flushed, les_solver_flush), copy
+   the final state to the host when results are kept, release the solver and its device memory. */
 static int job_finish(les_serve* s, serve_req* q) {
     int rc = les_solver_loop_end(q->sol);
+    /* the end-of-run writes (final VTK, point rows, profile_stats.bin) of the enabled outputs */
+    if (rc == LESGPU_OK && q->out_dir[0]) rc = les_solver_flush(q->sol);
     if (rc == LESGPU_OK && s->opt.keep_results) {
         const size_t n = (size_t)q->cfg.nx * q->cfg.ny * q->cfg.nz;
         q->result = (double*)malloc(LESGPU_NSTATE * n * sizeof(double));

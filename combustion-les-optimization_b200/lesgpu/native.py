@@ -33,6 +33,7 @@ ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "EIO", -5: "ESTATE", -6: 
 LESGPU_EINVAL, LESGPU_ECUDA, LESGPU_ENOMEM, LESGPU_EIO, LESGPU_ESTATE, LESGPU_ENONFINITE = -1, -2, -3, -4, -5, -6
 
 LES_OUT_PROBES, LES_OUT_MONITOR, LES_OUT_CHECKPOINT, LES_OUT_POINTS, LES_OUT_VTK = 1, 2, 4, 8, 16
+LES_OUT_PSTAT = 32          # probe-row statistics on the device -> profile_stats.bin
 AVG_NAMES = ["u", "v", "w", "uu", "vv", "ww", "uv", "uw", "vw", "G"]
 STRESS_NAMES = ["uu", "vv", "ww", "uv", "uw", "vw", "G_mean"]
 

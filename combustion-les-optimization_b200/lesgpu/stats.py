@@ -296,3 +296,22 @@ def probe_rows(lines: np.ndarray, t0: int, dy: float, x_locations: np.ndarray) -
             for c, idx in (("u", 0), ("v", 1), ("w", 2), ("G", 3), ("nu_t", 4), ("S_mag", 5)):
                 cols[c].append(lines[q, n, keep, idx])
     return {c: (np.concatenate(v) if v else np.zeros(0)) for c, v in cols.items()}
+
+
+def read_moments_file(path: str):
+    """profile_stats.bin (les_solver_pstat_write): the edges and the moment sums."""
+    with open(path, "rb") as f:
+        raw = f.read()
+    hdr = np.frombuffer(raw[:20], dtype=np.int32)
+    if int(hdr[0]) != 0x53505350:
+        raise ValueError(f"{path}: not a profile_stats file")
+    ny, nrc, nho, npdf = (int(x) for x in hdr[1:])
+    vals = np.frombuffer(raw[20:], dtype=np.float64)
+    edges, o = {}, 0
+    for k, n in (("y_mm", ny), ("g_rc", nrc), ("g_ho", nho), ("u", npdf), ("v", npdf)):
+        edges[k] = vals[o:o + n + 1].copy()
+        o += n + 1
+    sums = vals[o:].copy()
+    if len(sums) != moments_size(edges):
+        raise ValueError(f"{path}: truncated")
+    return edges, sums

@@ -217,6 +217,10 @@ int lesgpu_pstat_begin(lesgpu_ctx* ctx, const double* y_edges_mm, int n_y, const
                        const double* g_ho_edges, int n_gho, const double* u_edges, const double* v_edges, int n_pdf);
 int lesgpu_pstat_accumulate(lesgpu_ctx* ctx, int nsteps, int n_lines);
 size_t lesgpu_pstat_size(const lesgpu_ctx* ctx);
+/* The bin counts and, when `edges` is not NULL, the edges in the order of lesgpu_pstat_begin's
+ * arguments (y, G right-closed, G half-open, u, v); *n_edges receives their total count. */
+int lesgpu_pstat_layout(const lesgpu_ctx* ctx, int* n_y, int* n_grc, int* n_gho, int* n_pdf, double* edges,
+                        size_t* n_edges);
 int lesgpu_pstat_read(lesgpu_ctx* ctx, double* out);
 int lesgpu_pstat_end(lesgpu_ctx* ctx);
 

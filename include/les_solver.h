@@ -53,6 +53,10 @@ typedef struct les_solver les_solver;
                                   by les_solver_flush and when the solver is destroyed */
 #define LES_OUT_VTK 16         /* Premixed_C3H8_Air_%04d.vtk every 500 steps (:4594-4598) and at
                                   les_solver_flush (:4611) */
+#define LES_OUT_PSTAT 32       /* no reference counterpart: the probe-row statistics accumulated on
+                                  the device during device-loop runs (les_solver_pstat_*, default
+                                  bins) instead of probe files, written as profile_stats.bin by
+                                  les_solver_flush and at the end of a served request */
 
 /* Load the species files, create the GPU context, build the attribute map and the initial
  * state exactly as initialize()+setting() (:1085-1285), seed rand() and place the SEM
@@ -140,6 +144,9 @@ int les_solver_pstat_begin(les_solver* s, const double* y_edges_mm, int n_y, con
                            int n_pdf);
 size_t les_solver_pstat_size(const les_solver* s);
 int les_solver_pstat_read(les_solver* s, double* out);
+/* profile_stats.bin: int32 magic 0x53505350, int32 n_y, n_grc, n_gho, n_pdf, then the edges
+ * (y mm, G right-closed, G half-open, u, v; n + 1 doubles each) and the sums. */
+int les_solver_pstat_write(les_solver* s, const char* path);
 
 /* Time averages (update_time_averages, :3166-3191) summed on the device from the step whose
  * t_loop reaches start_step (the reference's start_avg_step); start_step < 0 turns them off.

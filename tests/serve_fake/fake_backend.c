@@ -111,6 +111,8 @@ int les_solver_loop_begin(les_solver* s, int chunk) {
     return LESGPU_OK;
 }
 
+int les_solver_flush(les_solver* s) { (void)s; return LESGPU_OK; }
+
 int les_solver_loop_end(les_solver* s) {
     if (!s || !s->loop_on || s->inflight) return LESGPU_ESTATE;
     s->loop_on = 0;

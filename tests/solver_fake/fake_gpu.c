@@ -175,6 +175,10 @@ int lesgpu_pstat_begin(lesgpu_ctx* c, const double* ye, int ny, const double* gr
 }
 int lesgpu_pstat_accumulate(lesgpu_ctx* c, int nsteps, int n_lines) { (void)c; (void)nsteps; (void)n_lines; return LESGPU_EINVAL; }
 size_t lesgpu_pstat_size(const lesgpu_ctx* c) { (void)c; return 0; }
+int lesgpu_pstat_layout(const lesgpu_ctx* c, int* a, int* b, int* d, int* e, double* edges, size_t* ne) {
+    (void)c; (void)a; (void)b; (void)d; (void)e; (void)edges; (void)ne;
+    return LESGPU_EINVAL;
+}
 int lesgpu_pstat_read(lesgpu_ctx* c, double* out) { (void)c; (void)out; return LESGPU_EINVAL; }
 
 /* for the test: the attribute map the "device" holds and how often it was uploaded */

@@ -112,3 +112,31 @@ def test_poisson_replay_small(N, S):
     assert st["done"] == 12 and st["failed"] == 0
     assert st["latency_p99_s"] >= st["latency_p50_s"] > 0
     srv.close()
+
+
+def test_served_request_statistics_without_probe_files(N, S, tmp_path):
+    """A request with LES_OUT_PSTAT alone: no probe files, and profile_stats.bin at the end
+    holds the device-accumulated statistics of its rows -- the same as les_solver's own
+    device statistics of the same run (summed in other chunks: counts exact, sums 1e-12)."""
+    from lesgpu import stats
+    from lesgpu.config import preset
+    cfg = preset("c1", seed=31)
+    srv = S.Server(quantum=9, prep_threads=2)
+    rid = srv.submit(cfg, 60, N.FP64, out_dir=str(tmp_path), out_flags=N.LES_OUT_PSTAT)
+    srv.submit(preset("tiny", seed=3), 25, N.FP64)
+    srv.drain()
+    assert srv.info(rid)["state_name"] == "done"
+    srv.close()
+    assert not list(tmp_path.glob("probe_data_*"))
+    edges, sums = stats.read_moments_file(str(tmp_path / "profile_stats.bin"))
+    solo = N.Solver(cfg)
+    e2 = solo.pstat_begin()
+    solo.run_device(60, chunk=64)
+    ref = solo.pstat_read()
+    solo.close()
+    for k in e2:
+        np.testing.assert_array_equal(edges[k], e2[k])
+    got, want = stats.from_moments(sums, edges), stats.from_moments(ref, e2)
+    assert sums[0] == ref[0] > 1000
+    np.testing.assert_allclose(sums, ref, rtol=1e-12, atol=1e-9)
+    np.testing.assert_allclose(got["flame_profile"]["re_uv"], want["flame_profile"]["re_uv"], rtol=1e-9, atol=1e-14)
