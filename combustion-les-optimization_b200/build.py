@@ -94,8 +94,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
         obj = os.path.join(bdir, name + ".o")
         flags = [nvcc, "-c", src, "-o", obj, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                  "-I", INC, "-I", os.path.join(HERE, "csrc")] + ARCH + [f"-D{d}" for d in defines]
-        fmad_off = FMAD_OFF - ({"les_f64"} if "LES_F64_CONTRACT" in defines else set())
-        flags += ["-fmad=false"] if name in fmad_off else ["-fmad=true"]
+        flags += ["-fmad=false"] if name in FMAD_OFF else ["-fmad=true"]
         if ptxas_verbose:
             flags += ["-Xptxas", "-v"]
         r = _run(flags, verbose)

@@ -175,13 +175,9 @@ __device__ __forceinline__ size_t cid(int i, int j, int k, int ny, int nz) {
 }
 
 __device__ __forceinline__ double cdv(double x, const DC& d) {
-#ifdef LES_F64_FAST_DIV
-    return x * d.r;
-#else
     double q = x * d.r;
     double e = fma(-q, d.c, x);
     return fma(e, d.r, q);
-#endif
 }
 __device__ __forceinline__ float cdv(float x, const DCT<float>& d) { return x * d.r; }
 
@@ -218,9 +214,6 @@ __device__ __forceinline__ double qsqrt(double x) { return sqrt(x); }
 // pairs (lesgpu_selfcheck_division).  A denominator that is zero, subnormal or not finite
 // takes the IEEE division.
 __device__ __forceinline__ double mdiv(double a, double b, double y) {
-#ifdef LES_F64_FAST_DIV
-    return a * y;
-#endif
     const double ab = fabs(b);
     if (!(ab >= 2.2250738585072014e-308 && ab <= 1.7976931348623157e308)) return a / b;
     const double q = a * y;
@@ -248,9 +241,6 @@ __device__ __forceinline__ double sdiv<float>(double a, double b) {
 // arguments, while a plain product rounds twice.  The exact square is split with fma,
 // the rest is carried as a double-double and rounded once at the end.
 __device__ __forceinline__ double pow3_rn(double x) {
-#ifdef LES_F64_FAST_POW
-    return (x * x) * x;
-#endif
     double p = x * x;
     double e = fma(x, x, -p);
     double h = p * x;
@@ -259,10 +249,6 @@ __device__ __forceinline__ double pow3_rn(double x) {
     return h + l;
 }
 __device__ __forceinline__ double pow4_rn(double x) {
-#ifdef LES_F64_FAST_POW
-    const double p2 = x * x;
-    return p2 * p2;
-#endif
     double p = x * x;
     double e = fma(x, x, -p);
     double h = p * p;
