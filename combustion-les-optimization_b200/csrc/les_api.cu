@@ -12,6 +12,7 @@
 #include <string.h>
 
 #include <string>
+#include <cstring>
 #include <vector>
 
 #include "les_ctx.h"
@@ -1276,7 +1277,58 @@ struct lesgpu_group {
     cudaEvent_t fork = nullptr, done = nullptr;
     std::vector<cudaEvent_t> joins, ready;
     cudaGraphExec_t exec = nullptr;
+    // batched form: members in batches of one shape, each batch's RK stages on its own stream
+    std::vector<std::vector<int>> batches;
+    std::vector<cudaStream_t> bstreams;
+    std::vector<cudaEvent_t> heads, stages;
+    std::vector<les::MemberTab*> tabs;     // device member tables, one per batch
 };
+
+namespace {
+
+// Members batch together when their constants agree except the model constants an ensemble
+// varies (read per member from the member table), and their tiles and arena layout agree.
+les::Consts masked_consts(const les::Consts& c) {
+    les::Consts m;
+    std::memcpy(&m, &c, sizeof(m));
+    m.cs_u = m.cs_b = m.cs_boost = m.accel_strength = m.accel_center = m.two_w2 = m.relax = 0.0;
+    m.d_w2 = les::DC{0.0, 0.0};
+    m.f.cs_u = m.f.cs_b = m.f.cs_boost = m.f.accel_strength = m.f.accel_center = m.f.relax = 0.0f;
+    m.f.d_w2 = les::DCT<float>{0.0f, 0.0f};
+    return m;
+}
+
+bool batchable(const DevCtx& a, const DevCtx& b) {
+    if (a.nx != b.nx || a.ny != b.ny || a.nz != b.nz || a.precision != b.precision) return false;
+    for (int q = 0; q < les::NSH_CLASSES; q++)
+        if (a.shape[q] != b.shape[q]) return false;
+    // per-cell fields at the same offsets within the two arenas
+    auto off = [](const DevCtx& d, const void* p) { return (const char*)p - (const char*)d.arena; };
+    for (int q = 0; q < les::NSTATE; q++)
+        if (off(a, a.S[q]) != off(b, b.S[q]) || off(a, a.St[q]) != off(b, b.St[q]) || off(a, a.F[q]) != off(b, b.F[q]))
+            return false;
+    for (int q = 0; q < les::NACC; q++)
+        if (off(a, a.acc[q]) != off(b, b.acc[q])) return false;
+    for (int q = 0; q < 4; q++)
+        if (off(a, a.kflow[q]) != off(b, b.kflow[q])) return false;
+    if (off(a, a.mu_mix) != off(b, b.mu_mix) || off(a, a.nu_t) != off(b, b.nu_t) || off(a, a.mu_eff) != off(b, b.mu_eff))
+        return false;
+    const les::Consts ca = masked_consts(a.hC), cb = masked_consts(b.hC);
+    return std::memcmp(&ca, &cb, sizeof(ca)) == 0;
+}
+
+les::MemberTab member_entry(const DevCtx& d0, const DevCtx& d) {
+    les::MemberTab e{};
+    e.delta = (long long)((const char*)d.arena - (const char*)d0.arena);
+    e.attr = d.attr;
+    e.S = d.dS;
+    e.part = d.part;
+    e.md = les::model_of<double>(d.hC);
+    e.mf = les::model_of<float>(d.hC);
+    return e;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -1284,6 +1336,10 @@ void lesgpu_group_destroy(lesgpu_group* g) {
     if (!g) return;
     if (g->root) cudaStreamSynchronize(g->root);
     if (g->exec) cudaGraphExecDestroy(g->exec);
+    for (les::MemberTab* t : g->tabs) if (t) cudaFree(t);
+    for (cudaEvent_t e : g->heads) if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : g->stages) if (e) cudaEventDestroy(e);
+    for (cudaStream_t st : g->bstreams) if (st) cudaStreamDestroy(st);
     for (cudaEvent_t e : g->joins) if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : g->ready) if (e) cudaEventDestroy(e);
     if (g->fork) cudaEventDestroy(g->fork);
@@ -1353,6 +1409,113 @@ int lesgpu_group_create(lesgpu_ctx* const* ctxs, int n, lesgpu_group** out) {
     *out = g;
     return LESGPU_OK;
 }
+
+int lesgpu_group_create_batched(lesgpu_ctx* const* ctxs, int n, lesgpu_group** out) {
+    if (!ctxs || n < 1 || !out) return LESGPU_EINVAL;
+    *out = nullptr;
+    for (int q = 0; q < n; q++) {
+        if (!ctxs[q]) return LESGPU_EINVAL;
+        const DevCtx& d = ctxs[q]->d;
+        if (!d.loop_ready) return fail(ctxs[q], LESGPU_ESTATE, "group members need lesgpu_loop_begin first");
+        if (d.timing) return fail(ctxs[q], LESGPU_ESTATE, "group members must have kernel timing off");
+        if (d.debug || d.grad_g || d.scalar_tma)
+            return fail(ctxs[q], LESGPU_ESTATE, "batched members need inspection, |grad G| and the staged pass off");
+        if (ctxs[q]->cfg.device != ctxs[0]->cfg.device)
+            return fail(ctxs[q], LESGPU_EINVAL, "group members must share one device");
+        for (int r = 0; r < q; r++)
+            if (ctxs[r] == ctxs[q]) return fail(ctxs[q], LESGPU_EINVAL, "context listed twice in a group");
+    }
+    lesgpu_group* g = new (std::nothrow) lesgpu_group();
+    if (!g) return LESGPU_ENOMEM;
+    g->m.assign(ctxs, ctxs + n);
+    g->device = ctxs[0]->cfg.device;
+    lesgpu_ctx* c0 = ctxs[0];
+    // batches: each member joins the first batch whose first member it matches
+    for (int q = 0; q < n; q++) {
+        size_t b = 0;
+        while (b < g->batches.size() && !batchable(ctxs[g->batches[b][0]]->d, ctxs[q]->d)) b++;
+        if (b == g->batches.size()) g->batches.emplace_back();
+        g->batches[b].push_back(q);
+    }
+    const size_t nb = g->batches.size();
+    cudaError_t e = cudaSetDevice(g->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&g->root, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->done, cudaEventDisableTiming);
+    g->joins.assign(n, nullptr);
+    g->ready.assign(n, nullptr);
+    g->heads.assign(n, nullptr);
+    g->bstreams.assign(nb, nullptr);
+    g->stages.assign(nb, nullptr);
+    g->tabs.assign(nb, nullptr);
+    for (int q = 0; q < n && e == cudaSuccess; q++) {
+        e = cudaEventCreateWithFlags(&g->joins[q], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->ready[q], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->heads[q], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctxs[q]->d.stream);
+    }
+    for (size_t b = 0; b < nb && e == cudaSuccess; b++) {
+        e = cudaStreamCreateWithFlags(&g->bstreams[b], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->stages[b], cudaEventDisableTiming);
+        std::vector<les::MemberTab> tab;
+        const DevCtx& d0 = ctxs[g->batches[b][0]]->d;
+        for (int q : g->batches[b]) tab.push_back(member_entry(d0, ctxs[q]->d));
+        if (e == cudaSuccess) e = cudaMalloc(&g->tabs[b], tab.size() * sizeof(les::MemberTab));
+        if (e == cudaSuccess)
+            e = cudaMemcpy(g->tabs[b], tab.data(), tab.size() * sizeof(les::MemberTab), cudaMemcpyHostToDevice);
+    }
+    if (e != cudaSuccess) { int r = cuda_fail(c0, e, "group_create_batched"); lesgpu_group_destroy(g); return r; }
+    // capture one step: every member's dt and draws (then its SEM plane) on its stream; each
+    // batch's RK stages on the batch stream once its members' dt is set; every member's
+    // boundary conditions and history on its stream once its batch is done
+    cudaGraph_t gr = nullptr;
+    e = cudaStreamBeginCapture(g->root, cudaStreamCaptureModeThreadLocal);
+    cudaError_t el = cudaSuccess;
+    if (e == cudaSuccess) {
+        el = cudaEventRecord(g->fork, g->root);
+        for (int q = 0; q < n && el == cudaSuccess; q++) {
+            DevCtx& d = ctxs[q]->d;
+            el = cudaStreamWaitEvent(d.stream, g->fork, 0);
+            if (el == cudaSuccess) el = les::loop_pre(d);
+            if (el == cudaSuccess) el = cudaEventRecord(g->heads[q], d.stream);
+            if (el == cudaSuccess) el = les::sem_inflow(d, d.stream);
+        }
+        for (size_t b = 0; b < nb && el == cudaSuccess; b++) {
+            for (int q : g->batches[b])
+                if (el == cudaSuccess) el = cudaStreamWaitEvent(g->bstreams[b], g->heads[q], 0);
+            DevCtx& d0 = ctxs[g->batches[b][0]]->d;
+            const int nm = (int)g->batches[b].size();
+            if (el == cudaSuccess)
+                el = (d0.precision == LESGPU_FP64) ? les::batch_stages_f64(d0, g->tabs[b], nm, g->bstreams[b])
+                                                   : les::batch_stages_f32(d0, g->tabs[b], nm, g->bstreams[b]);
+            if (el == cudaSuccess) el = cudaEventRecord(g->stages[b], g->bstreams[b]);
+            for (int q : g->batches[b]) {
+                DevCtx& d = ctxs[q]->d;
+                if (el == cudaSuccess) el = cudaStreamWaitEvent(d.stream, g->stages[b], 0);
+                if (el == cudaSuccess)
+                    el = (d.precision == LESGPU_FP64) ? les::batch_tail_f64(d) : les::batch_tail_f32(d);
+                if (el == cudaSuccess) el = cudaEventRecord(g->joins[q], d.stream);
+                if (el == cudaSuccess) el = cudaStreamWaitEvent(g->root, g->joins[q], 0);
+            }
+        }
+        cudaError_t ee = cudaStreamEndCapture(g->root, &gr);
+        if (el == cudaSuccess) el = ee;
+    } else {
+        el = e;
+    }
+    if (el == cudaSuccess) el = cudaGraphInstantiate(&g->exec, gr, 0);
+    if (gr) cudaGraphDestroy(gr);
+    if (el != cudaSuccess) {
+        cudaGetLastError();
+        int r = cuda_fail(c0, el, "batched group capture");
+        lesgpu_group_destroy(g);
+        return r;
+    }
+    *out = g;
+    return LESGPU_OK;
+}
+
+int lesgpu_group_batches(const lesgpu_group* g) { return g ? (int)(g->batches.empty() ? g->m.size() : g->batches.size()) : 0; }
 
 int lesgpu_group_run(lesgpu_group* g, int nsteps) {
     if (!g || nsteps < 0) return LESGPU_EINVAL;

@@ -41,6 +41,14 @@ struct DCT {
 };
 using DC = DCT<double>;
 
+// Model constants that vary between the members of an ensemble (the constants a Bayesian
+// optimiser proposes: les_combustion_solver.c:257-262, :2834).
+template <typename R>
+struct ModelK {
+    R cs_u, cs_b, cs_boost, accel_strength, accel_center, relax;
+    DCT<R> d_w2;
+};
+
 // Constants that enter the per-cell arithmetic.  The FP32 form reads float copies of them
 // (ConstsF, filled on the host), so no double-to-float conversion runs per cell; the FP64
 // form reads the double originals.  X(name, dims) for values, XD(name, dims) for divisors.
@@ -126,6 +134,17 @@ __host__ __device__ __forceinline__ const typename KSel<R>::type& kc(const Const
     return KSel<R>::get(C);
 }
 
+// The model constants of the cell's member: the launch's own constants, or the member table's.
+template <typename R>
+__host__ __device__ __forceinline__ ModelK<R> model_of(const Consts& C) {
+    const auto& K = kc<R>(C);
+    ModelK<R> m;
+    m.cs_u = K.cs_u; m.cs_b = K.cs_b; m.cs_boost = K.cs_boost; m.accel_strength = K.accel_strength;
+    m.accel_center = K.accel_center; m.relax = K.relax; m.d_w2 = K.d_w2;
+    return m;
+}
+
+
 // Host: fill C.f from the double values.
 inline void to_float(float& d, double s) { d = (float)s; }
 inline void to_float(DCT<float>& d, const DC& s) { d.c = (float)s.c; d.r = (float)s.r; }
@@ -137,6 +156,36 @@ inline void fill_float_consts(Consts& C) {
 #define LES_CONV(name, dims) to_float(C.f.name, C.name);
     LES_FCONSTS(LES_CONV, LES_CONV)
 #undef LES_CONV
+}
+
+// A batched launch (les_launch.cuh, batch_stages) steps several members of one grid shape in
+// one launch; each block finds its member's buffers and model constants here.
+struct Scalars;
+struct MemberTab {
+    long long delta;            // byte offset of this member's field arena from the first member's
+    const uint8_t* attr;        // attribute map
+    Scalars* S;                 // reduction results, dt, step counters
+    double* part;               // per-block partials
+    ModelK<double> md;          // model constants, FP64 form
+    ModelK<float> mf;           // and FP32 form
+};
+// Kernel argument of the batched stage kernels: the member table and the z-extent of one
+// member's grid of blocks (blockIdx.z = member * gz + block z within the member).
+struct Batch {
+    const MemberTab* mt;
+    int gz;
+};
+
+template <typename R>
+__device__ __forceinline__ const ModelK<R>& member_model(const MemberTab& e);
+template <>
+__device__ __forceinline__ const ModelK<double>& member_model<double>(const MemberTab& e) { return e.md; }
+template <>
+__device__ __forceinline__ const ModelK<float>& member_model<float>(const MemberTab& e) { return e.mf; }
+
+template <typename T>
+__device__ __forceinline__ T* shifted(T* p, long long d) {
+    return (T*)((char*)p + d);
 }
 
 // Reduction results written by the kernels' last-block epilogues.

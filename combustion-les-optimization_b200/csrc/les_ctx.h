@@ -158,6 +158,14 @@ cudaError_t probe_f64(DevCtx& c, int n, int kline);
 cudaError_t check_f64(DevCtx& c, int field);
 cudaError_t rhs_only_f64(DevCtx& c, int t_loop);
 cudaError_t step_f32(DevCtx& c, double dt, int t_loop, bool device_mode);
+// Batched members (les_launch.cuh): step head and tail of one member, the RK stages of nmem
+// members of one shape in one launch per pass.
+cudaError_t batch_head_f64(DevCtx& c);
+cudaError_t batch_tail_f64(DevCtx& c);
+cudaError_t batch_stages_f64(DevCtx& c0, const MemberTab* mt, int nmem, cudaStream_t st);
+cudaError_t batch_head_f32(DevCtx& c);
+cudaError_t batch_tail_f32(DevCtx& c);
+cudaError_t batch_stages_f32(DevCtx& c0, const MemberTab* mt, int nmem, cudaStream_t st);
 cudaError_t rhs_only_f32(DevCtx& c, int t_loop);
 cudaError_t umax_f32(DevCtx& c);
 cudaError_t monitor_f32(DevCtx& c);

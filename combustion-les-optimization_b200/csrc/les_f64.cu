@@ -13,6 +13,11 @@ cudaError_t step_f64(DevCtx& c, double dt, int t_loop, bool device_mode) {
     return step_impl<double>(c, dt, t_loop, device_mode);
 }
 cudaError_t rhs_only_f64(DevCtx& c, int t_loop) { return rhs_only_impl<double>(c, t_loop); }
+cudaError_t batch_head_f64(DevCtx& c) { return batch_head<double>(c); }
+cudaError_t batch_tail_f64(DevCtx& c) { return batch_tail<double>(c); }
+cudaError_t batch_stages_f64(DevCtx& c0, const MemberTab* mt, int nmem, cudaStream_t st) {
+    return batch_stages<double>(c0, mt, nmem, st);
+}
 cudaError_t umax_f64(DevCtx& c) { return umax_impl<double>(c); }
 cudaError_t monitor_f64(DevCtx& c) { return monitor_impl<double>(c); }
 cudaError_t probe_f64(DevCtx& c, int n, int kline) { return probe_impl<double>(c, n, kline); }

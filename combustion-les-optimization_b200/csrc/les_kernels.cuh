@@ -61,6 +61,30 @@ struct KFlow {               // momentum and G right-hand sides handed from C1 t
 
 #define LES_KERNEL_CONSTS const __grid_constant__ Consts C
 
+// A member's fields in a batched launch: every per-cell field lives in the member's arena at
+// the same offset as in the first member's, so its pointers are the first member's shifted by
+// the arenas' distance.  Optional buffers outside the arena (inspection, |grad G|) are off in
+// batched launches.
+template <typename T>
+__device__ __forceinline__ void shift_all(T& s, long long d) {
+#pragma unroll
+    for (int q = 0; q < (int)(sizeof(s.p) / sizeof(s.p[0])); q++) s.p[q] = shifted(s.p[q], d);
+}
+template <typename R>
+__device__ __forceinline__ void shift_props(PropBuf<R>& P, long long d) {
+    P.mu_mix = shifted(P.mu_mix, d);
+    P.nu = shifted(P.nu, d);
+#pragma unroll
+    for (int s = 0; s < NSP; s++) P.D[s] = shifted(P.D[s], d);
+    P.aT = shifted(P.aT, d);
+    P.nu_t = shifted(P.nu_t, d);
+    P.S_mag = shifted(P.S_mag, d);
+    P.ST = shifted(P.ST, d);
+    P.mu_eff = shifted(P.mu_eff, d);
+    P.dbg_cp = P.dbg_lam = P.dbg_alpha = nullptr;
+    P.grad_g = nullptr;
+}
+
 // Minimum resident blocks per SM requested from the register allocator (filter / flow /
 // scalar).  These kernels are latency-bound; swept on B200 at 256x128x128: FP64 5/4/4 (the
 // scalar pass at 3 blocks 3.41 ms, at 4 3.17 ms; the filter at 4 3.14 ms, at 5 3.02 ms; the
@@ -333,17 +357,29 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
 
 // ------------------------------------------------------------------ pass A: filter + props
 
-template <typename R, typename RI = R>
+template <typename R, typename RI = R, bool BATCH = false>
 __global__ void __launch_bounds__(NT, MinBlocks<R>::filter)
     k_filter_props(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<RI> in, F11<R> F, PropBuf<R> P,
-                   double* __restrict__ part, Scalars* __restrict__ S, int want_max) {
+                   double* __restrict__ part, Scalars* __restrict__ S, int want_max, Batch B) {
     const auto& K = kc<R>(C);
     __shared__ double sh[NT / 32];
     __shared__ bool last;
+    int bz = blockIdx.z;
+    if constexpr (BATCH) {
+        const int m = blockIdx.z / B.gz;
+        bz = blockIdx.z - m * B.gz;
+        const MemberTab& e = B.mt[m];
+        shift_all(in, e.delta);
+        shift_all(F, e.delta);
+        shift_props(P, e.delta);
+        attr = e.attr;
+        part = e.part;
+        S = e.S;
+    }
     const int nx = C.nx, ny = C.ny, nz = C.nz;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z * blockDim.z + threadIdx.z;
+    const int i = bz * blockDim.z + threadIdx.z;
     const int tid = (threadIdx.z * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
     const ptrdiff_t sI = (ptrdiff_t)ny * nz, sJ = (ptrdiff_t)nz;
     double mass = 0.0, mnu = 0.0, mal = 0.0;
@@ -387,9 +423,10 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::filter)
         }
     }
     // partial sums for the stage's <rho_f> (:2536-2550) and, on the last stage, the
-    // nu/alpha maxima that feed the next dt (:4401-4408)
-    const unsigned nblk = gridDim.x * gridDim.y * gridDim.z;
-    const unsigned bid = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    // nu/alpha maxima that feed the next dt (:4401-4408); in a batched launch, over the
+    // member's own blocks
+    const unsigned nblk = gridDim.x * gridDim.y * (BATCH ? (unsigned)B.gz : gridDim.z);
+    const unsigned bid = ((unsigned)bz * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
     double bm = block_sum<NT>(mass, sh, tid);
     double bn = 0.0, ba = 0.0;
     if (want_max) {
@@ -426,14 +463,27 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::filter)
 
 // ------------------------------------------------------------------ pass B: strain + nu_t + S_T
 
-template <typename R>
+template <typename R, bool BATCH = false>
 __global__ void __launch_bounds__(NT, MinBlocks<R>::strain)
-    k_strain(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> F, PropBuf<R> P) {
+    k_strain(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> F, PropBuf<R> P, Batch B) {
     const auto& K = kc<R>(C);
+    int bz = blockIdx.z;
+    ModelK<R> M;
+    if constexpr (BATCH) {
+        const int m = blockIdx.z / B.gz;
+        bz = blockIdx.z - m * B.gz;
+        const MemberTab& e = B.mt[m];
+        shift_all(F, e.delta);
+        shift_props(P, e.delta);
+        attr = e.attr;
+        M = member_model<R>(e);
+    } else {
+        M = model_of<R>(C);
+    }
     const int nx = C.nx, ny = C.ny, nz = C.nz;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z * blockDim.z + threadIdx.z;
+    const int i = bz * blockDim.z + threadIdx.z;
     if (k >= nz || j >= ny || i >= C.nx) return;
     const ptrdiff_t sI = (ptrdiff_t)ny * nz, sJ = (ptrdiff_t)nz;
     const size_t id = cid(i, j, k, ny, nz);
@@ -460,8 +510,8 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::strain)
         R g = F.p[4][id];
         if (g < R(0.0)) g = R(0.0);
         if (g > R(1.0)) g = R(1.0);
-        R cs = (R)K.cs_u + ((R)K.cs_b - (R)K.cs_u) * g;
-        cs += (R)K.cs_boost * R(4.0) * g * (R(1.0) - g);
+        R cs = M.cs_u + (M.cs_b - M.cs_u) * g;
+        cs += M.cs_boost * R(4.0) * g * (R(1.0) - g);
         const R dx = (R)K.dx;
         R nut = (cs * dx) * (cs * dx) * Smag;
         P.nu_t[id] = nut;
@@ -712,15 +762,32 @@ __device__ __forceinline__ R lap3(const Consts& C, const A& q) {
 
 // C1: momentum (:2552-2697) with calculate_convection_conservative (:683-727) and the G
 // equation (:2706-2825).  Writes k_rhou, k_rhov, k_rhow, k_G of fluid cells.
-template <typename R>
+template <typename R, bool BATCH = false>
 __global__ void __launch_bounds__(NT, MinBlocks<R>::flow)
     k_rhs_flow(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> F, PropBuf<R> P, KFlow<R> kf,
-               KDbg<R> kd, const Scalars* __restrict__ Sc) {
+               KDbg<R> kd, const Scalars* __restrict__ Sc, Batch B) {
     const auto& K = kc<R>(C);
+    int bz = blockIdx.z;
+    ModelK<R> M;
+    if constexpr (BATCH) {
+        const int m = blockIdx.z / B.gz;
+        bz = blockIdx.z - m * B.gz;
+        const MemberTab& e = B.mt[m];
+        shift_all(F, e.delta);
+        shift_props(P, e.delta);
+        shift_all(kf, e.delta);
+#pragma unroll
+        for (int q = 0; q < NACC; q++) kd.p[q] = nullptr;
+        attr = e.attr;
+        Sc = e.S;
+        M = member_model<R>(e);
+    } else {
+        M = model_of<R>(C);
+    }
     const int nx = C.nx, ny = C.ny, nz = C.nz;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z * blockDim.z + threadIdx.z;
+    const int i = bz * blockDim.z + threadIdx.z;
     if (k >= nz || j >= ny || i >= C.nx) return;
     const ptrdiff_t sI = (ptrdiff_t)ny * nz, sJ = (ptrdiff_t)nz;
     const size_t id = cid(i, j, k, ny, nz);
@@ -788,10 +855,10 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::flow)
                 } else {
                     if (dGz > R(0.0)) dGz = R(0.0);
                 }
-                R df = Gl - (R)K.accel_center;
-                R window = qexp(cdv(-(df * df), K.d_w2));
+                R df = Gl - M.accel_center;
+                R window = qexp(cdv(-(df * df), M.d_w2));
                 // tip_mask is the literal 1.0 in the momentum source (:2638)
-                R cf = (R)K.accel_strength * r0 * window * R(1.0);
+                R cf = M.accel_strength * r0 * window * R(1.0);
                 fx = cf * dGx * R(0.05);
                 fy = cf * dGy * R(1.0);
                 fz = cf * dGz * R(1.0);
@@ -854,8 +921,8 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::flow)
         if (C.flame_accel) {
             R Gl = Gf[0];
             if (Gl > R(0.1) && Gl < R(0.99)) {
-                R df = Gl - (R)K.accel_center;
-                R window = qexp(cdv(-(df * df), K.d_w2));
+                R df = Gl - M.accel_center;
+                R window = qexp(cdv(-(df * df), M.d_w2));
                 // tip_mask = 1 - exp(-r^2 / 0^2) is exactly 1 for every fluid cell (j >= 1)
                 // because TIP_PROTECTION_RADIUS is 0.0 (:234, :2806-2807).
                 R adc = R(5.0) * (P.nu_t[id] + R(1.0e-5)) * window * R(1.0);
@@ -897,7 +964,7 @@ __device__ __forceinline__ void rhs_scalar_cell(const Consts& C, const uint8_t* 
                                                 const PropBuf<R>& P, const F11<RS>& S0, const F11<R>& St,
                                                 const AccBuf<R>& acc, const KFlow<R>& kf, const KDbg<R>& kd,
                                                 const Scalars* __restrict__ Sc, int stage, int i, int j, int k,
-                                                const Src& src) {
+                                                const Src& src, const R relax) {
     const auto& K = kc<R>(C);
     const int nx = C.nx, ny = C.ny, nz = C.nz;
     const size_t id = cid(i, j, k, ny, nz);
@@ -935,7 +1002,6 @@ __device__ __forceinline__ void rhs_scalar_cell(const Consts& C, const uint8_t* 
     if (g < R(0.0)) g = R(0.0);
     if (g > R(1.0)) g = R(1.0);
     const SgsFaces<R> gs = sgs_faces<R>(src.nu(), K.d_sct2);
-    const R relax = (R)K.relax;
 #pragma unroll
     for (int s = 0; s < NSP; s++) {
         const auto qY = src.y(s);
@@ -1030,14 +1096,34 @@ __device__ __forceinline__ void rhs_scalar_cell(const Consts& C, const uint8_t* 
     }
 }
 
-template <typename R, typename RS = R>
+template <typename R, typename RS = R, bool BATCH = false>
 __global__ void __launch_bounds__(NT, MinBlocks<R>::scalar)
     k_rhs_scalar(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> F, PropBuf<R> P, F11<RS> S0, F11<R> St,
-                 AccBuf<R> acc, KFlow<R> kf, KDbg<R> kd, const Scalars* __restrict__ Sc, int stage) {
+                 AccBuf<R> acc, KFlow<R> kf, KDbg<R> kd, const Scalars* __restrict__ Sc, int stage, Batch B) {
+    int bz = blockIdx.z;
+    R relax;
+    if constexpr (BATCH) {
+        const int m = blockIdx.z / B.gz;
+        bz = blockIdx.z - m * B.gz;
+        const MemberTab& e = B.mt[m];
+        shift_all(F, e.delta);
+        shift_props(P, e.delta);
+        shift_all(S0, e.delta);
+        shift_all(St, e.delta);
+        shift_all(acc, e.delta);
+        shift_all(kf, e.delta);
+#pragma unroll
+        for (int q = 0; q < NACC; q++) kd.p[q] = nullptr;
+        attr = e.attr;
+        Sc = e.S;
+        relax = member_model<R>(e).relax;
+    } else {
+        relax = (R)kc<R>(C).relax;
+    }
     const int ny = C.ny, nz = C.nz;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z * blockDim.z + threadIdx.z;
+    const int i = bz * blockDim.z + threadIdx.z;
     if (k >= nz || j >= ny || i >= C.nx) return;
     const size_t id = cid(i, j, k, ny, nz);
     GSrc<R> src;
@@ -1047,7 +1133,7 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::scalar)
 #pragma unroll
     for (int s = 0; s < NSP; s++) src.Y[s] = F.p[6 + s] + id;
     src.nut = P.nu_t + id;
-    rhs_scalar_cell<R, RS>(C, attr, F, P, S0, St, acc, kf, kd, Sc, stage, i, j, k, src);
+    rhs_scalar_cell<R, RS>(C, attr, F, P, S0, St, acc, kf, kd, Sc, stage, i, j, k, src, relax);
 }
 
 // ------------------------------------------------------------------ boundary conditions

@@ -56,6 +56,37 @@ static inline size_t cell_blocks(const DevCtx& c, int cls) {
     return (size_t)g.x * g.y * g.z;
 }
 
+// The end of a step after the four RK stages: boundary conditions, EOS, time averages and,
+// in the device loop, the step's history and counters.
+template <typename R>
+void step_tail(DevCtx& c, cudaStream_t st, bool device_mode) {
+    F11<RS> S = f11<RS>(c.S);
+    PropBuf<R> P = props<R>(c);
+    const dim3 gE = cell_grid(c, SH_EOS), bE = cell_block(c, SH_EOS);
+    {
+        const int tpb = 128;
+        k_bc_iface<RS, R><<<dim3((c.nz + tpb - 1) / tpb, c.ny), tpb, 0, st>>>(c.hC, c.attr, S, c.plane, c.noise,
+                                                                                c.inlet_pos);
+        if (c.nx > 2) {
+            k_bc_jface<RS, R><<<dim3((c.nz + tpb - 1) / tpb, c.nx - 2), tpb, 0, st>>>(c.hC, c.attr, S);
+            k_bc_kface<RS, R><<<dim3((c.ny + tpb - 1) / tpb, c.nx - 2), tpb, 0, st>>>(c.hC, c.attr, S);
+        }
+        k_bc_eos<RS, R><<<gE, bE, 0, st>>>(c.hC, c.attr, S, c.part, c.dS);
+    }
+    if (c.avg) {
+        AvgBuf A;
+        for (int q = 0; q < NAVG; q++) A.p[q] = c.avg + (size_t)q * c.n;
+        k_time_avg<RS, R><<<MON_BLOCKS, NT, 0, st>>>(S, A, c.dS, c.n, c.avg_start);
+    }
+    if (device_mode) {
+        const int tpb = 64;
+        k_loop_post<RS, R><<<dim3((c.ny + tpb - 1) / tpb, c.loop_nst > 0 ? c.loop_nst : 1), tpb, 0, st>>>(
+            c.hC, S, P, c.dS, c.loop_st, c.loop_nst, c.loop_kline, c.loop_cap, c.hist_probe, c.hist_dt, c.hist_umax);
+        k_loop_monitor<RS, R><<<MON_BLOCKS, NT, 0, st>>>(c.hC, S, c.part, c.dS, c.n, c.loop_cap, c.hist_mon);
+        k_loop_tick<<<1, 1, 0, st>>>(c.dS);
+    }
+}
+
 // One time step.  Host-driven (device_mode false): dt and t_loop come from the caller and
 // the inflow from lesgpu_set_inflow.  Device loop (true): dt, the vortex update and the
 // inflow noise are computed on the GPU first, and the step's history is recorded at the
@@ -70,7 +101,6 @@ cudaError_t step_impl(DevCtx& c, double dt, int t_loop, bool device_mode) {
     const dim3 gB = cell_grid(c, SH_STRAIN), bB = cell_block(c, SH_STRAIN);
     const dim3 gC = cell_grid(c, SH_FLOW), bC = cell_block(c, SH_FLOW);
     const dim3 gD = cell_grid(c, SH_SCALAR), bD = cell_block(c, SH_SCALAR);
-    const dim3 gE = cell_grid(c, SH_EOS), bE = cell_block(c, SH_EOS);
     F11<RS> S = f11<RS>(c.S);
     F11<R> St = f11<R>(c.St), F = f11<R>(c.F);
     PropBuf<R> P = props<R>(c);
@@ -102,49 +132,84 @@ cudaError_t step_impl(DevCtx& c, double dt, int t_loop, bool device_mode) {
     // four RK4 stages (:4428-4544)
     for (int s = 0; s < 4; s++) {
         tm = tmark_begin(c, 1);
-        if (s == 0) k_filter_props<R, RS><<<gA, bA, 0, st>>>(c.hC, c.attr, S, F, P, c.part, c.dS, 0);
-        else k_filter_props<R, R><<<gA, bA, 0, st>>>(c.hC, c.attr, St, F, P, c.part, c.dS, s == 3 ? 1 : 0);
+        if (s == 0) k_filter_props<R, RS><<<gA, bA, 0, st>>>(c.hC, c.attr, S, F, P, c.part, c.dS, 0, Batch{});
+        else k_filter_props<R, R><<<gA, bA, 0, st>>>(c.hC, c.attr, St, F, P, c.part, c.dS, s == 3 ? 1 : 0, Batch{});
         tmark_end(c, tm);
         tm = tmark_begin(c, 2);
-        k_strain<R><<<gB, bB, 0, st>>>(c.hC, c.attr, F, P);
+        k_strain<R><<<gB, bB, 0, st>>>(c.hC, c.attr, F, P, Batch{});
         tmark_end(c, tm);
         // the k-arrays of the first stage are kept for inspection when requested
         const KDbg<R>& kds = (s == 0) ? kd : knone;
         tm = tmark_begin(c, 3);
-        k_rhs_flow<R><<<gC, bC, 0, st>>>(c.hC, c.attr, F, P, kf, kds, c.dS);
+        k_rhs_flow<R><<<gC, bC, 0, st>>>(c.hC, c.attr, F, P, kf, kds, c.dS, Batch{});
         tmark_end(c, tm);
         tm = tmark_begin(c, 5);
         if (c.scalar_tma && c.tma_ok) launch_scalar_tma<R, RS>(c, st, F, P, S, St, acc, kf, kds, s);
-        else k_rhs_scalar<R, RS><<<gD, bD, 0, st>>>(c.hC, c.attr, F, P, S, St, acc, kf, kds, c.dS, s);
+        else k_rhs_scalar<R, RS><<<gD, bD, 0, st>>>(c.hC, c.attr, F, P, S, St, acc, kf, kds, c.dS, s, Batch{});
         tmark_end(c, tm);
     }
     // apply_boundary_conditions (:2967-3161)
     if (overlap) cudaStreamWaitEvent(st, c.ev_join, 0);
     tm = tmark_begin(c, 4);
-    {
-        const int tpb = 128;
-        k_bc_iface<RS, R><<<dim3((c.nz + tpb - 1) / tpb, c.ny), tpb, 0, st>>>(c.hC, c.attr, S, c.plane, c.noise,
-                                                                                c.inlet_pos);
-        if (c.nx > 2) {
-            k_bc_jface<RS, R><<<dim3((c.nz + tpb - 1) / tpb, c.nx - 2), tpb, 0, st>>>(c.hC, c.attr, S);
-            k_bc_kface<RS, R><<<dim3((c.ny + tpb - 1) / tpb, c.nx - 2), tpb, 0, st>>>(c.hC, c.attr, S);
-        }
-        k_bc_eos<RS, R><<<gE, bE, 0, st>>>(c.hC, c.attr, S, c.part, c.dS);
-    }
-    if (c.avg) {
-        AvgBuf A;
-        for (int q = 0; q < NAVG; q++) A.p[q] = c.avg + (size_t)q * c.n;
-        k_time_avg<RS, R><<<MON_BLOCKS, NT, 0, st>>>(S, A, c.dS, c.n, c.avg_start);
-    }
-    if (device_mode) {
-        const int tpb = 64;
-        k_loop_post<RS, R><<<dim3((c.ny + tpb - 1) / tpb, c.loop_nst > 0 ? c.loop_nst : 1), tpb, 0, st>>>(
-            c.hC, S, P, c.dS, c.loop_st, c.loop_nst, c.loop_kline, c.loop_cap, c.hist_probe, c.hist_dt, c.hist_umax);
-        k_loop_monitor<RS, R><<<MON_BLOCKS, NT, 0, st>>>(c.hC, S, c.part, c.dS, c.n, c.loop_cap, c.hist_mon);
-        k_loop_tick<<<1, 1, 0, st>>>(c.dS);
-    }
+    step_tail<R>(c, st, device_mode);
     tmark_end(c, tm);
     tmark_flush(c);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ batched members
+// Several members of one grid shape and precision, stepped together: each member's step head
+// (dt, vortex and noise draws, SEM plane) and tail (boundary conditions, history) on its own
+// stream as above, and the four RK stages of all of them in one launch per pass, whose grid is
+// the first member's grid repeated along z once per member.  Every block reads its member's
+// arena offset, attribute map, reductions and model constants from the member table (les_common.cuh,
+// MemberTab); the tiles are the first member's.
+
+template <typename R>
+cudaError_t batch_head(DevCtx& c) {
+    loop_pre(c);
+    sem_inflow(c, c.stream);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t batch_tail(DevCtx& c) {
+    step_tail<R>(c, c.stream, true);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t batch_stages(DevCtx& c0, const MemberTab* mt, int nmem, cudaStream_t st) {
+    if (nmem < 1 || !part_fits(c0, cell_blocks(c0, SH_FILTER), 3)) return cudaErrorInvalidValue;
+    auto grid = [&](int cls, Batch& b) {
+        dim3 g = cell_grid(c0, cls);
+        b.mt = mt;
+        b.gz = (int)g.z;
+        g.z *= (unsigned)nmem;
+        return g;
+    };
+    Batch BA, BB, BC, BD;
+    const dim3 gA = grid(SH_FILTER, BA), bA = cell_block(c0, SH_FILTER);
+    const dim3 gB = grid(SH_STRAIN, BB), bB = cell_block(c0, SH_STRAIN);
+    const dim3 gC = grid(SH_FLOW, BC), bC = cell_block(c0, SH_FLOW);
+    const dim3 gD = grid(SH_SCALAR, BD), bD = cell_block(c0, SH_SCALAR);
+    if (gA.z > 65535u || gB.z > 65535u || gC.z > 65535u || gD.z > 65535u) return cudaErrorInvalidConfiguration;
+    F11<RS> S = f11<RS>(c0.S);
+    F11<R> St = f11<R>(c0.St), F = f11<R>(c0.F);
+    PropBuf<R> P = props<R>(c0);
+    AccBuf<R> acc;
+    for (int q = 0; q < NACC; q++) acc.p[q] = (R*)c0.acc[q];
+    KDbg<R> knone;
+    for (int q = 0; q < NACC; q++) knone.p[q] = nullptr;
+    KFlow<R> kf;
+    for (int q = 0; q < 4; q++) kf.p[q] = (R*)c0.kflow[q];
+    for (int s = 0; s < 4; s++) {
+        if (s == 0) k_filter_props<R, RS, true><<<gA, bA, 0, st>>>(c0.hC, c0.attr, S, F, P, c0.part, c0.dS, 0, BA);
+        else k_filter_props<R, R, true><<<gA, bA, 0, st>>>(c0.hC, c0.attr, St, F, P, c0.part, c0.dS, s == 3 ? 1 : 0, BA);
+        k_strain<R, true><<<gB, bB, 0, st>>>(c0.hC, c0.attr, F, P, BB);
+        k_rhs_flow<R, true><<<gC, bC, 0, st>>>(c0.hC, c0.attr, F, P, kf, knone, c0.dS, BC);
+        k_rhs_scalar<R, RS, true><<<gD, bD, 0, st>>>(c0.hC, c0.attr, F, P, S, St, acc, kf, knone, c0.dS, s, BD);
+    }
     return cudaGetLastError();
 }
 
@@ -168,20 +233,22 @@ cudaError_t rhs_only_impl(DevCtx& c, int t_loop) {
     k_set_step<<<1, 1, 0, st>>>(c.dS, 0.0, t_loop);
     int tm = tmark_begin(c, 1);
     k_filter_props<R, RS><<<cell_grid(c, SH_FILTER), cell_block(c, SH_FILTER), 0, st>>>(c.hC, c.attr, S, F, P,
-                                                                                       c.part, c.dS, 1);
+                                                                                       c.part, c.dS, 1, Batch{});
     tmark_end(c, tm);
     tm = tmark_begin(c, 2);
-    k_strain<R><<<cell_grid(c, SH_STRAIN), cell_block(c, SH_STRAIN), 0, st>>>(c.hC, c.attr, F, P);
+    k_strain<R><<<cell_grid(c, SH_STRAIN), cell_block(c, SH_STRAIN), 0, st>>>(c.hC, c.attr, F, P, Batch{});
     tmark_end(c, tm);
     tm = tmark_begin(c, 3);
-    k_rhs_flow<R><<<cell_grid(c, SH_FLOW), cell_block(c, SH_FLOW), 0, st>>>(c.hC, c.attr, F, P, kf, kd, c.dS);
+    k_rhs_flow<R><<<cell_grid(c, SH_FLOW), cell_block(c, SH_FLOW), 0, st>>>(c.hC, c.attr, F, P, kf, kd, c.dS,
+                                                                            Batch{});
     tmark_end(c, tm);
     tm = tmark_begin(c, 5);
     if (c.scalar_tma && c.tma_ok)
         launch_scalar_tma<R, RS>(c, st, F, P, S, St, acc, kf, kd, 0);
     else
         k_rhs_scalar<R, RS><<<cell_grid(c, SH_SCALAR), cell_block(c, SH_SCALAR), 0, st>>>(c.hC, c.attr, F, P, S, St,
-                                                                                           acc, kf, kd, c.dS, 0);
+                                                                                           acc, kf, kd, c.dS, 0,
+                                                                                           Batch{});
     tmark_end(c, tm);
     tmark_flush(c);
     return cudaGetLastError();

@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(TMA_TK* TMA_TJ, (sizeof(R) == 8) ? 2 : 3)
                                (kl + G::KOFF);
             }
             src.Nv.bw = G::BW;
-            rhs_scalar_cell<R, RS>(C, attr, F, P, S0, St, acc, kf, kd, Sc, stage, i, j, k, src);
+            rhs_scalar_cell<R, RS>(C, attr, F, P, S0, St, acc, kf, kd, Sc, stage, i, j, k, src, (R)kc<R>(C).relax);
         }
         __syncthreads();                            // the plane of step rc - 2 is free
         if (tid == 0 && rc + 3 < nsteps) {

@@ -16,6 +16,7 @@
 
 struct les_ensemble {
     int n;
+    int batched;          /* lesgpu_group_create_batched instead of lesgpu_group_create */
     les_solver** members;
     char err[256];
 };
@@ -91,7 +92,7 @@ int les_ensemble_run(les_ensemble* e, int nsteps, int chunk) {
     }
     if (rc == LESGPU_OK) {
         for (int q = 0; q < e->n; q++) ctxs[q] = les_solver_ctx(e->members[q]);
-        rc = lesgpu_group_create(ctxs, e->n, &g);
+        rc = e->batched ? lesgpu_group_create_batched(ctxs, e->n, &g) : lesgpu_group_create(ctxs, e->n, &g);
     }
     int left = nsteps;
     while (rc == LESGPU_OK && left > 0) {
@@ -120,6 +121,12 @@ int les_ensemble_run(les_ensemble* e, int nsteps, int chunk) {
         if (bad < 0 && ctxs == NULL && e->n > 0) msg = lesgpu_last_error(les_solver_ctx(e->members[0]));
         return eerr(e, rc, msg, bad);
     }
+    return LESGPU_OK;
+}
+
+int les_ensemble_set_batched(les_ensemble* e, int enable) {
+    if (!e) return LESGPU_EINVAL;
+    e->batched = enable != 0;
     return LESGPU_OK;
 }
 

@@ -39,10 +39,12 @@ def ensemble_configs(n: int = 64, seed: int = 2024, grids: Sequence[str] = ("e12
 
 
 class Ensemble:
-    """n solvers on one device stepped by one multi-stream graph per step."""
+    """n solvers on one device stepped by one CUDA graph per step: a multi-stream graph of
+    every member's kernels, or (batched=True) one launch per RK pass for all members of one
+    grid shape (lesgpu_group_create_batched)."""
 
     def __init__(self, cfgs: Sequence[SolverConfig], precision: int = N.FP32, autotune: bool = True, device: int = 0,
-                 chem: str = N.CHEM_BIN, tran: str = N.TRAN_BIN):
+                 chem: str = N.CHEM_BIN, tran: str = N.TRAN_BIN, batched: bool = False):
         L = N.lib()
         arr = (N.LesgpuConfig * len(cfgs))(*[N.LesgpuConfig.from_config(c, precision, device) for c in cfgs])
         h = C.c_void_p()
@@ -50,6 +52,10 @@ class Ensemble:
         if rc != 0:
             raise N.LesgpuError(rc, "les_ensemble_create failed")
         self._h = h
+        if batched:
+            rc = L.les_ensemble_set_batched(h, 1)
+            if rc != 0:
+                raise N.LesgpuError(rc, "les_ensemble_set_batched failed")
         self.cfgs = list(cfgs)
         self.members = [N.Solver.wrap(L.les_ensemble_member(h, q), c) for q, c in enumerate(self.cfgs)]
 
@@ -93,6 +99,8 @@ def main(argv=None) -> int:
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--chunk", type=int, default=64)
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--batched", action="store_true",
+                    help="one launch per RK pass for all members of a grid shape instead of the multi-stream graph")
     ap.add_argument("--sequential", action="store_true",
                     help="also time one solo solver per grid and sum them over the members")
     a = ap.parse_args(argv)
@@ -100,9 +108,10 @@ def main(argv=None) -> int:
     grids = tuple(a.grids.split(","))
     cfgs = ensemble_configs(a.members, grids=grids)
     out = {"members": a.members, "grids": dict(Counter(grids[q % len(grids)] for q in range(a.members))),
-           "precision": a.precision, "steps": a.steps, "chunk": a.chunk, "autotune": not a.no_autotune}
+           "precision": a.precision, "steps": a.steps, "chunk": a.chunk, "autotune": not a.no_autotune,
+           "form": "batched" if a.batched else "multi-stream"}
     t = time.perf_counter()
-    ens = Ensemble(cfgs, precision=prec, autotune=not a.no_autotune)
+    ens = Ensemble(cfgs, precision=prec, autotune=not a.no_autotune, batched=a.batched)
     out["create_s"] = time.perf_counter() - t
     tiles = {}
     for q, m in enumerate(ens.members):

@@ -169,6 +169,18 @@ int lesgpu_loop_end(lesgpu_ctx* ctx, unsigned int rng_window[31], double* vortic
  * results are bit-identical to running it alone with the same tiles.  Changing a member's
  * tiles or history layout after lesgpu_group_create requires a new group. */
 int lesgpu_group_create(lesgpu_ctx* const* ctxs, int n, lesgpu_group** out);
+/* The batched form of a group: members whose constants agree except the model constants an
+ * optimiser varies (CS_UNBURNED, CS_BURNT, CS_FLAME_BOOST, the flame-acceleration strength,
+ * width and centre, the nudging coefficient) and whose grid shape, precision and tiles agree
+ * form one batch, and each RK pass of a batch is ONE launch over a (member, tile) grid: blocks
+ * find their member's field arena, attribute map, reductions and model constants in a member
+ * table.  Each member's dt, rand() draws and SEM plane before, and its boundary conditions and
+ * history after, run on its own stream; one step of everything is one CUDA graph.  Members need
+ * inspection buffers, |grad G| and the staged scalar pass off.  Results are bit-identical to
+ * running each member alone with the same tiles.  lesgpu_group_batches: the number of batches
+ * (in the multi-stream form, the number of members). */
+int lesgpu_group_create_batched(lesgpu_ctx* const* ctxs, int n, lesgpu_group** out);
+int lesgpu_group_batches(const lesgpu_group* g);
 int lesgpu_group_run(lesgpu_group* g, int nsteps);
 void lesgpu_group_destroy(lesgpu_group* g);
 

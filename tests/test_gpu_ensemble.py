@@ -191,3 +191,65 @@ def test_staged_scalar_pass_gives_the_same_bits(N, name, prec):
             np.testing.assert_array_equal(out[0][f], out[1][f], err_msg=f)
         else:
             np.testing.assert_allclose(out[1][f], out[0][f], rtol=1e-5, atol=1e-9, err_msg=f)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_batched_ensemble_matches_solo_runs(N, prec, tmp_path):
+    """The batched form (one launch per RK pass over the members of a grid shape, each block
+    reading its member's arena, reductions and model constants from the member table): every
+    member bit-identical to a solo run with the same tiles, output files included.  Two grid
+    shapes, members with different model constants and seeds, and one member whose other
+    constants differ (its own batch)."""
+    from lesgpu.config import preset
+    from lesgpu.ensemble import Ensemble
+    P = N.FP64 if prec == "fp64" else N.FP32
+    cfgs = [preset("tiny", seed=21, cs_unburned=0.09, relax=2500.0),
+            preset("small", seed=22, accel_strength=3.5, cs_burnt=0.3),
+            preset("tiny", seed=23, cs_unburned=0.2, accel_center=0.5, accel_width=0.2, cs_flame_boost=0.1),
+            preset("small", seed=24, relax=100.0),
+            preset("tiny", seed=25, s_l=0.45, courant=0.2)]
+    ens = Ensemble(cfgs, precision=P, autotune=True, batched=True)
+    dirs = []
+    for q, m in enumerate(ens.members):
+        d = tmp_path / f"ens{q}"
+        d.mkdir()
+        m.set_outputs(str(d), N.LES_OUT_PROBES | N.LES_OUT_MONITOR)
+        dirs.append(str(d))
+    ens.run(9, chunk=4)
+    ens.run(5, chunk=5)
+    got = [m.state() for m in ens.members]
+    tiles = [m.ctx.get_tiles() for m in ens.members]
+    ens.close()
+    for q, (cfg, st, tl) in enumerate(zip(cfgs, got, tiles)):
+        solo = N.Solver(cfg, precision=P)
+        solo.ctx.set_tiles(tl)
+        d = tmp_path / f"solo{q}"
+        d.mkdir()
+        solo.set_outputs(str(d), N.LES_OUT_PROBES | N.LES_OUT_MONITOR)
+        solo.run_device(14, chunk=14)
+        ref = solo.state()
+        for f in STATE:
+            np.testing.assert_array_equal(st[f], ref[f], err_msg=f"member {q}: {f}")
+        assert _files(dirs[q]) == _files(str(d)), f"member {q}: output files differ"
+        solo.close()
+
+
+def test_batched_group_forms_batches_by_shape_and_constants(N):
+    """Members batch together only when grid, precision, tiles and every kernel constant but
+    the optimiser's agree (the Courant number only enters each member's own dt)."""
+    import ctypes as C
+    from lesgpu.config import preset
+    cfgs = [preset("tiny", seed=1), preset("tiny", seed=2, cs_unburned=0.1, relax=10.0), preset("small", seed=3),
+            preset("tiny", seed=4, s_l=0.45), preset("small", seed=5, accel_strength=1.0, courant=0.2)]
+    sols = [N.Solver(c) for c in cfgs]
+    for s in sols:
+        s.loop_begin(chunk=4)
+    arr = (C.c_void_p * len(sols))(*[s.ctx._h.value for s in sols])
+    g = C.c_void_p()
+    assert N.lib().lesgpu_group_create_batched(arr, len(sols), C.byref(g)) == 0
+    assert N.lib().lesgpu_group_batches(g) == 3          # {tiny 1, 2}, {small 3, 5}, {tiny 4}
+    assert N.lib().lesgpu_group_run(g, 3) == 0
+    N.lib().lesgpu_group_destroy(g)
+    for s in sols:
+        s.loop_end()
+        s.close()
