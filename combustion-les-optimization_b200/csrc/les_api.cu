@@ -1410,8 +1410,8 @@ int lesgpu_group_create(lesgpu_ctx* const* ctxs, int n, lesgpu_group** out) {
     return LESGPU_OK;
 }
 
-int lesgpu_group_create_batched(lesgpu_ctx* const* ctxs, int n, lesgpu_group** out) {
-    if (!ctxs || n < 1 || !out) return LESGPU_EINVAL;
+int lesgpu_group_create_batched(lesgpu_ctx* const* ctxs, int n, int max_per_batch, lesgpu_group** out) {
+    if (!ctxs || n < 1 || !out || max_per_batch < 0) return LESGPU_EINVAL;
     *out = nullptr;
     for (int q = 0; q < n; q++) {
         if (!ctxs[q]) return LESGPU_EINVAL;
@@ -1430,10 +1430,14 @@ int lesgpu_group_create_batched(lesgpu_ctx* const* ctxs, int n, lesgpu_group** o
     g->m.assign(ctxs, ctxs + n);
     g->device = ctxs[0]->cfg.device;
     lesgpu_ctx* c0 = ctxs[0];
-    // batches: each member joins the first batch whose first member it matches
+    // batches: each member joins the first batch whose first member it matches and that has
+    // room (at most max_per_batch members; 0: no limit)
     for (int q = 0; q < n; q++) {
         size_t b = 0;
-        while (b < g->batches.size() && !batchable(ctxs[g->batches[b][0]]->d, ctxs[q]->d)) b++;
+        while (b < g->batches.size() &&
+               (!batchable(ctxs[g->batches[b][0]]->d, ctxs[q]->d) ||
+                (max_per_batch > 0 && (int)g->batches[b].size() >= max_per_batch)))
+            b++;
         if (b == g->batches.size()) g->batches.emplace_back();
         g->batches[b].push_back(q);
     }

@@ -17,6 +17,7 @@
 struct les_ensemble {
     int n;
     int batched;          /* lesgpu_group_create_batched instead of lesgpu_group_create */
+    int per_batch;        /* its max_per_batch */
     les_solver** members;
     char err[256];
 };
@@ -92,7 +93,7 @@ int les_ensemble_run(les_ensemble* e, int nsteps, int chunk) {
     }
     if (rc == LESGPU_OK) {
         for (int q = 0; q < e->n; q++) ctxs[q] = les_solver_ctx(e->members[q]);
-        rc = e->batched ? lesgpu_group_create_batched(ctxs, e->n, &g) : lesgpu_group_create(ctxs, e->n, &g);
+        rc = e->batched ? lesgpu_group_create_batched(ctxs, e->n, e->per_batch, &g) : lesgpu_group_create(ctxs, e->n, &g);
     }
     int left = nsteps;
     while (rc == LESGPU_OK && left > 0) {
@@ -124,9 +125,10 @@ int les_ensemble_run(les_ensemble* e, int nsteps, int chunk) {
     return LESGPU_OK;
 }
 
-int les_ensemble_set_batched(les_ensemble* e, int enable) {
-    if (!e) return LESGPU_EINVAL;
+int les_ensemble_set_batched(les_ensemble* e, int enable, int max_per_batch) {
+    if (!e || max_per_batch < 0) return LESGPU_EINVAL;
     e->batched = enable != 0;
+    e->per_batch = max_per_batch;
     return LESGPU_OK;
 }
 

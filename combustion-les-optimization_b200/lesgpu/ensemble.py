@@ -44,7 +44,7 @@ class Ensemble:
     grid shape (lesgpu_group_create_batched)."""
 
     def __init__(self, cfgs: Sequence[SolverConfig], precision: int = N.FP32, autotune: bool = True, device: int = 0,
-                 chem: str = N.CHEM_BIN, tran: str = N.TRAN_BIN, batched: bool = False):
+                 chem: str = N.CHEM_BIN, tran: str = N.TRAN_BIN, batched: bool = False, per_batch: int = 0):
         L = N.lib()
         arr = (N.LesgpuConfig * len(cfgs))(*[N.LesgpuConfig.from_config(c, precision, device) for c in cfgs])
         h = C.c_void_p()
@@ -53,7 +53,7 @@ class Ensemble:
             raise N.LesgpuError(rc, "les_ensemble_create failed")
         self._h = h
         if batched:
-            rc = L.les_ensemble_set_batched(h, 1)
+            rc = L.les_ensemble_set_batched(h, 1, per_batch)
             if rc != 0:
                 raise N.LesgpuError(rc, "les_ensemble_set_batched failed")
         self.cfgs = list(cfgs)
@@ -101,6 +101,7 @@ def main(argv=None) -> int:
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--batched", action="store_true",
                     help="one launch per RK pass for all members of a grid shape instead of the multi-stream graph")
+    ap.add_argument("--per-batch", type=int, default=0, help="with --batched: at most this many members per launch")
     ap.add_argument("--sequential", action="store_true",
                     help="also time one solo solver per grid and sum them over the members")
     a = ap.parse_args(argv)
@@ -109,9 +110,9 @@ def main(argv=None) -> int:
     cfgs = ensemble_configs(a.members, grids=grids)
     out = {"members": a.members, "grids": dict(Counter(grids[q % len(grids)] for q in range(a.members))),
            "precision": a.precision, "steps": a.steps, "chunk": a.chunk, "autotune": not a.no_autotune,
-           "form": "batched" if a.batched else "multi-stream"}
+           "form": f"batched (max {a.per_batch or 'all'} per launch)" if a.batched else "multi-stream"}
     t = time.perf_counter()
-    ens = Ensemble(cfgs, precision=prec, autotune=not a.no_autotune, batched=a.batched)
+    ens = Ensemble(cfgs, precision=prec, autotune=not a.no_autotune, batched=a.batched, per_batch=a.per_batch)
     out["create_s"] = time.perf_counter() - t
     tiles = {}
     for q, m in enumerate(ens.members):

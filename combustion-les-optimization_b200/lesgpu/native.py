@@ -173,8 +173,8 @@ def lib():
         _sig(L, "lesgpu_group_destroy", None, [vp])
         _sig(L, "les_ensemble_create", C.c_int, [vp, C.c_int, C.c_char_p, C.c_char_p, C.c_int, C.POINTER(vp)])
         _sig(L, "les_ensemble_run", C.c_int, [vp, C.c_int, C.c_int])
-        _sig(L, "les_ensemble_set_batched", C.c_int, [vp, C.c_int])
-        _sig(L, "lesgpu_group_create_batched", C.c_int, [vp, C.c_int, C.POINTER(vp)])
+        _sig(L, "les_ensemble_set_batched", C.c_int, [vp, C.c_int, C.c_int])
+        _sig(L, "lesgpu_group_create_batched", C.c_int, [vp, C.c_int, C.c_int, C.POINTER(vp)])
         _sig(L, "lesgpu_group_batches", C.c_int, [vp])
         _sig(L, "les_ensemble_size", C.c_int, [vp])
         _sig(L, "les_ensemble_member", vp, [vp, C.c_int])

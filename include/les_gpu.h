@@ -177,9 +177,12 @@ int lesgpu_group_create(lesgpu_ctx* const* ctxs, int n, lesgpu_group** out);
  * table.  Each member's dt, rand() draws and SEM plane before, and its boundary conditions and
  * history after, run on its own stream; one step of everything is one CUDA graph.  Members need
  * inspection buffers, |grad G| and the staged scalar pass off.  Results are bit-identical to
- * running each member alone with the same tiles.  lesgpu_group_batches: the number of batches
- * (in the multi-stream form, the number of members). */
-int lesgpu_group_create_batched(lesgpu_ctx* const* ctxs, int n, lesgpu_group** out);
+ * running each member alone with the same tiles in FP64 (in FP32 up to the FMA contraction
+ * of the batched kernels, ~1e-7).  max_per_batch > 0 caps a batch's size: smaller batches on
+ * their own streams let one batch's passes overlap another's (0: no cap).
+ * lesgpu_group_batches: the number of batches (in the multi-stream form, the number of
+ * members). */
+int lesgpu_group_create_batched(lesgpu_ctx* const* ctxs, int n, int max_per_batch, lesgpu_group** out);
 int lesgpu_group_batches(const lesgpu_group* g);
 int lesgpu_group_run(lesgpu_group* g, int nsteps);
 void lesgpu_group_destroy(lesgpu_group* g);

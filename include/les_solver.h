@@ -180,9 +180,10 @@ int les_ensemble_create(const lesgpu_config* cfgs, int n, const char* chem_path,
                         les_ensemble** out);
 int les_ensemble_run(les_ensemble* e, int nsteps, int chunk);
 /* Step the members with the batched group form (lesgpu_group_create_batched: one launch per
- * RK pass for all members of one grid shape) instead of the multi-stream graph; off by
- * default.  Same results either way. */
-int les_ensemble_set_batched(les_ensemble* e, int enable);
+ * RK pass for the members of one grid shape, at most max_per_batch per launch, 0: no cap)
+ * instead of the multi-stream graph (enable = 0, the default).  Same results in FP64; in FP32
+ * up to the batched kernels' FMA contraction. */
+int les_ensemble_set_batched(les_ensemble* e, int enable, int max_per_batch);
 int les_ensemble_size(const les_ensemble* e);
 les_solver* les_ensemble_member(les_ensemble* e, int i);
 const char* les_ensemble_last_error(const les_ensemble* e);

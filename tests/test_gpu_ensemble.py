@@ -196,10 +196,12 @@ def test_staged_scalar_pass_gives_the_same_bits(N, name, prec):
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
 def test_batched_ensemble_matches_solo_runs(N, prec, tmp_path):
     """The batched form (one launch per RK pass over the members of a grid shape, each block
-    reading its member's arena, reductions and model constants from the member table): every
-    member bit-identical to a solo run with the same tiles, output files included.  Two grid
-    shapes, members with different model constants and seeds, and one member whose other
-    constants differ (its own batch)."""
+    reading its member's arena, reductions and model constants from the member table) against
+    solo runs with the same tiles: FP64 members bit-identical, output files included; FP32
+    members within 1e-6 relative L2 per field (the FP32 unit is built with FMA contraction,
+    and the batched instantiation of a kernel may contract differently from the solo one).
+    Two grid shapes, members with different model constants and seeds, and one member whose
+    other constants differ (its own batch)."""
     from lesgpu.config import preset
     from lesgpu.ensemble import Ensemble
     P = N.FP64 if prec == "fp64" else N.FP32
@@ -208,7 +210,7 @@ def test_batched_ensemble_matches_solo_runs(N, prec, tmp_path):
             preset("tiny", seed=23, cs_unburned=0.2, accel_center=0.5, accel_width=0.2, cs_flame_boost=0.1),
             preset("small", seed=24, relax=100.0),
             preset("tiny", seed=25, s_l=0.45, courant=0.2)]
-    ens = Ensemble(cfgs, precision=P, autotune=True, batched=True)
+    ens = Ensemble(cfgs, precision=P, autotune=True, batched=True, per_batch=0 if prec == "fp64" else 2)
     dirs = []
     for q, m in enumerate(ens.members):
         d = tmp_path / f"ens{q}"
@@ -228,9 +230,14 @@ def test_batched_ensemble_matches_solo_runs(N, prec, tmp_path):
         solo.set_outputs(str(d), N.LES_OUT_PROBES | N.LES_OUT_MONITOR)
         solo.run_device(14, chunk=14)
         ref = solo.state()
-        for f in STATE:
-            np.testing.assert_array_equal(st[f], ref[f], err_msg=f"member {q}: {f}")
-        assert _files(dirs[q]) == _files(str(d)), f"member {q}: output files differ"
+        if P == N.FP64:
+            for f in STATE:
+                np.testing.assert_array_equal(st[f], ref[f], err_msg=f"member {q}: {f}")
+            assert _files(dirs[q]) == _files(str(d)), f"member {q}: output files differ"
+        else:
+            for f in STATE:
+                e = np.linalg.norm(st[f] - ref[f]) / max(np.linalg.norm(ref[f]), 1e-300)
+                assert e <= 1e-6, f"member {q}: {f} rel L2 {e:.2e}"
         solo.close()
 
 
@@ -246,9 +253,13 @@ def test_batched_group_forms_batches_by_shape_and_constants(N):
         s.loop_begin(chunk=4)
     arr = (C.c_void_p * len(sols))(*[s.ctx._h.value for s in sols])
     g = C.c_void_p()
-    assert N.lib().lesgpu_group_create_batched(arr, len(sols), C.byref(g)) == 0
+    assert N.lib().lesgpu_group_create_batched(arr, len(sols), 0, C.byref(g)) == 0
     assert N.lib().lesgpu_group_batches(g) == 3          # {tiny 1, 2}, {small 3, 5}, {tiny 4}
     assert N.lib().lesgpu_group_run(g, 3) == 0
+    N.lib().lesgpu_group_destroy(g)
+    g = C.c_void_p()
+    assert N.lib().lesgpu_group_create_batched(arr, len(sols), 1, C.byref(g)) == 0
+    assert N.lib().lesgpu_group_batches(g) == 5          # at most one member per batch
     N.lib().lesgpu_group_destroy(g)
     for s in sols:
         s.loop_end()
