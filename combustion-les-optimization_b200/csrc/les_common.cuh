@@ -194,7 +194,7 @@ struct Scalars {
     double umax, numax, alphamax;       // dt inputs (:1472-1485, :4401-4408)
     double mon[6];                      // monitor reductions
     double sem[6];                      // SEM sums (debug)
-    unsigned int counter[5];            // last-block counters (0: filter, 1: bc, 2: aux, 3: monitor, 4: props)
+    unsigned int counter[4];            // last-block counters (0: filter, 1: bc, 2: aux, 3: monitor)
     int nonfinite;                      // bit 1: rand() jump table too short (device loop)
     double dt;                          // dt of the step being computed
     double umax_used;                   // |u|max that produced dt (after the inlet fallback)

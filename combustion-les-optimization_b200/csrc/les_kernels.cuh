@@ -461,134 +461,6 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::filter)
     }
 }
 
-// Pass A as two kernels (build option LES_SPLIT_PROPS): the filter alone, with the <rho_f>
-// partial sums, then the cell-local properties from the filtered fields, with the nu/alpha
-// maxima on the last stage.  Same arithmetic as k_filter_props.
-template <typename R, typename RI = R>
-__global__ void __launch_bounds__(NT) k_filter_only(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<RI> in,
-                                                   F11<R> F, double* __restrict__ part, Scalars* __restrict__ S) {
-    const auto& K = kc<R>(C);
-    __shared__ double sh[NT / 32];
-    __shared__ bool last;
-    const int nx = C.nx, ny = C.ny, nz = C.nz;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z * blockDim.z + threadIdx.z;
-    const int tid = (threadIdx.z * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
-    const ptrdiff_t sI = (ptrdiff_t)ny * nz, sJ = (ptrdiff_t)nz;
-    double mass = 0.0;
-    if (k < nz && j < ny && i < C.nx) {
-        const size_t id = cid(i, j, k, ny, nz);
-        const int a = attr[id];
-        const bool filt = (a == 3) && i >= 1 && i < nx - 1 && j >= 1 && j < ny - 1 && k >= 1 && k < nz - 1;
-        R rf = R(0);
-#pragma unroll
-        for (int q = 0; q < NSTATE; q++) {
-            const RI* __restrict__ x = in.p[q] + id;
-            R f;
-            if (filt) {
-                f = cdv(R(x[-sI]) + R(x[-sJ]) + R(x[-1]) + R(FILTER_W) * R(x[0]) + R(x[1]) + R(x[sJ]) + R(x[sI]),
-                        K.d_filter);
-            } else {
-                f = R(x[0]);
-            }
-            F.p[q][id] = f;
-            if (q == 5) rf = f;
-        }
-        if (a == 1 || a == 2 || a == 3 || a == 5) mass = (((double)rf * C.dx) * C.dy) * C.dz;
-    }
-    const unsigned nblk = gridDim.x * gridDim.y * gridDim.z;
-    const unsigned bid = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-    double bm = block_sum<NT>(mass, sh, tid);
-    if (tid == 0) {
-        part[bid] = bm;
-        __threadfence();
-        unsigned t = atomicAdd(&S->counter[0], 1u);
-        last = (t == nblk - 1);
-    }
-    __syncthreads();
-    if (last) {
-        __threadfence();
-        double s = 0.0;
-#pragma unroll 8
-        for (unsigned q = tid; q < nblk; q += NT) s += __ldcg(&part[q]);
-        s = block_sum<NT>(s, sh, tid);
-        if (tid == 0) {
-            S->rho_avg = (C.total_volume > 0) ? (s / C.total_volume) : 1.2;
-            S->counter[0] = 0u;
-        }
-    }
-}
-
-template <typename R>
-__global__ void __launch_bounds__(NT, MinBlocks<R>::filter)
-    k_props(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> F, PropBuf<R> P, double* __restrict__ part,
-            Scalars* __restrict__ S, int want_max) {
-    __shared__ double sh[NT / 32];
-    __shared__ bool last;
-    const int ny = C.ny, nz = C.nz;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z * blockDim.z + threadIdx.z;
-    const int tid = (threadIdx.z * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
-    double mnu = 0.0, mal = 0.0;
-    if (k < nz && j < ny && i < C.nx) {
-        const size_t id = cid(i, j, k, ny, nz);
-        const int a = attr[id];
-        if (a == 3) {
-            R Yf[NSP];
-#pragma unroll
-            for (int s = 0; s < NSP; s++) Yf[s] = F.p[6 + s][id];
-            R mu_mix, nu, D[NSP], aT, cp, lam, alpha;
-            cell_props<R>(C, F.p[3][id], Yf, F.p[5][id], mu_mix, nu, D, aT, cp, lam, alpha);
-            P.mu_mix[id] = mu_mix;
-            P.nu[id] = nu;
-#pragma unroll
-            for (int s = 0; s < NSP; s++) P.D[s][id] = D[s];
-            P.aT[id] = aT;
-            if (P.dbg_cp) { P.dbg_cp[id] = cp; P.dbg_lam[id] = lam; P.dbg_alpha[id] = alpha; }
-            mnu = (double)nu;
-            mal = (double)alpha;
-        } else if (P.dbg_cp) {
-            P.mu_mix[id] = R(1.8e-5);
-            P.nu[id] = R(1.5e-5);
-#pragma unroll
-            for (int s = 0; s < NSP; s++) P.D[s][id] = R(0);
-            P.aT[id] = R(0);
-            P.dbg_cp[id] = R(1000.0); P.dbg_lam[id] = R(0); P.dbg_alpha[id] = R(0);
-        }
-    }
-    if (!want_max) return;                     // uniform across the grid
-    const unsigned nblk = gridDim.x * gridDim.y * gridDim.z;
-    const unsigned bid = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-    double bn = block_max<NT>(mnu, sh, tid);
-    double ba = block_max<NT>(mal, sh, tid);
-    if (tid == 0) {
-        part[nblk + bid] = bn;
-        part[2 * nblk + bid] = ba;
-        __threadfence();
-        unsigned t = atomicAdd(&S->counter[4], 1u);
-        last = (t == nblk - 1);
-    }
-    __syncthreads();
-    if (last) {
-        __threadfence();
-        double mn = 0.0, ma = 0.0;
-#pragma unroll 8
-        for (unsigned q = tid; q < nblk; q += NT) {
-            mn = fmax(mn, __ldcg(&part[nblk + q]));
-            ma = fmax(ma, __ldcg(&part[2 * nblk + q]));
-        }
-        mn = block_max<NT>(mn, sh, tid);
-        ma = block_max<NT>(ma, sh, tid);
-        if (tid == 0) {
-            S->numax = mn;
-            S->alphamax = ma;
-            S->counter[4] = 0u;
-        }
-    }
-}
-
 // ------------------------------------------------------------------ pass B: strain + nu_t + S_T
 
 template <typename R, bool BATCH = false>

@@ -132,14 +132,8 @@ cudaError_t step_impl(DevCtx& c, double dt, int t_loop, bool device_mode) {
     // four RK4 stages (:4428-4544)
     for (int s = 0; s < 4; s++) {
         tm = tmark_begin(c, 1);
-#ifdef LES_SPLIT_PROPS
-        if (s == 0) k_filter_only<R, RS><<<gA, bA, 0, st>>>(c.hC, c.attr, S, F, c.part, c.dS);
-        else k_filter_only<R, R><<<gA, bA, 0, st>>>(c.hC, c.attr, St, F, c.part, c.dS);
-        k_props<R><<<gA, bA, 0, st>>>(c.hC, c.attr, F, P, c.part, c.dS, s == 3 ? 1 : 0);
-#else
         if (s == 0) k_filter_props<R, RS><<<gA, bA, 0, st>>>(c.hC, c.attr, S, F, P, c.part, c.dS, 0, Batch{});
         else k_filter_props<R, R><<<gA, bA, 0, st>>>(c.hC, c.attr, St, F, P, c.part, c.dS, s == 3 ? 1 : 0, Batch{});
-#endif
         tmark_end(c, tm);
         tm = tmark_begin(c, 2);
         k_strain<R><<<gB, bB, 0, st>>>(c.hC, c.attr, F, P, Batch{});
