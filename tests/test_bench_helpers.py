@@ -22,6 +22,9 @@ def test_algorithmic_bytes_per_cell():
     assert b.kernel_bytes_per_cell("rhs_scalar", 4) == 307
     assert b.kernel_bytes_per_cell("filter_props", 4) == 131
     assert b.STEP_BYTES_PER_CELL == 52 * 4 * 8
+    # a stage kernel's launch is credited with one stage's share of the whole-step figure
+    assert set(b.STAGE_KERNELS) == {"filter_props", "strain", "rhs_flow", "rhs_scalar"}
+    assert b.STEP_BYTES_PER_CELL * 8 / 8 / 4 == 416
 
 
 def test_committed_traffic_covers_the_stage_kernels():
