@@ -128,6 +128,7 @@ void les_serve_default_options(les_serve_options* o) {
     o->keep_results = 1;
     o->autotune = 0;
     o->backfill = 0;
+    o->policy = LES_SERVE_FIFO;
     o->device = 0;
     o->prep_threads = 4;
 }
@@ -282,6 +283,7 @@ int les_serve_create(const les_serve_options* opt, les_serve** out) {
     if (!opt || !out || opt->max_slots < 1 || opt->quantum_steps < 1 || opt->budget_bytes == 0) return LESGPU_EINVAL;
     if (!opt->chem_path[0] || !opt->tran_path[0]) return LESGPU_EINVAL;
     if (opt->prep_threads < 0 || opt->prep_threads > 64) return LESGPU_EINVAL;
+    if (opt->policy != LES_SERVE_FIFO && opt->policy != LES_SERVE_SHORTEST) return LESGPU_EINVAL;
     *out = NULL;
     les_serve* s = (les_serve*)calloc(1, sizeof(les_serve));
     if (!s) return LESGPU_ENOMEM;
@@ -453,9 +455,50 @@ static void harvest(les_serve* s) {
     }
 }
 
-/* Reserve budget and a slot for queued requests in arrival order and hand them to the
-   set-up workers.  Returns how many were handed out. */
+/* A queued request that may be admitted now: not yet handed out, and not waiting for other
+   requests to end after its set-up found the device full. */
+static int admissible(const les_serve* s, const serve_req* q) {
+    if (q->state != LES_REQ_QUEUED || phase_of((les_serve*)s, (serve_req*)q) != PH_NONE) return 0;
+    if (q->retry_after >= 0 && s->n_done + s->n_failed + s->n_cancelled <= q->retry_after && s->n_slots > 0) return 0;
+    return 1;
+}
+
+static void admit_one(les_serve* s, serve_req* q) {
+    pthread_mutex_lock(&s->mu);
+    s->in_use += q->bytes;
+    s->n_slots++;
+    pthread_mutex_unlock(&s->mu);
+    q->t_admit = now_s();
+    if (s->t_first_admit < 0) s->t_first_admit = q->t_admit;
+    hand_out(s, q, PH_PREP);
+}
+
+/* LES_SERVE_SHORTEST: the admissible request with the least work (cells x steps) first, ties
+   in arrival order; without backfill the round stops at the first one whose memory does not
+   fit, with backfill the shortest that fits is taken. */
+static int admit_shortest(les_serve* s) {
+    int k = 0;
+    while (s->n_slots < s->opt.max_slots) {
+        serve_req* best = NULL;
+        double best_w = 0.0;
+        for (long long i = s->head; i < s->n; i++) {
+            serve_req* q = s->reqs[i];
+            if (!admissible(s, q)) continue;
+            if (s->opt.backfill && s->in_use + q->bytes > s->opt.budget_bytes) continue;
+            const double w = (double)q->cfg.nx * q->cfg.ny * q->cfg.nz * (double)q->nsteps;
+            if (!best || w < best_w) { best = q; best_w = w; }
+        }
+        if (!best || s->in_use + best->bytes > s->opt.budget_bytes) break;
+        admit_one(s, best);
+        k++;
+    }
+    return k;
+}
+
+/* Reserve budget and a slot for queued requests in arrival order (or least work first) and
+   hand them to the set-up workers.  Returns how many were handed out. */
 static int admit_queued(les_serve* s) {
+    if (s->opt.policy == LES_SERVE_SHORTEST) return admit_shortest(s);
     int k = 0;
     for (long long i = s->head; i < s->n && s->n_slots < s->opt.max_slots; i++) {
         serve_req* q = s->reqs[i];
@@ -468,13 +511,7 @@ static int admit_queued(les_serve* s) {
             if (s->opt.backfill) continue;
             break;
         }
-        pthread_mutex_lock(&s->mu);
-        s->in_use += q->bytes;
-        s->n_slots++;
-        pthread_mutex_unlock(&s->mu);
-        q->t_admit = now_s();
-        if (s->t_first_admit < 0) s->t_first_admit = q->t_admit;
-        hand_out(s, q, PH_PREP);
+        admit_one(s, q);
         k++;
     }
     return k;

@@ -30,7 +30,12 @@ STATE_NAMES = {QUEUED: "queued", ACTIVE: "active", DONE: "done", CANCELLED: "can
 class ServeOptions(C.Structure):
     _fields_ = [("budget_bytes", C.c_size_t), ("max_slots", C.c_int), ("quantum_steps", C.c_int),
                 ("keep_results", C.c_int), ("autotune", C.c_int), ("backfill", C.c_int), ("device", C.c_int),
-                ("chem_path", C.c_char * 1024), ("tran_path", C.c_char * 1024), ("prep_threads", C.c_int)]
+                ("chem_path", C.c_char * 1024), ("tran_path", C.c_char * 1024), ("prep_threads", C.c_int),
+                ("policy", C.c_int)]
+
+
+# admission order (les_serve.h)
+FIFO, SHORTEST = 0, 1
 
 
 class RequestInfo(C.Structure):
@@ -77,7 +82,8 @@ def request_bytes(cfg: SolverConfig, precision: int = N.FP32, quantum: int = 16)
 class Server:
     def __init__(self, budget_bytes: int = 150 * 10**9, max_slots: int = 16, quantum: int = 16,
                  keep_results: bool = True, autotune: bool = False, backfill: bool = False, device: int = 0,
-                 chem: str = N.CHEM_BIN, tran: str = N.TRAN_BIN, prep_threads: Optional[int] = None):
+                 chem: str = N.CHEM_BIN, tran: str = N.TRAN_BIN, prep_threads: Optional[int] = None,
+                 policy: int = FIFO):
         L = _lib()
         o = ServeOptions()
         L.les_serve_default_options(C.byref(o))
@@ -86,6 +92,7 @@ class Server:
         o.chem_path, o.tran_path = chem.encode(), tran.encode()
         if prep_threads is not None:
             o.prep_threads = prep_threads
+        o.policy = policy
         h = C.c_void_p()
         rc = L.les_serve_create(C.byref(o), C.byref(h))
         if rc:
@@ -219,16 +226,18 @@ def main(argv=None) -> int:
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--prep-threads", type=int, default=None, help="set-up / tear-down worker threads")
     ap.add_argument("--max-slots", type=int, default=16, help="at most this many requests on the device at once")
+    ap.add_argument("--policy", choices=["fifo", "shortest"], default="fifo",
+                    help="admission order: arrival, or least work (cells x steps) first")
     a = ap.parse_args(argv)
     prec = N.FP32 if a.precision == "fp32" else N.FP64
     reqs = poisson_requests(a.requests, rate=a.rate, steps=tuple(a.steps), seed=a.seed)
     srv = Server(budget_bytes=int(a.budget_gb * 1e9), max_slots=a.max_slots, quantum=a.quantum, autotune=True,
-                 prep_threads=a.prep_threads)
+                 prep_threads=a.prep_threads, policy=SHORTEST if a.policy == "shortest" else FIFO)
     st = replay(srv, reqs, prec)
     srv.close()
     st.pop("ids")
     st.update(requests=a.requests, rate=a.rate, steps=list(a.steps), quantum=a.quantum, precision=a.precision,
-              prep_threads=a.prep_threads, max_slots=a.max_slots,
+              prep_threads=a.prep_threads, max_slots=a.max_slots, policy=a.policy,
               demand_cell_steps=sum(r.cfg.cells * r.nsteps for r in reqs))
     print(json.dumps(st))
     return 0

@@ -11,8 +11,9 @@
  * the host, releasing device memory), so that host work overlaps the device's.
  *
  *   les_serve_submit   queue a request (refused at once if it can never fit the budget);
- *   les_serve_step     one scheduling round: admit queued requests in arrival order while a
- *                      slot is free and their memory fits (their set-up goes to the
+ *   les_serve_step     one scheduling round: admit queued requests (in arrival order, or
+ *                      least work first with LES_SERVE_SHORTEST) while a slot is free and
+ *                      their memory fits (their set-up goes to the
  *                      workers; with nothing running the round waits for it), start
  *                      requests whose set-up is done, and collect the step history of every
  *                      running request in turn, queueing its next quantum_steps steps (one
@@ -51,7 +52,15 @@ typedef struct les_serve_options {
     char tran_path[1024];
     int prep_threads;         /* host threads that set up and tear down requests (0: the
                                  thread calling les_serve_step does it) */
+    int policy;               /* LES_SERVE_FIFO (arrival order) or LES_SERVE_SHORTEST (least work,
+                                 cells x steps, first; ties in arrival order) */
 } les_serve_options;
+
+/* Admission order.  LES_SERVE_SHORTEST lowers the median latency of a burst of requests of
+ * uneven size (the short ones no longer wait behind the long ones) at the cost of the long
+ * ones, which can wait while shorter requests keep arriving. */
+#define LES_SERVE_FIFO 0
+#define LES_SERVE_SHORTEST 1
 
 typedef struct les_serve_request_info {
     int state, error, steps_done, nsteps;

@@ -57,12 +57,13 @@ def _cfg(N, nx, ny, nz, seed):
 
 
 class Server:
-    def __init__(self, fake, budget, slots=8, quantum=4, threads=4, autotune=True):
+    def __init__(self, fake, budget, slots=8, quantum=4, threads=4, autotune=True, policy=0, backfill=0):
         L, S, N = fake
         self.L, self.S, self.N = L, S, N
         o = S.ServeOptions()
         L.les_serve_default_options(C.byref(o))
         o.budget_bytes, o.max_slots, o.quantum_steps, o.autotune, o.prep_threads = budget, slots, quantum, int(autotune), threads
+        o.policy, o.backfill = policy, backfill
         o.chem_path, o.tran_path = b"unused", b"unused"
         self.h = C.c_void_p()
         assert L.les_serve_create(C.byref(o), C.byref(self.h)) == 0
@@ -265,3 +266,41 @@ def test_stress_many_requests(fake, threads, limit_factor):
     for rid, (c, n) in zip(ids, reqs):
         assert srv.result(rid)[5][0] == c.seed * 1000 + n + 5 + 1e6 * (c.nx % 8)
     srv.close()
+
+
+@pytest.mark.parametrize("threads,backfill", [(0, 0), (3, 0), (3, 1)])
+def test_shortest_work_first_admission(fake, threads, backfill):
+    """LES_SERVE_SHORTEST admits the queued request with the least work (cells x steps)
+    first: with one slot, requests submitted together complete in order of work (ties in
+    arrival order), every request finishes with its steps, and the budget is never exceeded."""
+    L, S, N = fake
+    L.fake_configure(0, 0.001, 50.0)
+    shapes = [(20, 8, 4), (8, 4, 4), (16, 4, 8), (12, 6, 4), (8, 4, 4)]
+    steps = [30, 40, 5, 12, 9]
+    reqs = [(_cfg(N, *shapes[q], seed=700 + q), steps[q]) for q in range(5)]
+    one = max(L.les_serve_request_bytes(C.byref(c), 3) for c, _ in reqs)
+    srv = Server(fake, int(2.5 * one), slots=1, quantum=3, threads=threads, policy=S.SHORTEST, backfill=backfill)
+    ids = [srv.submit(c, n) for c, n in reqs]
+    order = []
+    while True:
+        left = srv.step()
+        assert srv.stats()["bytes_in_use"] <= int(2.5 * one)
+        for rid in ids:
+            if rid not in order and srv.info(rid)["state"] == 2:          # LES_REQ_DONE
+                order.append(rid)
+        if left == 0:
+            break
+    work = {rid: c.nx * c.ny * c.nz * n for rid, (c, n) in zip(ids, reqs)}
+    assert sorted(order, key=lambda r: (work[r], r)) == order, (order, work)
+    for rid, (c, n) in zip(ids, reqs):
+        assert srv.result(rid)[0][0] == c.seed * 1000 + n + 1e6 * (c.nx % 8)
+    srv.close()
+
+
+def test_unknown_policy_is_refused(fake):
+    L, S, N = fake
+    o = S.ServeOptions()
+    L.les_serve_default_options(C.byref(o))
+    o.chem_path, o.tran_path, o.policy = b"unused", b"unused", 7
+    h = C.c_void_p()
+    assert L.les_serve_create(C.byref(o), C.byref(h)) == -1
