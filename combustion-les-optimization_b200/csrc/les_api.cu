@@ -1336,7 +1336,8 @@ void lesgpu_group_destroy(lesgpu_group* g) {
     if (!g) return;
     if (g->root) cudaStreamSynchronize(g->root);
     if (g->exec) cudaGraphExecDestroy(g->exec);
-    for (les::MemberTab* t : g->tabs) if (t) cudaFree(t);
+    for (les::MemberTab* t : g->tabs) if (t && g->root) cudaFreeAsync(t, g->root);
+    if (g->root) cudaStreamSynchronize(g->root);
     for (cudaEvent_t e : g->heads) if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : g->stages) if (e) cudaEventDestroy(e);
     for (cudaStream_t st : g->bstreams) if (st) cudaStreamDestroy(st);
@@ -1464,9 +1465,14 @@ int lesgpu_group_create_batched(lesgpu_ctx* const* ctxs, int n, int max_per_batc
         std::vector<les::MemberTab> tab;
         const DevCtx& d0 = ctxs[g->batches[b][0]]->d;
         for (int q : g->batches[b]) tab.push_back(member_entry(d0, ctxs[q]->d));
-        if (e == cudaSuccess) e = cudaMalloc(&g->tabs[b], tab.size() * sizeof(les::MemberTab));
+        // from the stream-ordered pool, like every other device buffer (no device-wide
+        // synchronisation when the group is destroyed)
         if (e == cudaSuccess)
-            e = cudaMemcpy(g->tabs[b], tab.data(), tab.size() * sizeof(les::MemberTab), cudaMemcpyHostToDevice);
+            e = cudaMallocAsync((void**)&g->tabs[b], tab.size() * sizeof(les::MemberTab), g->root);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(g->tabs[b], tab.data(), tab.size() * sizeof(les::MemberTab), cudaMemcpyHostToDevice,
+                                g->root);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(g->root);
     }
     if (e != cudaSuccess) { int r = cuda_fail(c0, e, "group_create_batched"); lesgpu_group_destroy(g); return r; }
     // capture one step: every member's dt and draws (then its SEM plane) on its stream; each
