@@ -1001,7 +1001,7 @@ static void drop_graph(DevCtx& d) {
 int lesgpu_set_tiles(lesgpu_ctx* ctx, const int tiles[5]) {
     if (!ctx || !tiles) return LESGPU_EINVAL;
     for (int q = 0; q < les::NSH_CLASSES; q++)
-        if (tiles[q] < 0 || tiles[q] >= les::NSHAPES) return fail(ctx, LESGPU_EINVAL, "tile index out of range");
+        if (!les::shape_allowed(q, tiles[q])) return fail(ctx, LESGPU_EINVAL, "tile index out of range for its class");
     DevCtx& d = ctx->d;
     CK(cudaStreamSynchronize(d.stream));
     for (int q = 0; q < les::NSH_CLASSES; q++) d.shape[q] = tiles[q];
@@ -1043,7 +1043,9 @@ int lesgpu_autotune(lesgpu_ctx* ctx, int reps, int tiles_out[5], double* ms_out)
     double ms[4][les::NSHAPES];
     cudaError_t e = cudaSuccess;
     for (int t = 0; t < les::NSHAPES && e == cudaSuccess; t++) {
-        for (int q = 0; q < les::NSH_CLASSES; q++) d.shape[q] = t;
+        // a 512-thread tile is timed for the strain, flow and scalar classes; the filter and
+        // EOS kernels keep the first tile meanwhile
+        for (int q = 0; q < les::NSH_CLASSES; q++) d.shape[q] = les::shape_allowed(q, t) ? t : 0;
         d.timing = false;
         e = (d.precision == LESGPU_FP64) ? les::rhs_only_f64(d, 0) : les::rhs_only_f32(d, 0);   // warm-up
         d.timing = true;
@@ -1051,7 +1053,8 @@ int lesgpu_autotune(lesgpu_ctx* ctx, int reps, int tiles_out[5], double* ms_out)
         for (int r = 0; r < reps && e == cudaSuccess; r++)
             e = (d.precision == LESGPU_FP64) ? les::rhs_only_f64(d, 0) : les::rhs_only_f32(d, 0);
         for (int c = 0; c < 4; c++)
-            ms[c][t] = d.kcount[cls_of[c]] > 0 ? d.kms[cls_of[c]] / (double)d.kcount[cls_of[c]] : 1e30;
+            ms[c][t] = (les::shape_allowed(c, t) && d.kcount[cls_of[c]] > 0)
+                           ? d.kms[cls_of[c]] / (double)d.kcount[cls_of[c]] : 1e30;
     }
     d.timing = was_timing;
     for (int q = 0; q < 8; q++) { d.kms[q] = 0.0; d.kcount[q] = 0; }

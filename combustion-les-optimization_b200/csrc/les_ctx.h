@@ -11,18 +11,31 @@
 
 namespace les {
 
-// Thread-block tiles of the per-cell kernels, (k extent, j extent, i extent), 256 threads each.
-// Every kernel indexes through blockDim, so the tile is a launch parameter chosen per kernel
-// class (lesgpu_set_tiles / lesgpu_autotune); the results do not depend on it except through
-// the order of the block partial sums of <rho_f>.  Tiles spanning several i-planes keep the
-// i-neighbours a block reads in its own SM's L1.
+// Thread-block tiles of the per-cell kernels, (k extent, j extent, i extent).  Every kernel
+// indexes through blockDim, so the tile is a launch parameter chosen per kernel class
+// (lesgpu_set_tiles / lesgpu_autotune); the results do not depend on it except through the
+// order of the block partial sums of <rho_f>.  Tiles spanning several i-planes keep the
+// i-neighbours a block reads in its own SM's L1.  The first NSHAPES_256 tiles have 256
+// threads and serve every class; the 512-thread tiles after them serve the classes without
+// block reductions (strain, flow, scalar), whose kernels are instantiated for both sizes: a
+// larger tile reads fewer halo cells per cell it computes, so the resident blocks' stencil
+// tiles take less of L1 (the scalar pass at 256x128x128 on B200: 0.71 ms per launch with
+// 16x4x8 against 0.75 with the best 256-thread tile; 1024-thread tiles were no faster in
+// FP64 and slower in FP32).
 struct Shape {
     int bx, by, bz;
 };
-constexpr int NSHAPES = 8;
-constexpr Shape kShapes[NSHAPES] = {{32, 8, 1}, {64, 4, 1}, {16, 16, 1}, {128, 2, 1},
-                                    {32, 4, 2}, {16, 8, 2}, {32, 2, 4}, {16, 4, 4}};
+constexpr int NSHAPES_256 = 8;
+constexpr int NSHAPES = 13;
+constexpr Shape kShapes[NSHAPES] = {{32, 8, 1}, {64, 4, 1}, {16, 16, 1}, {128, 2, 1}, {32, 4, 2},
+                                    {16, 8, 2}, {32, 2, 4}, {16, 4, 4}, {32, 8, 2}, {32, 4, 4},
+                                    {16, 8, 4}, {16, 4, 8}, {64, 4, 2}};
 enum { SH_FILTER = 0, SH_STRAIN = 1, SH_FLOW = 2, SH_SCALAR = 3, SH_EOS = 4, NSH_CLASSES = 5 };
+constexpr int shape_threads(int s) { return kShapes[s].bx * kShapes[s].by * kShapes[s].bz; }
+// whether tile s may serve kernel class cls (the filter and EOS kernels reduce over 256-thread blocks)
+constexpr bool shape_allowed(int cls, int s) {
+    return s >= 0 && s < NSHAPES && (s < NSHAPES_256 || (cls != SH_FILTER && cls != SH_EOS));
+}
 
 inline size_t blocks_for_shape(int nx, int ny, int nz, int s) {
     const Shape t = kShapes[s];

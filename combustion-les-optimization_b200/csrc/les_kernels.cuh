@@ -125,6 +125,9 @@ struct MinBlocks<float> {
     static constexpr int filter = LES_MINB_FILTER_F32, strain = LES_MINB_STRAIN_F32, flow = LES_MINB_FLOW_F32,
                          scalar = LES_MINB_SCALAR_F32;
 };
+// The same register budget for a block of `ntb` threads: the resident threads per SM of the
+// 256-thread budget in whole blocks (at least one).
+constexpr int lb_blocks(int minb, int ntb) { return (minb * NT) / ntb > 0 ? (minb * NT) / ntb : 1; }
 
 // ---------------------------------------------------------------------------- helpers
 
@@ -463,8 +466,8 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::filter)
 
 // ------------------------------------------------------------------ pass B: strain + nu_t + S_T
 
-template <typename R, bool BATCH = false>
-__global__ void __launch_bounds__(NT, MinBlocks<R>::strain)
+template <typename R, bool BATCH = false, int NTB = NT>
+__global__ void __launch_bounds__(NTB, lb_blocks(MinBlocks<R>::strain, NTB))
     k_strain(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> F, PropBuf<R> P, Batch B) {
     const auto& K = kc<R>(C);
     int bz = blockIdx.z;
@@ -762,8 +765,8 @@ __device__ __forceinline__ R lap3(const Consts& C, const A& q) {
 
 // C1: momentum (:2552-2697) with calculate_convection_conservative (:683-727) and the G
 // equation (:2706-2825).  Writes k_rhou, k_rhov, k_rhow, k_G of fluid cells.
-template <typename R, bool BATCH = false>
-__global__ void __launch_bounds__(NT, MinBlocks<R>::flow)
+template <typename R, bool BATCH = false, int NTB = NT>
+__global__ void __launch_bounds__(NTB, lb_blocks(MinBlocks<R>::flow, NTB))
     k_rhs_flow(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> F, PropBuf<R> P, KFlow<R> kf,
                KDbg<R> kd, const Scalars* __restrict__ Sc, Batch B) {
     const auto& K = kc<R>(C);
@@ -1096,8 +1099,8 @@ __device__ __forceinline__ void rhs_scalar_cell(const Consts& C, const uint8_t* 
     }
 }
 
-template <typename R, typename RS = R, bool BATCH = false>
-__global__ void __launch_bounds__(NT, MinBlocks<R>::scalar)
+template <typename R, typename RS = R, bool BATCH = false, int NTB = NT>
+__global__ void __launch_bounds__(NTB, lb_blocks(MinBlocks<R>::scalar, NTB))
     k_rhs_scalar(LES_KERNEL_CONSTS, const uint8_t* __restrict__ attr, F11<R> F, PropBuf<R> P, F11<RS> S0, F11<R> St,
                  AccBuf<R> acc, KFlow<R> kf, KDbg<R> kd, const Scalars* __restrict__ Sc, int stage, Batch B) {
     int bz = blockIdx.z;

@@ -46,6 +46,31 @@ static inline dim3 cell_grid(const DevCtx& c, int cls) {
                 (unsigned)((c.nx + t.bz - 1) / t.bz));
 }
 
+// The strain, flow and scalar passes with the kernel instance of their tile's block size.
+template <typename R, bool BATCH>
+static inline void launch_strain(dim3 g, dim3 b, cudaStream_t st, const Consts& hC, const uint8_t* attr,
+                                 const F11<R>& F, const PropBuf<R>& P, const Batch& B) {
+    if (b.x * b.y * b.z == 512) k_strain<R, BATCH, 512><<<g, b, 0, st>>>(hC, attr, F, P, B);
+    else k_strain<R, BATCH><<<g, b, 0, st>>>(hC, attr, F, P, B);
+}
+template <typename R, bool BATCH>
+static inline void launch_flow(dim3 g, dim3 b, cudaStream_t st, const Consts& hC, const uint8_t* attr,
+                               const F11<R>& F, const PropBuf<R>& P, const KFlow<R>& kf, const KDbg<R>& kd,
+                               Scalars* dS, const Batch& B) {
+    if (b.x * b.y * b.z == 512) k_rhs_flow<R, BATCH, 512><<<g, b, 0, st>>>(hC, attr, F, P, kf, kd, dS, B);
+    else k_rhs_flow<R, BATCH><<<g, b, 0, st>>>(hC, attr, F, P, kf, kd, dS, B);
+}
+template <typename R, bool BATCH>
+static inline void launch_scalar(dim3 g, dim3 b, cudaStream_t st, const Consts& hC, const uint8_t* attr,
+                                 const F11<R>& F, const PropBuf<R>& P, const F11<RS>& S, const F11<R>& St,
+                                 const AccBuf<R>& acc, const KFlow<R>& kf, const KDbg<R>& kd, Scalars* dS,
+                                 int stage, const Batch& B) {
+    if (b.x * b.y * b.z == 512)
+        k_rhs_scalar<R, RS, BATCH, 512><<<g, b, 0, st>>>(hC, attr, F, P, S, St, acc, kf, kd, dS, stage, B);
+    else
+        k_rhs_scalar<R, RS, BATCH><<<g, b, 0, st>>>(hC, attr, F, P, S, St, acc, kf, kd, dS, stage, B);
+}
+
 // Every launch that writes per-block partials checks the buffer first: `per_block` values
 // per block for `blocks` blocks must fit in c.part.
 static inline bool part_fits(const DevCtx& c, size_t blocks, size_t per_block) {
@@ -136,16 +161,16 @@ cudaError_t step_impl(DevCtx& c, double dt, int t_loop, bool device_mode) {
         else k_filter_props<R, R><<<gA, bA, 0, st>>>(c.hC, c.attr, St, F, P, c.part, c.dS, s == 3 ? 1 : 0, Batch{});
         tmark_end(c, tm);
         tm = tmark_begin(c, 2);
-        k_strain<R><<<gB, bB, 0, st>>>(c.hC, c.attr, F, P, Batch{});
+        launch_strain<R, false>(gB, bB, st, c.hC, c.attr, F, P, Batch{});
         tmark_end(c, tm);
         // the k-arrays of the first stage are kept for inspection when requested
         const KDbg<R>& kds = (s == 0) ? kd : knone;
         tm = tmark_begin(c, 3);
-        k_rhs_flow<R><<<gC, bC, 0, st>>>(c.hC, c.attr, F, P, kf, kds, c.dS, Batch{});
+        launch_flow<R, false>(gC, bC, st, c.hC, c.attr, F, P, kf, kds, c.dS, Batch{});
         tmark_end(c, tm);
         tm = tmark_begin(c, 5);
         if (c.scalar_tma && c.tma_ok) launch_scalar_tma<R, RS>(c, st, F, P, S, St, acc, kf, kds, s);
-        else k_rhs_scalar<R, RS><<<gD, bD, 0, st>>>(c.hC, c.attr, F, P, S, St, acc, kf, kds, c.dS, s, Batch{});
+        else launch_scalar<R, false>(gD, bD, st, c.hC, c.attr, F, P, S, St, acc, kf, kds, c.dS, s, Batch{});
         tmark_end(c, tm);
     }
     // apply_boundary_conditions (:2967-3161)
@@ -206,9 +231,9 @@ cudaError_t batch_stages(DevCtx& c0, const MemberTab* mt, int nmem, cudaStream_t
     for (int s = 0; s < 4; s++) {
         if (s == 0) k_filter_props<R, RS, true><<<gA, bA, 0, st>>>(c0.hC, c0.attr, S, F, P, c0.part, c0.dS, 0, BA);
         else k_filter_props<R, R, true><<<gA, bA, 0, st>>>(c0.hC, c0.attr, St, F, P, c0.part, c0.dS, s == 3 ? 1 : 0, BA);
-        k_strain<R, true><<<gB, bB, 0, st>>>(c0.hC, c0.attr, F, P, BB);
-        k_rhs_flow<R, true><<<gC, bC, 0, st>>>(c0.hC, c0.attr, F, P, kf, knone, c0.dS, BC);
-        k_rhs_scalar<R, RS, true><<<gD, bD, 0, st>>>(c0.hC, c0.attr, F, P, S, St, acc, kf, knone, c0.dS, s, BD);
+        launch_strain<R, true>(gB, bB, st, c0.hC, c0.attr, F, P, BB);
+        launch_flow<R, true>(gC, bC, st, c0.hC, c0.attr, F, P, kf, knone, c0.dS, BC);
+        launch_scalar<R, true>(gD, bD, st, c0.hC, c0.attr, F, P, S, St, acc, kf, knone, c0.dS, s, BD);
     }
     return cudaGetLastError();
 }
@@ -236,19 +261,18 @@ cudaError_t rhs_only_impl(DevCtx& c, int t_loop) {
                                                                                        c.part, c.dS, 1, Batch{});
     tmark_end(c, tm);
     tm = tmark_begin(c, 2);
-    k_strain<R><<<cell_grid(c, SH_STRAIN), cell_block(c, SH_STRAIN), 0, st>>>(c.hC, c.attr, F, P, Batch{});
+    launch_strain<R, false>(cell_grid(c, SH_STRAIN), cell_block(c, SH_STRAIN), st, c.hC, c.attr, F, P, Batch{});
     tmark_end(c, tm);
     tm = tmark_begin(c, 3);
-    k_rhs_flow<R><<<cell_grid(c, SH_FLOW), cell_block(c, SH_FLOW), 0, st>>>(c.hC, c.attr, F, P, kf, kd, c.dS,
-                                                                            Batch{});
+    launch_flow<R, false>(cell_grid(c, SH_FLOW), cell_block(c, SH_FLOW), st, c.hC, c.attr, F, P, kf, kd, c.dS,
+                          Batch{});
     tmark_end(c, tm);
     tm = tmark_begin(c, 5);
     if (c.scalar_tma && c.tma_ok)
         launch_scalar_tma<R, RS>(c, st, F, P, S, St, acc, kf, kd, 0);
     else
-        k_rhs_scalar<R, RS><<<cell_grid(c, SH_SCALAR), cell_block(c, SH_SCALAR), 0, st>>>(c.hC, c.attr, F, P, S, St,
-                                                                                           acc, kf, kd, c.dS, 0,
-                                                                                           Batch{});
+        launch_scalar<R, false>(cell_grid(c, SH_SCALAR), cell_block(c, SH_SCALAR), st, c.hC, c.attr, F, P, S, St,
+                                acc, kf, kd, c.dS, 0, Batch{});
     tmark_end(c, tm);
     tmark_flush(c);
     return cudaGetLastError();

@@ -362,8 +362,10 @@ class Context:
         return v.value
 
     # thread-block tiles (k extent, j extent, i extent) indexed by lesgpu_set_tiles, per
-    # class {filter, strain, rhs_flow, rhs_scalar, eos}
-    TILES = [(32, 8, 1), (64, 4, 1), (16, 16, 1), (128, 2, 1), (32, 4, 2), (16, 8, 2), (32, 2, 4), (16, 4, 4)]
+    # class {filter, strain, rhs_flow, rhs_scalar, eos}; the 512-thread tiles from index 8 on
+    # serve the strain, flow and scalar classes only (LESGPU_NTILES entries in all)
+    TILES = [(32, 8, 1), (64, 4, 1), (16, 16, 1), (128, 2, 1), (32, 4, 2), (16, 8, 2), (32, 2, 4), (16, 4, 4),
+             (32, 8, 2), (32, 4, 4), (16, 8, 4), (16, 4, 8), (64, 4, 2)]
 
     def autotune(self, reps: int = 3):
         """Install the fastest tile per kernel class; returns (tiles[5], ms[4 classes, tiles])."""

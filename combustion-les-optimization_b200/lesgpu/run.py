@@ -39,6 +39,8 @@ def main(argv=None) -> int:
     if a.tiles == "auto":
         tiles, ms = s.ctx.autotune(3)
         out["tiles"] = tiles
+        # ms per launch, rows filter/strain/flow/scalar, one column per tile (None: not served)
+        out["autotune_ms"] = [[round(float(x), 5) if x < 1e29 else None for x in row] for row in ms]
     elif a.tiles != "default":
         s.ctx.set_tiles([int(t) for t in a.tiles.split(",")])
         out["tiles"] = s.ctx.get_tiles()

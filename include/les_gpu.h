@@ -296,15 +296,18 @@ int lesgpu_avg_upload(lesgpu_ctx* ctx, const double* const* sums, int count);
 
 /* Thread-block tiles of the per-cell kernels (no reference counterpart; the reference is
  * serial C).  tiles[c] for the classes {filter, strain, rhs_flow, rhs_scalar, eos} indexes
- * the LESGPU_NTILES shapes (k extent x j extent x i extent, 256 threads): 0 = 32x8x1,
- * 1 = 64x4x1, 2 = 16x16x1, 3 = 128x2x1, 4 = 32x4x2, 5 = 16x8x2, 6 = 32x2x4, 7 = 16x4x4.
- * lesgpu_autotune times `reps` evaluations of the four stage kernels per shape at the
- * current state, picks the fastest shape per class (eos follows filter), installs it and
- * optionally returns it and the times (ms_out: 4 classes x LESGPU_NTILES, ms per launch).  It
- * leaves the state, the dt inputs and the step counters as they were.  The tile changes
- * only the launch geometry; results change only through the summation order of the block
- * partials of <rho_f> (rounding level). */
-#define LESGPU_NTILES 8
+ * the LESGPU_NTILES shapes (k extent x j extent x i extent).  256 threads, every class:
+ * 0 = 32x8x1, 1 = 64x4x1, 2 = 16x16x1, 3 = 128x2x1, 4 = 32x4x2, 5 = 16x8x2, 6 = 32x2x4,
+ * 7 = 16x4x4; 512 threads, the strain, rhs_flow and rhs_scalar classes only (a filter or
+ * eos index above 7 is refused with LESGPU_EINVAL): 8 = 32x8x2, 9 = 32x4x4, 10 = 16x8x4,
+ * 11 = 16x4x8, 12 = 64x4x2.  lesgpu_autotune times `reps` evaluations of the four stage
+ * kernels per shape at the current state, picks the fastest shape per class (eos follows
+ * filter), installs it and optionally returns it and the times (ms_out: 4 classes x
+ * LESGPU_NTILES, ms per launch; 1e30 where a shape does not serve the class).  It leaves the
+ * state, the dt inputs and the step counters as they were.  The tile changes only the launch
+ * geometry; results change only through the summation order of the block partials of
+ * <rho_f> (rounding level). */
+#define LESGPU_NTILES 13
 int lesgpu_set_tiles(lesgpu_ctx* ctx, const int tiles[5]);
 int lesgpu_get_tiles(const lesgpu_ctx* ctx, int tiles[5]);
 int lesgpu_autotune(lesgpu_ctx* ctx, int reps, int tiles_out[5], double* ms_out);
