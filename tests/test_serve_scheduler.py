@@ -275,9 +275,10 @@ def test_shortest_work_first_admission(fake, threads, backfill):
     arrival order), every request finishes with its steps, and the budget is never exceeded."""
     L, S, N = fake
     L.fake_configure(0, 0.001, 50.0)
-    shapes = [(20, 8, 4), (8, 4, 4), (16, 4, 8), (12, 6, 4), (8, 4, 4)]
-    steps = [30, 40, 5, 12, 9]
-    reqs = [(_cfg(N, *shapes[q], seed=700 + q), steps[q]) for q in range(5)]
+    # requests 2 and 5 ask for the same work (2560 cell-steps): 2 arrived first, so it goes first
+    shapes = [(20, 8, 4), (8, 4, 4), (16, 4, 8), (12, 6, 4), (8, 4, 4), (8, 8, 8)]
+    steps = [30, 40, 5, 12, 9, 5]
+    reqs = [(_cfg(N, *shapes[q], seed=700 + q), steps[q]) for q in range(len(shapes))]
     one = max(L.les_serve_request_bytes(C.byref(c), 3) for c, _ in reqs)
     srv = Server(fake, int(2.5 * one), slots=1, quantum=3, threads=threads, policy=S.SHORTEST, backfill=backfill)
     ids = [srv.submit(c, n) for c, n in reqs]
@@ -291,6 +292,7 @@ def test_shortest_work_first_admission(fake, threads, backfill):
         if left == 0:
             break
     work = {rid: c.nx * c.ny * c.nz * n for rid, (c, n) in zip(ids, reqs)}
+    assert len(set(work.values())) < len(work)           # the tie is there
     assert sorted(order, key=lambda r: (work[r], r)) == order, (order, work)
     for rid, (c, n) in zip(ids, reqs):
         assert srv.result(rid)[0][0] == c.seed * 1000 + n + 1e6 * (c.nx % 8)
