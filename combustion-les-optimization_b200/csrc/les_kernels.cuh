@@ -249,11 +249,13 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
     const R L2 = L * L;
     const R L3 = pow3_rn(L);
     // pure-species viscosity and conductivity (:394-398, :431-437)
-    R muk[NSP], lamk[NSP];
+    // species with X < 1e-12 take no part in either mixing rule: their pure-species values
+    // are not evaluated
+    R muk[NSP];
 #pragma unroll
     for (int s = 0; s < NSP; s++) {
-        muk[s] = fit_prop<R>(K.eta[s], C.eta_zero[s], L, L2, L3) * R(0.1);
-        lamk[s] = fit_prop<R>(K.lam[s], C.lam_zero[s], L, L2, L3) * R(1e-5);
+        muk[s] = R(1.0);
+        if (!(X[s] < R(1e-12))) muk[s] = fit_prop<R>(K.eta[s], C.eta_zero[s], L, L2, L3) * R(0.1);
     }
     // Wilke (:1530-1546) and Wassiljew (:1842-1863) share the same phi_ij, the same skip
     // rule and the same summation order, so one denominator per species serves both.
@@ -266,6 +268,9 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
     R smu[NSP], rsmu[NSP];
 #pragma unroll
     for (int s = 0; s < NSP; s++) {
+        smu[s] = R(1.0);
+        rsmu[s] = R(1.0);
+        if (X[s] < R(1e-12)) continue;
         smu[s] = qsqrt(muk[s]);
         if constexpr (kF32) rsmu[s] = rsqrtf(muk[s]);
         else rsmu[s] = qdiv(R(1.0), smu[s]);
@@ -284,14 +289,16 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
             den += X[b] * ph;
         }
         if (den > R(1e-9)) {
+            // the pure-species conductivity only where it is used
+            const R lamk = fit_prop<R>(K.lam[a], C.lam_zero[a], L, L2, L3) * R(1e-5);
             if constexpr (kF32) {
                 const R iden = qdiv(R(1.0), den);
                 mu += (X[a] * muk[a]) * iden;
-                lam += (X[a] * lamk[a]) * iden;
+                lam += (X[a] * lamk) * iden;
             } else {
                 const R yden = qdiv(R(1.0), den);
                 mu += mdiv(X[a] * muk[a], den, yden);
-                lam += mdiv(X[a] * lamk[a], den, yden);
+                lam += mdiv(X[a] * lamk, den, yden);
             }
         }
     }
