@@ -189,9 +189,11 @@ __device__ __forceinline__ double eos_rho_state(const Consts& C, double T, const
 }
 
 // Cell-local mixture properties of one fluid cell (attr == 3).
-template <typename R>
+// The diffusivities D_k are handed to store_d as soon as they are known (before the mixing
+// rules, so that they and the fit polynomial's powers of ln T are not held across them).
+template <typename R, typename StoreD>
 __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP], R rhof, R& mu_mix, R& nu,
-                                           R D[NSP], R& aT, R& cp_out, R& lam_out, R& alpha) {
+                                           const StoreD& store_d, R& aT, R& cp_out, R& lam_out, R& alpha) {
     const auto& K = kc<R>(C);
     R X[NSP];
     R syw = R(0);
@@ -225,8 +227,10 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
     if (!ok) {
         nu = R(1.5e-5);
         mu_mix = R(1.8e-5);
+        R D[NSP];
 #pragma unroll
         for (int s = 0; s < NSP; s++) D[s] = R(1e-5);
+        store_d(D);
         R lam = R(0.025);
         lam_out = lam;
         alpha = R(1.8e-5);
@@ -248,6 +252,60 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
     const R L = qlog(Tl);
     const R L2 = L * L;
     const R L3 = pow3_rn(L);
+    {
+        // Hirschfelder-Curtiss (:1716-1749): sx_a = sum over b != a (ascending b) of X_b / D_ab.
+        // With a symmetric fit table each D_ab is evaluated once per unordered pair and both
+        // sums take their term from it; the rows are visited in ascending order, so each sx_a
+        // still receives its terms in ascending b.  1 / D_ab is taken directly as
+        // exp(-P_ab(ln T)) * 1e4 (D_ab = exp(P_ab) * 1e-4), one exponential and no division: the
+        // terms X_b / D_ab differ from the reference's quotients by at most ~2 ulp (the FP64
+        // property pass 2.82 -> 2.53 ms per 256x128x128 step); the skip rule D_ab > 1e-12 reads
+        // 1 / D_ab < 1e12.
+        R sxa[NSP], D[NSP];
+#pragma unroll
+        for (int a = 0; a < NSP; a++) sxa[a] = R(0);
+        if (C.dco_sym) {
+#pragma unroll
+            for (int a = 0; a < NSP; a++)
+#pragma unroll
+                for (int b = a + 1; b < NSP; b++) {
+                    if (!(X[a] > R(1e-12) || X[b] > R(1e-12))) continue;
+                    if (C.dco_zero[a][b]) continue;          // D_ab = 0 fails D_ab > 1e-12
+                    const auto& co = K.dco[a][b];
+                    const R lp = (R)co[0] + (R)co[1] * L + (R)co[2] * L2 + (R)co[3] * L3;
+                    const R y = qexp(-lp) * R(1e4);
+                    if (!(y < R(1e12))) continue;
+                    if (X[b] > R(1e-12)) sxa[a] += X[b] * y;
+                    if (X[a] > R(1e-12)) sxa[b] += X[a] * y;
+                }
+        } else {
+#pragma unroll
+            for (int a = 0; a < NSP; a++)
+#pragma unroll
+                for (int b = 0; b < NSP; b++) {
+                    if (a == b || !(X[b] > R(1e-12))) continue;
+                    const R v = fit_prop<R>(K.dco[a][b], C.dco_zero[a][b], L, L2, L3) * R(1e-4);
+                    if (v > R(1e-12)) sxa[a] += qdiv(X[b], v);
+                }
+        }
+#pragma unroll
+        for (int a = 0; a < NSP; a++) {
+            const R sx = sxa[a];
+            R Dv;
+            if (fabs(R(1.0) - X[a]) < R(1e-9)) {
+                int o = (a != N2) ? N2 : O2;
+                Dv = fit_prop<R>(K.dco[a][o], C.dco_zero[a][o], L, L2, L3) * R(1e-4);
+            } else if (sx > R(1e-12)) {
+                Dv = qdiv(R(1.0) - X[a], sx);
+            } else {
+                Dv = R(1e-5);
+            }
+            // pressure correction PATM / (p0 + P_f) (:1743-1746): P is identically zero in the
+            // reference (it is never assigned a non-zero value), so the factor is exactly 1.
+            D[a] = fmax(R(1e-9), fmin(R(1e-2), Dv));
+        }
+        store_d(D);
+    }
     // pure-species viscosity and conductivity (:394-398, :431-437)
     // species with X < 1e-12 take no part in either mixing rule: their pure-species values
     // are not evaluated
@@ -265,25 +323,24 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
     // from 3.02 to 2.77 ms per 256x128x128 step); mu_a / mu_a stays exactly 1 for a positive
     // finite mu_a.
     R mu = R(0), lam = R(0);
-    R smu[NSP], rsmu[NSP];
+    R rsmu[NSP];
 #pragma unroll
     for (int s = 0; s < NSP; s++) {
-        smu[s] = R(1.0);
         rsmu[s] = R(1.0);
         if (X[s] < R(1e-12)) continue;
-        smu[s] = qsqrt(muk[s]);
         if constexpr (kF32) rsmu[s] = rsqrtf(muk[s]);
-        else rsmu[s] = qdiv(R(1.0), smu[s]);
+        else rsmu[s] = qdiv(R(1.0), qsqrt(muk[s]));
     }
 #pragma unroll
     for (int a = 0; a < NSP; a++) {
         if (X[a] < R(1e-12)) continue;
+        const R smu_a = qsqrt(muk[a]);
         R den = R(0);
 #pragma unroll
         for (int b = 0; b < NSP; b++) {
             if (X[b] < R(1e-12)) continue;
             // as in the reference, a zero or infinite mu_a gives NaN on the diagonal too
-            const R sr = (a == b && muk[a] > R(0) && muk[a] <= R(1e300)) ? R(1.0) : smu[a] * rsmu[b];
+            const R sr = (a == b && muk[a] > R(0) && muk[a] <= R(1e300)) ? R(1.0) : smu_a * rsmu[b];
             R t = R(1.0) + sr * (R)K.wpow[a][b];
             R ph = cdv(t * t, K.d_wden[a][b]);
             den += X[b] * ph;
@@ -312,57 +369,6 @@ __device__ __forceinline__ void cell_props(const Consts& C, R Tl, const R Yf[NSP
     if (qok) q = qdiv(lmix, rhof * Cp);
     alpha = fmax(R(1e-7), qok ? q : R(1.8e-5));
     aT = q;
-    // Hirschfelder-Curtiss (:1716-1749): sx_a = sum over b != a (ascending b) of X_b / D_ab.
-    // With a symmetric fit table each D_ab is evaluated once per unordered pair and both
-    // sums take their term from it; the rows are visited in ascending order, so each sx_a
-    // still receives its terms in ascending b.  1 / D_ab is taken directly as
-    // exp(-P_ab(ln T)) * 1e4 (D_ab = exp(P_ab) * 1e-4), one exponential and no division: the
-    // terms X_b / D_ab differ from the reference's quotients by at most ~2 ulp (the FP64
-    // property pass 2.82 -> 2.53 ms per 256x128x128 step); the skip rule D_ab > 1e-12 reads
-    // 1 / D_ab < 1e12.
-    R sxa[NSP];
-#pragma unroll
-    for (int a = 0; a < NSP; a++) sxa[a] = R(0);
-    if (C.dco_sym) {
-#pragma unroll
-        for (int a = 0; a < NSP; a++)
-#pragma unroll
-            for (int b = a + 1; b < NSP; b++) {
-                if (!(X[a] > R(1e-12) || X[b] > R(1e-12))) continue;
-                if (C.dco_zero[a][b]) continue;          // D_ab = 0 fails D_ab > 1e-12
-                const auto& co = K.dco[a][b];
-                const R lp = (R)co[0] + (R)co[1] * L + (R)co[2] * L2 + (R)co[3] * L3;
-                const R y = qexp(-lp) * R(1e4);
-                if (!(y < R(1e12))) continue;
-                if (X[b] > R(1e-12)) sxa[a] += X[b] * y;
-                if (X[a] > R(1e-12)) sxa[b] += X[a] * y;
-            }
-    } else {
-#pragma unroll
-        for (int a = 0; a < NSP; a++)
-#pragma unroll
-            for (int b = 0; b < NSP; b++) {
-                if (a == b || !(X[b] > R(1e-12))) continue;
-                const R v = fit_prop<R>(K.dco[a][b], C.dco_zero[a][b], L, L2, L3) * R(1e-4);
-                if (v > R(1e-12)) sxa[a] += qdiv(X[b], v);
-            }
-    }
-#pragma unroll
-    for (int a = 0; a < NSP; a++) {
-        const R sx = sxa[a];
-        R Dv;
-        if (fabs(R(1.0) - X[a]) < R(1e-9)) {
-            int o = (a != N2) ? N2 : O2;
-            Dv = fit_prop<R>(K.dco[a][o], C.dco_zero[a][o], L, L2, L3) * R(1e-4);
-        } else if (sx > R(1e-12)) {
-            Dv = qdiv(R(1.0) - X[a], sx);
-        } else {
-            Dv = R(1e-5);
-        }
-        // pressure correction PATM / (p0 + P_f) (:1743-1746): P is identically zero in the
-        // reference (it is never assigned a non-zero value), so the factor is exactly 1.
-        D[a] = fmax(R(1e-9), fmin(R(1e-2), Dv));
-    }
 }
 
 // ------------------------------------------------------------------ pass A: filter + props
@@ -411,12 +417,14 @@ __global__ void __launch_bounds__(NT, MinBlocks<R>::filter)
         }
         if (a == 1 || a == 2 || a == 3 || a == 5) mass = (((double)f[5] * C.dx) * C.dy) * C.dz;
         if (a == 3) {
-            R mu_mix, nu, D[NSP], aT, cp, lam, alpha;
-            cell_props<R>(C, f[3], &f[6], f[5], mu_mix, nu, D, aT, cp, lam, alpha);
+            R mu_mix, nu, aT, cp, lam, alpha;
+            auto store_d = [&](const R* D) {
+#pragma unroll
+                for (int s = 0; s < NSP; s++) P.D[s][id] = D[s];
+            };
+            cell_props<R>(C, f[3], &f[6], f[5], mu_mix, nu, store_d, aT, cp, lam, alpha);
             P.mu_mix[id] = mu_mix;
             P.nu[id] = nu;
-#pragma unroll
-            for (int s = 0; s < NSP; s++) P.D[s][id] = D[s];
             P.aT[id] = aT;
             if (P.dbg_cp) { P.dbg_cp[id] = cp; P.dbg_lam[id] = lam; P.dbg_alpha[id] = alpha; }
             mnu = (double)nu;
