@@ -52,3 +52,22 @@ def test_bind_device_rejects_a_negative_device(lesgpu_native):
     lib.lesgpu_bind_device.argtypes = [ctypes.c_int]
     lib.lesgpu_bind_device.restype = ctypes.c_int
     assert lib.lesgpu_bind_device(-1) == -1          # LESGPU_EINVAL, no CUDA call made
+
+
+def test_tile_tables_agree():
+    """The tile table of the kernels (csrc/les_ctx.h), the count the header publishes
+    (LESGPU_NTILES: lesgpu_autotune writes 4 x LESGPU_NTILES times into the caller's buffer)
+    and the binding's table, which sizes that buffer, list the same tiles."""
+    from lesgpu import native
+    with open(os.path.join(ROOT, "include", "les_gpu.h")) as f:
+        ntiles = int(re.search(r"#define\s+LESGPU_NTILES\s+(\d+)", f.read()).group(1))
+    with open(os.path.join(ROOT, "combustion-les-optimization_b200", "csrc", "les_ctx.h")) as f:
+        ctx = f.read()
+    body = re.search(r"kShapes\[NSHAPES\]\s*=\s*\{(.*?)\};", ctx, re.S).group(1)
+    shapes = [tuple(int(x) for x in m) for m in re.findall(r"\{\s*(\d+)\s*,\s*(\d+)\s*,\s*(\d+)\s*\}", body)]
+    assert int(re.search(r"constexpr int NSHAPES = (\d+);", ctx).group(1)) == ntiles
+    assert len(shapes) == ntiles
+    assert [tuple(t) for t in native.Context.TILES] == shapes
+    n256 = int(re.search(r"constexpr int NSHAPES_256 = (\d+);", ctx).group(1))
+    assert all(bx * by * bz == 256 for bx, by, bz in shapes[:n256])
+    assert all(bx * by * bz == 512 for bx, by, bz in shapes[n256:])
